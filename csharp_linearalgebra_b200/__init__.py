@@ -1,0 +1,349 @@
+"""tensile_b200: the Tensile dense hot path on B200 (sm_100a).
+
+A host-side mirror of the reference library's public surface for the hot path
+(src/Tensile: Workspace.Multiply, FactorLu / LuDecomposition<T>.Solve /
+SolveAdjoint / Determinant / ReciprocalCondition, NormEstimate.Of over dense
+power operators, MatrixExponential.Expm, MatrixExponentialAction.Expmv),
+calling the CUDA library through its C ABI. Matrices are numpy arrays
+(float64 or complex128); they are read in column-major order, as Matrix<T>
+stores them.
+
+Errors map to the reference's exceptions:
+  ArgumentException            -> ValueError
+  ArgumentNullException        -> ValueError
+  ArgumentOutOfRangeException  -> OverflowError / ValueError
+  InvalidOperationException    -> SingularMatrixError (singular factorization)
+  AllocationLimitException     -> AllocationLimitError
+  ObjectDisposedException      -> ObjectDisposedError
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+__all__ = [
+    "Workspace", "LuDecomposition", "NormEstimateResult", "ExpmDiagnostics", "ExpmvDiagnostics",
+    "SingularMatrixError", "AllocationLimitError", "ObjectDisposedError", "DeviceTimeoutError",
+    "DEFAULT_SEED", "DEFAULT_COLUMNS", "DEFAULT_MAX_ITERATIONS",
+]
+
+DEFAULT_COLUMNS = 2          # NormEstimate.DefaultColumns
+DEFAULT_MAX_ITERATIONS = 5   # NormEstimate.DefaultMaxIterations
+DEFAULT_SEED = 20260915      # NormEstimate.DefaultSeed
+
+
+class SingularMatrixError(ArithmeticError):
+    """InvalidOperationException for an exactly singular factorization."""
+
+
+class AllocationLimitError(MemoryError):
+    """AllocationLimitException: a request exceeds TensileLimits.MaxElements."""
+
+
+class ObjectDisposedError(RuntimeError):
+    """ObjectDisposedException: the workspace has been disposed."""
+
+
+class DeviceTimeoutError(RuntimeError):
+    """A bounded device-side wait gave up; the context stays usable."""
+
+
+def _raise(code: int, msg: str):
+    if code == N.TNS_E_ARGUMENT or code == N.TNS_E_NULL:
+        raise ValueError(msg)
+    if code == N.TNS_E_SINGULAR:
+        raise SingularMatrixError(msg)
+    if code == N.TNS_E_ALLOCATION_LIMIT:
+        raise AllocationLimitError(msg)
+    if code == N.TNS_E_OUT_OF_RANGE:
+        raise OverflowError(msg)
+    if code == N.TNS_E_DISPOSED:
+        raise ObjectDisposedError(msg)
+    if code == N.TNS_E_TIMEOUT:
+        raise DeviceTimeoutError(msg)
+    if code == N.TNS_E_OUT_OF_MEMORY:
+        raise MemoryError(msg)
+    raise RuntimeError(f"tensile_b200 error {code}: {msg}")
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _fortran(a, complex_: bool):
+    return np.asfortranarray(a, dtype=np.complex128 if complex_ else np.float64)
+
+
+def _ld(a: np.ndarray) -> int:
+    return max(1, a.shape[0])
+
+
+@dataclass(frozen=True)
+class NormEstimateResult:
+    """NormEstimateResult(Value, Iterations, Products)."""
+    value: float
+    iterations: int
+    products: int
+
+
+@dataclass
+class ExpmDiagnostics:
+    degree: int = 0
+    squarings: int = 0
+
+
+@dataclass
+class ExpmvDiagnostics:
+    degree: int = 0
+    scaling: int = 0
+    applications: int = 0
+    early_exits: int = 0
+
+
+class Workspace:
+    """One CUDA stream plus the device buffers of one workspace
+    (src/Tensile/Workspace.cs). Operations on one workspace are serialised."""
+
+    def __init__(self, device: int = 0, max_elements: int | None = None):
+        self._lib = N.load()
+        h = C.c_void_p()
+        rc = self._lib.tns_create(int(device), int(max_elements or 0), C.byref(h))
+        if rc != N.TNS_OK:
+            _raise(rc, self._lib.tns_last_error(None).decode())
+        self._h = h
+
+    # -- plumbing -----------------------------------------------------------
+    def _call(self, name, *args):
+        if self._h is None:
+            raise ObjectDisposedError("The workspace has been disposed.")
+        rc = getattr(self._lib, name)(self._h, *args)
+        if rc != N.TNS_OK:
+            _raise(rc, self._lib.tns_last_error(self._h).decode())
+
+    def dispose(self):
+        if getattr(self, "_h", None) is not None:
+            self._lib.tns_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.dispose()
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_max_elements(self, value: int):
+        self._call("tns_set_max_elements", int(value))
+
+    # -- products -----------------------------------------------------------
+    def multiply(self, a, b, c=None, alpha=1.0, beta=0.0):
+        """C := beta*C + alpha*A*B (Workspace.Multiply). Returns C."""
+        cplx = any(np.iscomplexobj(x) for x in (a, b, c) if x is not None) or \
+            isinstance(alpha, complex) or isinstance(beta, complex)
+        a, b = _fortran(a, cplx), _fortran(b, cplx)
+        if a.ndim != 2 or b.ndim != 2:
+            raise ValueError("operands must be matrices")
+        m, k = a.shape
+        k2, n = b.shape
+        if k != k2:
+            raise ValueError(f"Inner dimensions disagree: A is {m}x{k}, B is {k2}x{n}.")
+        if c is None:
+            c = np.zeros((m, n), dtype=a.dtype, order="F")
+        else:
+            c = _fortran(c, cplx).copy(order="F")
+            if c.shape != (m, n):
+                raise ValueError(f"Destination is {c.shape[0]}x{c.shape[1]}, expected {m}x{n}.")
+        if cplx:
+            al = np.array([complex(alpha).real, complex(alpha).imag])
+            be = np.array([complex(beta).real, complex(beta).imag])
+            self._call("tns_zgemm", m, n, k, _p(al), _p(a), _ld(a), _p(b), _ld(b), _p(be), _p(c), _ld(c))
+        else:
+            self._call("tns_dgemm", m, n, k, float(alpha), _p(a), _ld(a), _p(b), _ld(b), float(beta),
+                       _p(c), _ld(c))
+        return c
+
+    # -- norms --------------------------------------------------------------
+    def _norm(self, a, kind: bytes) -> float:
+        cplx = np.iscomplexobj(a)
+        a = _fortran(a, cplx)
+        out = C.c_double()
+        self._call("tns_znorm" if cplx else "tns_dnorm", kind, a.shape[0], a.shape[1], _p(a), _ld(a),
+                   C.byref(out))
+        return out.value
+
+    def one_norm(self, a) -> float:
+        return self._norm(a, b"1")
+
+    def infinity_norm(self, a) -> float:
+        return self._norm(a, b"I")
+
+    def frobenius_norm(self, a) -> float:
+        return self._norm(a, b"F")
+
+    # -- LU -----------------------------------------------------------------
+    def factor_lu(self, a, block_size: int = 0) -> "LuDecomposition":
+        """P*A = L*U with partial pivoting (Workspace.FactorLu)."""
+        cplx = np.iscomplexobj(a)
+        f = _fortran(a, cplx).copy(order="F")
+        if f.ndim != 2:
+            raise ValueError("a matrix is required")
+        m, n = f.shape
+        piv = np.zeros(min(m, n), dtype=np.int32)
+        info = N.LuInfo()
+        self._call("tns_zgetrf" if cplx else "tns_dgetrf", m, n, _p(f), _ld(f), int(block_size), _p(piv),
+                   C.byref(info))
+        return LuDecomposition(self, f, piv, info)
+
+    # -- estimation ---------------------------------------------------------
+    def estimate_power_norm(self, a, power: int = 1, columns: int = DEFAULT_COLUMNS,
+                            max_iterations: int = DEFAULT_MAX_ITERATIONS,
+                            seed: int = DEFAULT_SEED) -> NormEstimateResult:
+        """NormEstimate.Of(new DenseMatrixOperator(a, power), ...): a lower
+        bound on ||A^power||_1 without forming the power."""
+        cplx = np.iscomplexobj(a)
+        a = _fortran(a, cplx)
+        if a.shape[0] != a.shape[1]:
+            raise ValueError(f"A linear operator must be square, got {a.shape[0]}x{a.shape[1]}.")
+        out = N.NormestResult()
+        self._call("tns_znormest1_power" if cplx else "tns_dnormest1_power", a.shape[0], _p(a), _ld(a),
+                   int(power), int(columns), int(max_iterations), int(seed), C.byref(out))
+        return NormEstimateResult(out.value, out.iterations, out.products)
+
+    # -- exponentials -------------------------------------------------------
+    def expm(self, a, diagnostics: ExpmDiagnostics | None = None):
+        """exp(A) (MatrixExponential.Expm)."""
+        cplx = np.iscomplexobj(a)
+        a = _fortran(a, cplx)
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise ValueError(f"The matrix exponential requires a square matrix, got {a.shape}.")
+        n = a.shape[0]
+        out = np.zeros((n, n), dtype=a.dtype, order="F")
+        info = N.ExpmInfo()
+        self._call("tns_zexpm" if cplx else "tns_dexpm", n, _p(a), _ld(a), _p(out), _ld(out), C.byref(info))
+        if diagnostics is not None:
+            diagnostics.degree, diagnostics.squarings = info.degree, info.squarings
+        return out
+
+    def expm_batched(self, mats, diagnostics: list | None = None):
+        """exp of every complex matrix in `mats` (the frequency-sweep form)."""
+        arrs = [_fortran(m, True) for m in mats]
+        for m in arrs:
+            if m.ndim != 2 or m.shape[0] != m.shape[1]:
+                raise ValueError("every matrix must be square")
+        outs = [np.zeros_like(m, order="F") for m in arrs]
+        cnt = len(arrs)
+        orders = (C.c_int * cnt)(*[m.shape[0] for m in arrs])
+        lds = (C.c_int * cnt)(*[_ld(m) for m in arrs])
+        ldo = (C.c_int * cnt)(*[_ld(m) for m in outs])
+        ap = (C.c_void_p * cnt)(*[m.ctypes.data for m in arrs])
+        op = (C.c_void_p * cnt)(*[m.ctypes.data for m in outs])
+        infos = (N.ExpmInfo * cnt)()
+        self._call("tns_zexpm_batched", cnt, orders, ap, lds, op, ldo, infos)
+        if diagnostics is not None:
+            diagnostics.clear()
+            diagnostics.extend(ExpmDiagnostics(i.degree, i.squarings) for i in infos)
+        return outs
+
+    def expmv(self, a, b, t: float = 1.0, diagnostics: ExpmvDiagnostics | None = None):
+        """exp(tA)B (MatrixExponentialAction.Expmv)."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+        a, b = _fortran(a, cplx), _fortran(b, cplx)
+        vec = b.ndim == 1
+        if vec:
+            b = b.reshape(-1, 1, order="F")
+        if a.shape[0] != a.shape[1]:
+            raise ValueError(f"The exponential action requires a square matrix, got {a.shape}.")
+        if b.shape[0] != a.shape[0]:
+            raise ValueError(f"B has {b.shape[0]} rows, expected the operator's order {a.shape[0]}.")
+        n, c = b.shape
+        out = np.zeros((n, c), dtype=a.dtype, order="F")
+        info = N.ExpmvInfo()
+        self._call("tns_zexpmv" if cplx else "tns_dexpmv", n, _p(a), _ld(a), c, _p(b), _ld(b), float(t),
+                   _p(out), _ld(out), C.byref(info))
+        if diagnostics is not None:
+            diagnostics.degree, diagnostics.scaling = info.degree, info.scaling
+            diagnostics.applications, diagnostics.early_exits = info.applications, info.early_exits
+        return out[:, 0] if vec else out
+
+
+class LuDecomposition:
+    """LuDecomposition<T> (src/Tensile/LuDecomposition.cs): packed factors,
+    0-based pivots, solves, determinant and reciprocal condition."""
+
+    def __init__(self, ws: Workspace, factors, pivots, info):
+        self._ws = ws
+        self.factors = factors
+        self.pivots = pivots
+        self.singular_column = info.singular_column
+        self.smallest_pivot = info.smallest_pivot
+        self.largest_pivot = info.largest_pivot
+        self.one_norm_of_a = info.one_norm
+
+    @property
+    def rows(self):
+        return self.factors.shape[0]
+
+    @property
+    def columns(self):
+        return self.factors.shape[1]
+
+    @property
+    def is_square(self):
+        return self.rows == self.columns
+
+    @property
+    def is_singular(self):
+        return self.singular_column >= 0
+
+    @property
+    def pivot_ratio(self):
+        return 0.0 if self.largest_pivot == 0.0 else self.smallest_pivot / self.largest_pivot
+
+    def _solve(self, b, adjoint: bool):
+        if not self.is_square:
+            raise SingularMatrixError("Solve requires a square factorization.")
+        cplx = np.iscomplexobj(self.factors)
+        x = _fortran(b, cplx).copy(order="F")
+        vec = x.ndim == 1
+        if vec:
+            x = x.reshape(-1, 1, order="F")
+        if x.shape[0] != self.rows:
+            raise ValueError(f"Right-hand side has {x.shape[0]} rows, expected {self.rows}.")
+        self._ws._call("tns_zgetrs" if cplx else "tns_dgetrs", self.rows, x.shape[1], _p(self.factors),
+                       _ld(self.factors), _p(self.pivots), int(self.singular_column), _p(x), _ld(x),
+                       int(adjoint))
+        return x[:, 0] if vec else x
+
+    def solve(self, b):
+        return self._solve(b, False)
+
+    def solve_adjoint(self, b):
+        return self._solve(b, True)
+
+    def determinant(self):
+        if not self.is_square:
+            raise SingularMatrixError("Determinant requires a square factorization.")
+        d = np.prod(np.diagonal(self.factors)) if self.rows else (1.0 + 0j if np.iscomplexobj(self.factors) else 1.0)
+        swaps = int(np.sum(self.pivots != np.arange(len(self.pivots))))
+        return -d if swaps % 2 else d
+
+    def reciprocal_condition(self) -> float:
+        """1/(||A||_1 * est ||A^-1||_1), 0 when singular (ReciprocalCondition)."""
+        cplx = np.iscomplexobj(self.factors)
+        out = C.c_double()
+        self._ws._call("tns_zgecon" if cplx else "tns_dgecon", self.rows, _p(self.factors), _ld(self.factors),
+                       _p(self.pivots), int(self.singular_column), float(self.one_norm_of_a), C.byref(out))
+        return out.value

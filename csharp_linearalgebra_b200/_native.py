@@ -1,0 +1,91 @@
+"""ctypes binding of libtensile_b200.so, the sm_100a CUDA library.
+
+This is the binding a caller of the C ABI (include/tensile_b200.h) writes; the
+C# one is in INTEGRATION.md. There is no fallback: if the library is missing or
+cannot load, importing the package's compute API raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtensile_b200.so")
+
+TNS_OK = 0
+TNS_E_ARGUMENT = 1
+TNS_E_SINGULAR = 2
+TNS_E_ALLOCATION_LIMIT = 3
+TNS_E_OUT_OF_MEMORY = 4
+TNS_E_DEVICE = 5
+TNS_E_TIMEOUT = 6
+TNS_E_DISPOSED = 7
+TNS_E_OUT_OF_RANGE = 8
+TNS_E_NULL = 9
+
+
+class LuInfo(C.Structure):
+    _fields_ = [("singular_column", C.c_int), ("smallest_pivot", C.c_double),
+                ("largest_pivot", C.c_double), ("one_norm", C.c_double)]
+
+
+class NormestResult(C.Structure):
+    _fields_ = [("value", C.c_double), ("iterations", C.c_int), ("products", C.c_int)]
+
+
+class ExpmInfo(C.Structure):
+    _fields_ = [("degree", C.c_int), ("squarings", C.c_int)]
+
+
+class ExpmvInfo(C.Structure):
+    _fields_ = [("degree", C.c_int), ("scaling", C.c_int), ("applications", C.c_int),
+                ("early_exits", C.c_int)]
+
+
+# name -> (restype, argtypes)
+_P, _I, _D, _LL, _CH = C.c_void_p, C.c_int, C.c_double, C.c_longlong, C.c_char
+SIGNATURES = {
+    "tns_create": (_I, [_I, _LL, C.POINTER(_P)]),
+    "tns_destroy": (_I, [_P]),
+    "tns_last_error": (C.c_char_p, [_P]),
+    "tns_set_max_elements": (_I, [_P, _LL]),
+    "tns_dgemm": (_I, [_P, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
+    "tns_dgemm_device": (_I, [_P, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
+    "tns_zgemm": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
+    "tns_zgemm_device": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
+    "tns_dnorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
+    "tns_znorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
+    "tns_dgetrf": (_I, [_P, _I, _I, _P, _I, _I, _P, C.POINTER(LuInfo)]),
+    "tns_zgetrf": (_I, [_P, _I, _I, _P, _I, _I, _P, C.POINTER(LuInfo)]),
+    "tns_dgetrs": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
+    "tns_zgetrs": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
+    "tns_dgecon": (_I, [_P, _I, _P, _I, _P, _I, _D, C.POINTER(_D)]),
+    "tns_zgecon": (_I, [_P, _I, _P, _I, _P, _I, _D, C.POINTER(_D)]),
+    "tns_dnormest1_power": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, C.POINTER(NormestResult)]),
+    "tns_znormest1_power": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, C.POINTER(NormestResult)]),
+    "tns_dexpm": (_I, [_P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_zexpm": (_I, [_P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_zexpm_batched": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "tns_zexpm_batched_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
+    "tns_dexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_zexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the native library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m csharp_linearalgebra_b200.build` "
+                "(nvcc, sm_100a). There is no CPU fallback.")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

@@ -1,0 +1,428 @@
+// The extern "C" boundary (include/tensile_b200.h). Validates arguments the way
+// the reference's KernelEntry / Workspace do, moves operands between the
+// caller's buffers and padded device matrices, runs the algorithm, and maps
+// internal errors to status codes. Nothing here computes.
+
+#include "tns_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <vector>
+
+struct tns_context {
+    tns::Context* impl;
+};
+
+namespace {
+
+using tns::Context;
+using tns::DMat;
+using tns::Error;
+using tns::fail;
+
+thread_local std::string g_error_no_ctx;
+
+void check_device_flag(Context& ctx) {
+    int h = 0;
+    TNS_CUDA(cudaMemcpyAsync(&h, ctx.d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    TNS_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (h != 0) {
+        TNS_CUDA(cudaMemsetAsync(ctx.d_err, 0, sizeof(int), ctx.stream));
+        TNS_CUDA(cudaStreamSynchronize(ctx.stream));
+        fail(TNS_E_TIMEOUT, "a device-side wait gave up (code " + std::to_string(h) + ")");
+    }
+}
+
+template <class F>
+int guarded(tns_context* c, F&& body) {
+    if (!c || !c->impl) {
+        g_error_no_ctx = "The context is null or has been destroyed.";
+        return TNS_E_DISPOSED;
+    }
+    Context& ctx = *c->impl;
+    try {
+        TNS_CUDA(cudaSetDevice(ctx.device));
+        body(ctx);
+        check_device_flag(ctx);
+        ctx.last_error.clear();
+        return TNS_OK;
+    } catch (const Error& e) {
+        ctx.last_error = e.what();
+        // Leave the stream idle so that the caller's buffers may be released.
+        cudaStreamSynchronize(ctx.stream);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx.last_error = "host allocation failed";
+        cudaStreamSynchronize(ctx.stream);
+        return TNS_E_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        ctx.last_error = e.what();
+        cudaStreamSynchronize(ctx.stream);
+        return TNS_E_DEVICE;
+    }
+}
+
+void require(bool cond, int code, const std::string& msg) {
+    if (!cond) fail(code, msg);
+}
+
+void check_operand(const void* p, int rows, int cols, int ld, const char* name) {
+    require(rows >= 0 && cols >= 0, TNS_E_ARGUMENT, std::string(name) + " has a negative dimension");
+    require(ld >= std::max(1, rows), TNS_E_ARGUMENT,
+            std::string(name) + ": leading dimension " + std::to_string(ld) + " is smaller than its " +
+                std::to_string(rows) + " rows");
+    require(p != nullptr || (long long)rows * cols == 0, TNS_E_NULL, std::string(name) + " is null");
+}
+
+DMat upload(Context& ctx, const double* src, int rows, int cols, int ld, bool cplx, bool on_device, const char* purpose) {
+    DMat m(ctx, rows, cols, cplx, purpose);
+    tns::copy_in(ctx, m, src, ld, on_device);
+    return m;
+}
+
+int gemm_entry(tns_context* c, bool cplx, bool dev, int m, int n, int k, const double* alpha, const double* a, int lda,
+               const double* b, int ldb, const double* beta, double* cm, int ldc) {
+    return guarded(c, [&](Context& ctx) {
+        require(alpha != nullptr && beta != nullptr, TNS_E_NULL, "alpha or beta is null");
+        check_operand(a, m, k, lda, "A");
+        check_operand(b, k, n, ldb, "B");
+        check_operand(cm, m, n, ldc, "C");
+        if (m == 0 || n == 0) return;
+        DMat A = upload(ctx, a, m, k, lda, cplx, dev, "the A operand");
+        DMat B = upload(ctx, b, k, n, ldb, cplx, dev, "the B operand");
+        bool need_c = !(beta[0] == 0.0 && beta[1] == 0.0);
+        DMat C = need_c ? upload(ctx, cm, m, n, ldc, cplx, dev, "the C operand") : DMat(ctx, m, n, cplx, "the C operand");
+        if (!cplx && alpha[0] == 0.0) {
+            // alpha == 0: C := beta*C only (Gemm.cs:125-127).
+            tns::scale_inplace(ctx, C.p, C.rows_p, C.cols_p, C.ld(), false, beta[0], 0.0);
+        } else {
+            tns::GemmProblem p = tns::make_gemm(A, B, C, alpha[0], alpha[1], beta[0], beta[1]);
+            tns::gemm(ctx, p, cplx);
+        }
+        tns::copy_out(ctx, C, cm, ldc, dev);
+        ctx.sync();
+    });
+}
+
+int norm_entry(tns_context* c, bool cplx, char kind, int m, int n, const double* a, int lda, double* out) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, m, n, lda, "A");
+        require(out != nullptr, TNS_E_NULL, "out is null");
+        require(kind == '1' || kind == 'I' || kind == 'i' || kind == 'F' || kind == 'f', TNS_E_ARGUMENT,
+                "norm kind must be '1', 'I' or 'F'");
+        if (m == 0 || n == 0) {
+            *out = 0.0;
+            return;
+        }
+        DMat A = upload(ctx, a, m, n, lda, cplx, false, "a norm operand");
+        if (kind == '1') *out = tns::norm1(ctx, A);
+        else if (kind == 'I' || kind == 'i') *out = tns::norminf(ctx, A);
+        else *out = tns::normfro(ctx, A);
+    });
+}
+
+int getrf_entry(tns_context* c, bool cplx, int m, int n, double* a, int lda, int nb, int* pivots, tns_lu_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, m, n, lda, "A");
+        int limit = std::min(m, n);
+        require(pivots != nullptr || limit == 0, TNS_E_NULL, "pivots is null");
+        tns_lu_info local{};
+        tns_lu_info* out = info ? info : &local;
+        *out = tns_lu_info{-1, 0.0, 0.0, 0.0};
+        if (limit == 0) return;
+        DMat A = upload(ctx, a, m, n, lda, cplx, false, "the matrix to factor");
+        // ||A||_1 before factoring (Workspace.cs:214).
+        double one = tns::norm1(ctx, A);
+        tns::DBuf piv(ctx, sizeof(int) * (size_t)limit);
+        tns::LuResult r = tns::getrf(ctx, A, m, n, nb, piv.as<int>());
+        std::vector<int> hp(limit);
+        TNS_CUDA(cudaMemcpyAsync(hp.data(), piv.p, sizeof(int) * limit, cudaMemcpyDeviceToHost, ctx.stream));
+        tns::copy_out(ctx, A, a, lda, false);
+        ctx.sync();
+        std::memcpy(pivots, hp.data(), sizeof(int) * limit);
+        out->singular_column = r.singular_column;
+        out->smallest_pivot = r.smallest_pivot;
+        out->largest_pivot = r.largest_pivot;
+        out->one_norm = one;
+    });
+}
+
+int getrs_entry(tns_context* c, bool cplx, int n, int nrhs, const double* lu, int lda, const int* pivots,
+                int singular_column, double* b, int ldb, int adjoint) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(lu, n, n, lda, "the factors");
+        check_operand(b, n, nrhs, ldb, "B");
+        require(pivots != nullptr || n == 0, TNS_E_NULL, "pivots is null");
+        if (singular_column >= 0)
+            fail(TNS_E_SINGULAR, "Matrix is singular: zero pivot at column " + std::to_string(singular_column) + ".");
+        if (n == 0 || nrhs == 0) return;
+        for (int k = 0; k < n; ++k)
+            require(pivots[k] >= k && pivots[k] < n, TNS_E_ARGUMENT, "pivot entry out of range");
+        DMat F = upload(ctx, lu, n, n, lda, cplx, false, "the factors");
+        DMat B = upload(ctx, b, n, nrhs, ldb, cplx, false, "the right-hand sides");
+        tns::DBuf piv(ctx, sizeof(int) * (size_t)n);
+        TNS_CUDA(cudaMemcpyAsync(piv.p, pivots, sizeof(int) * n, cudaMemcpyHostToDevice, ctx.stream));
+        tns::getrs(ctx, F, piv.as<int>(), B, nrhs, adjoint != 0);
+        tns::copy_out(ctx, B, b, ldb, false);
+        ctx.sync();
+    });
+}
+
+int gecon_entry(tns_context* c, bool cplx, int n, const double* lu, int lda, const int* pivots, int singular_column,
+                double anorm, double* rcond) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(lu, n, n, lda, "the factors");
+        require(rcond != nullptr, TNS_E_NULL, "rcond is null");
+        if (singular_column >= 0 || anorm == 0.0 || n == 0) {
+            *rcond = 0.0;
+            return;
+        }
+        require(pivots != nullptr, TNS_E_NULL, "pivots is null");
+        for (int k = 0; k < n; ++k)
+            require(pivots[k] >= k && pivots[k] < n, TNS_E_ARGUMENT, "pivot entry out of range");
+        DMat F = upload(ctx, lu, n, n, lda, cplx, false, "the factors");
+        tns::DBuf piv(ctx, sizeof(int) * (size_t)n);
+        TNS_CUDA(cudaMemcpyAsync(piv.p, pivots, sizeof(int) * n, cudaMemcpyHostToDevice, ctx.stream));
+        tns::NormestResult r = tns::normest_lu_inverse(ctx, F, piv.as<int>(), 2, 5, 20260915);
+        *rcond = r.value == 0.0 ? 0.0 : 1.0 / (anorm * r.value);
+    });
+}
+
+int normest_entry(tns_context* c, bool cplx, int n, const double* a, int lda, int power, int t, int itmax, int seed,
+                  tns_normest_result* out) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        require(out != nullptr, TNS_E_NULL, "out is null");
+        require(power >= 1, TNS_E_OUT_OF_RANGE, "power must be at least 1");
+        *out = tns_normest_result{0.0, 0, 0};
+        if (n == 0) return;
+        require((long long)n * std::clamp(t, 1, n) <= 2147483647LL, TNS_E_OUT_OF_RANGE, "probe panel too large");
+        ctx.check_limit((long long)n * std::clamp(t, 1, n), "an estimator probe panel");
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the operator");
+        tns::NormestResult r = tns::normest_power(ctx, A, power, t, itmax, seed);
+        out->value = r.value;
+        out->iterations = r.iterations;
+        out->products = r.products;
+    });
+}
+
+// exp of a 1 x 1 matrix: the scalar exponential (MatrixExponential.cs:158-175).
+void scalar_exp(const double* a, double* out, bool cplx) {
+    if (!cplx) {
+        out[0] = std::exp(a[0]);
+    } else {
+        double e = std::exp(a[0]);
+        out[0] = e * std::cos(a[1]);
+        out[1] = e * std::sin(a[1]);
+    }
+}
+
+int expm_entry(tns_context* c, bool cplx, int n, const double* a, int lda, double* out, int ldo, tns_expm_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(out, n, n, ldo, "the result");
+        tns_expm_info local{};
+        tns_expm_info* inf = info ? info : &local;
+        *inf = tns_expm_info{0, 0};
+        if (n == 0) return;
+        if (n == 1) {
+            scalar_exp(a, out, cplx);
+            return;
+        }
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the matrix to exponentiate");
+        DMat R;
+        tns::ExpmInfo ei;
+        tns::expm(ctx, A, R, &ei);
+        tns::copy_out(ctx, R, out, ldo, false);
+        ctx.sync();
+        inf->degree = ei.degree;
+        inf->squarings = ei.squarings;
+    });
+}
+
+int expmv_entry(tns_context* c, bool cplx, int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
+                double* out, int ldo, tns_expmv_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(b, n, ncols, ldb, "B");
+        check_operand(out, n, ncols, ldo, "the result");
+        tns_expmv_info local{};
+        tns_expmv_info* inf = info ? info : &local;
+        *inf = tns_expmv_info{0, 0, 0, 0};
+        if (n == 0 || ncols == 0) return;
+        require(std::isfinite(t), TNS_E_OUT_OF_RANGE, "t must be finite");
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the operator");
+        DMat B = upload(ctx, b, n, ncols, ldb, cplx, false, "the panel");
+        DMat R;
+        tns::ExpmvInfo ei;
+        tns::expmv(ctx, A, B, t, R, &ei);
+        tns::copy_out(ctx, R, out, ldo, false);
+        ctx.sync();
+        inf->degree = ei.degree;
+        inf->scaling = ei.scaling;
+        inf->applications = ei.applications;
+        inf->early_exits = ei.early_exits;
+    });
+}
+
+int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
+                        double* const* out, const int* ldo, tns_expm_info* infos) {
+    return guarded(c, [&](Context& ctx) {
+        require(count >= 0, TNS_E_ARGUMENT, "negative batch size");
+        if (count == 0) return;
+        require(orders && a && lda && out && ldo, TNS_E_NULL, "a batch array is null");
+        for (int i = 0; i < count; ++i) {
+            check_operand(a[i], orders[i], orders[i], lda[i], "A[i]");
+            check_operand(out[i], orders[i], orders[i], ldo[i], "out[i]");
+        }
+        for (int i = 0; i < count; ++i) {
+            int n = orders[i];
+            tns_expm_info inf{0, 0};
+            if (n == 1) {
+                if (dev) {
+                    double h[2], r[2];
+                    TNS_CUDA(cudaMemcpy(h, a[i], 16, cudaMemcpyDeviceToHost));
+                    scalar_exp(h, r, true);
+                    TNS_CUDA(cudaMemcpy(out[i], r, 16, cudaMemcpyHostToDevice));
+                } else {
+                    scalar_exp(a[i], out[i], true);
+                }
+            } else if (n > 1) {
+                DMat A = upload(ctx, a[i], n, n, lda[i], true, dev, "a matrix to exponentiate");
+                DMat R;
+                tns::ExpmInfo ei;
+                tns::expm(ctx, A, R, &ei);
+                tns::copy_out(ctx, R, out[i], ldo[i], dev);
+                inf.degree = ei.degree;
+                inf.squarings = ei.squarings;
+            }
+            if (infos) infos[i] = inf;
+        }
+        ctx.sync();
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+int tns_create(int device, long long max_elements, tns_context** out) {
+    if (!out) return TNS_E_NULL;
+    *out = nullptr;
+    try {
+        auto* c = new tns_context{new Context(device)};
+        if (max_elements > 0) c->impl->max_elements = std::min(max_elements, 2147483591LL);
+        *out = c;
+        return TNS_OK;
+    } catch (const Error& e) {
+        g_error_no_ctx = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_error_no_ctx = e.what();
+        return TNS_E_DEVICE;
+    }
+}
+
+int tns_destroy(tns_context* ctx) {
+    if (!ctx) return TNS_E_DISPOSED;
+    delete ctx->impl;
+    ctx->impl = nullptr;
+    delete ctx;
+    return TNS_OK;
+}
+
+const char* tns_last_error(const tns_context* ctx) {
+    if (!ctx || !ctx->impl) return g_error_no_ctx.c_str();
+    return ctx->impl->last_error.c_str();
+}
+
+int tns_set_max_elements(tns_context* ctx, long long max_elements) {
+    return guarded(ctx, [&](Context& c) {
+        require(max_elements > 0 && max_elements <= 2147483591LL, TNS_E_OUT_OF_RANGE,
+                "MaxElements must be positive and at most Array.MaxLength");
+        c.max_elements = max_elements;
+    });
+}
+
+int tns_dgemm(tns_context* c, int m, int n, int k, double alpha, const double* a, int lda, const double* b, int ldb,
+              double beta, double* cm, int ldc) {
+    double al[2] = {alpha, 0.0}, be[2] = {beta, 0.0};
+    return gemm_entry(c, false, false, m, n, k, al, a, lda, b, ldb, be, cm, ldc);
+}
+int tns_dgemm_device(tns_context* c, int m, int n, int k, double alpha, const double* a, int lda, const double* b,
+                     int ldb, double beta, double* cm, int ldc) {
+    double al[2] = {alpha, 0.0}, be[2] = {beta, 0.0};
+    return gemm_entry(c, false, true, m, n, k, al, a, lda, b, ldb, be, cm, ldc);
+}
+int tns_zgemm(tns_context* c, int m, int n, int k, const double* alpha, const double* a, int lda, const double* b,
+              int ldb, const double* beta, double* cm, int ldc) {
+    return gemm_entry(c, true, false, m, n, k, alpha, a, lda, b, ldb, beta, cm, ldc);
+}
+int tns_zgemm_device(tns_context* c, int m, int n, int k, const double* alpha, const double* a, int lda,
+                     const double* b, int ldb, const double* beta, double* cm, int ldc) {
+    return gemm_entry(c, true, true, m, n, k, alpha, a, lda, b, ldb, beta, cm, ldc);
+}
+
+int tns_dnorm(tns_context* c, char kind, int m, int n, const double* a, int lda, double* out) {
+    return norm_entry(c, false, kind, m, n, a, lda, out);
+}
+int tns_znorm(tns_context* c, char kind, int m, int n, const double* a, int lda, double* out) {
+    return norm_entry(c, true, kind, m, n, a, lda, out);
+}
+
+int tns_dgetrf(tns_context* c, int m, int n, double* a, int lda, int nb, int* pivots, tns_lu_info* info) {
+    return getrf_entry(c, false, m, n, a, lda, nb, pivots, info);
+}
+int tns_zgetrf(tns_context* c, int m, int n, double* a, int lda, int nb, int* pivots, tns_lu_info* info) {
+    return getrf_entry(c, true, m, n, a, lda, nb, pivots, info);
+}
+int tns_dgetrs(tns_context* c, int n, int nrhs, const double* lu, int lda, const int* pivots, int singular_column,
+               double* b, int ldb, int adjoint) {
+    return getrs_entry(c, false, n, nrhs, lu, lda, pivots, singular_column, b, ldb, adjoint);
+}
+int tns_zgetrs(tns_context* c, int n, int nrhs, const double* lu, int lda, const int* pivots, int singular_column,
+               double* b, int ldb, int adjoint) {
+    return getrs_entry(c, true, n, nrhs, lu, lda, pivots, singular_column, b, ldb, adjoint);
+}
+int tns_dgecon(tns_context* c, int n, const double* lu, int lda, const int* pivots, int singular_column, double anorm,
+               double* rcond) {
+    return gecon_entry(c, false, n, lu, lda, pivots, singular_column, anorm, rcond);
+}
+int tns_zgecon(tns_context* c, int n, const double* lu, int lda, const int* pivots, int singular_column, double anorm,
+               double* rcond) {
+    return gecon_entry(c, true, n, lu, lda, pivots, singular_column, anorm, rcond);
+}
+int tns_dnormest1_power(tns_context* c, int n, const double* a, int lda, int power, int t, int itmax, int seed,
+                        tns_normest_result* out) {
+    return normest_entry(c, false, n, a, lda, power, t, itmax, seed, out);
+}
+int tns_znormest1_power(tns_context* c, int n, const double* a, int lda, int power, int t, int itmax, int seed,
+                        tns_normest_result* out) {
+    return normest_entry(c, true, n, a, lda, power, t, itmax, seed, out);
+}
+int tns_dexpm(tns_context* c, int n, const double* a, int lda, double* out, int ldo, tns_expm_info* info) {
+    return expm_entry(c, false, n, a, lda, out, ldo, info);
+}
+int tns_zexpm(tns_context* c, int n, const double* a, int lda, double* out, int ldo, tns_expm_info* info) {
+    return expm_entry(c, true, n, a, lda, out, ldo, info);
+}
+int tns_zexpm_batched(tns_context* c, int count, const int* orders, const double* const* a, const int* lda,
+                      double* const* out, const int* ldo, tns_expm_info* infos) {
+    return zexpm_batched_entry(c, false, count, orders, a, lda, out, ldo, infos);
+}
+int tns_zexpm_batched_device(tns_context* c, int count, const int* orders, const double* const* a, const int* lda,
+                             double* const* out, const int* ldo, tns_expm_info* infos) {
+    return zexpm_batched_entry(c, true, count, orders, a, lda, out, ldo, infos);
+}
+int tns_dexpmv(tns_context* c, int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
+               double* out, int ldo, tns_expmv_info* info) {
+    return expmv_entry(c, false, n, a, lda, ncols, b, ldb, t, out, ldo, info);
+}
+int tns_zexpmv(tns_context* c, int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
+               double* out, int ldo, tns_expmv_info* info) {
+    return expmv_entry(c, true, n, a, lda, ncols, b, ldb, t, out, ldo, info);
+}
+
+}  // extern "C"

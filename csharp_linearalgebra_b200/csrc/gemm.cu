@@ -1,0 +1,380 @@
+// FP64 GEMM on the B200 tensor cores (DMMA), real and complex (fused 4M).
+//
+// Replaces the reference's BLIS-style CPU GEMM (src/Tensile.Kernels/Gemm.cs:117-203,
+// ParallelGemm.cs:138-229, MicroKernels.cs:57-273) and its 4M complex product
+// (src/Tensile/ComplexKernels.cs:49-108). C := beta*C + alpha*A*B, column-major.
+//
+// Design
+//  - tcgen05 has no f64 kind, so the math is warp-level mma.sync m16n8k4 f64.
+//  - Operand tiles are staged in shared memory by the TMA engine's bulk copies
+//    (cp.async.bulk, one per tile column) completing on mbarriers; a producer
+//    warp runs STAGES tiles ahead of the consumer (math) warps. Each smem
+//    column is padded so that the DMMA fragment loads are bank-conflict free
+//    (real: A stride = 4 mod 16 doubles, B stride 20; complex: A stride
+//    = 2 mod 8 complex, B stride 20).
+//  - The MMA computes C^T = B^T A^T, so a thread's accumulator pair covers two
+//    consecutive rows of column-major C and the epilogue stores 16-byte pairs.
+//  - Complex (interleaved re,im) runs the 4M product inside one kernel: four
+//    real MMAs per fragment pair, Re += Br*Ar - Bi*Ai, Im += Br*Ai + Bi*Ar, so
+//    no split, combine or extra pass over memory.
+//  - Persistent CTAs walk a list of problems (grouped GEMM): the same kernel
+//    serves one product, or every matrix of a batch in one launch.
+//  - Every wait is bounded (device_util.cuh): a stuck pipeline records an error
+//    in the context flag and the kernel returns.
+//
+// Operand requirements (checked on the host before every launch): pointers and
+// leading dimensions 16-byte aligned, M and N even, K a multiple of 16. The
+// library's device matrices are zero-padded to multiples of 64, which meets
+// all of them.
+
+#include "device_util.cuh"
+#include "tns_internal.h"
+
+#include <algorithm>
+#include <vector>
+
+namespace tns {
+
+template <bool CPLX, int WARPS_M, int WARPS_N, int STAGES_>
+struct GemmCfg {
+    static constexpr bool kComplex = CPLX;
+    static constexpr int ESZ = CPLX ? 16 : 8;  // bytes per element
+    static constexpr int WM = 32;              // C rows per warp = 4 mma-N fragments of 8
+    static constexpr int WN = CPLX ? 32 : 64;  // C columns per warp, mma-M fragments of 16
+    static constexpr int MF = WM / 8;
+    static constexpr int NF = WN / 16;
+    static constexpr int BM = WARPS_M * WM;
+    static constexpr int BN = WARPS_N * WN;
+    static constexpr int BK = 16;
+    static constexpr int STAGES = STAGES_;
+    static constexpr int LDA_S = BM + (CPLX ? 2 : 4);  // smem A column stride, elements
+    static constexpr int LDB_S = BK + 4;               // smem B column stride, elements
+    static constexpr int A_STAGE = BK * LDA_S;         // elements
+    static constexpr int B_STAGE = BN * LDB_S;
+    static constexpr int STAGE_BYTES = (A_STAGE + B_STAGE) * ESZ;
+    static constexpr int CONSUMERS = WARPS_M * WARPS_N;
+    static constexpr int THREADS = (CONSUMERS + 1) * 32;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
+    static_assert((LDA_S * ESZ) % 16 == 0 && (LDB_S * ESZ) % 16 == 0, "smem columns must stay 16B aligned");
+    static_assert(SMEM <= 227 * 1024, "shared memory budget");
+};
+
+__device__ __forceinline__ int find_problem(const GemmProblem* probs, int nprob, int tile) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].tile_begin <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Problems of one launch: up to four travel in the parameter block, a longer
+// list lives in device memory.
+struct GemmLaunch {
+    GemmProblem inl[4];
+    const GemmProblem* list;
+    int nprob;
+    int total_tiles;
+    int* err;
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid_constant__ GemmLaunch L) {
+    const GemmProblem* probs = L.list ? L.list : L.inl;
+    const int nprob = L.nprob;
+    const int total_tiles = L.total_tiles;
+    int* err = L.err;
+    using E = typename std::conditional<Cfg::kComplex, double2, double>::type;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
+    uint64_t* empty = full + Cfg::STAGES;
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < Cfg::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], Cfg::CONSUMERS);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    auto stage_a = [&](int s) { return reinterpret_cast<E*>(smem + s * Cfg::STAGE_BYTES); };
+    auto stage_b = [&](int s) {
+        return reinterpret_cast<E*>(smem + s * Cfg::STAGE_BYTES + Cfg::A_STAGE * Cfg::ESZ);
+    };
+
+    if (warp == Cfg::CONSUMERS) {
+        // ------------------------------ producer ------------------------------
+        uint32_t it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+            const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
+            int local = tile - P.tile_begin;
+            int m0 = (local % P.tiles_m) * Cfg::BM;
+            int n0 = (local / P.tiles_m) * Cfg::BN;
+            int rows = min(Cfg::BM, P.M - m0);
+            int cols = min(Cfg::BN, P.N - n0);
+            uint32_t bytes = (uint32_t)(Cfg::BK * rows + cols * Cfg::BK) * Cfg::ESZ;
+            const E* A = reinterpret_cast<const E*>(P.A);
+            const E* B = reinterpret_cast<const E*>(P.B);
+            for (int k0 = 0; k0 < P.K; k0 += Cfg::BK, ++it) {
+                int s = it % Cfg::STAGES;
+                uint32_t round = it / Cfg::STAGES;
+                if (!mbar_wait_bounded(&empty[s], (round & 1) ^ 1, err, kDevTimeoutEmpty)) {
+                    ok = false;
+                    break;
+                }
+                if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes);
+                __syncwarp();
+                E* As = stage_a(s);
+                E* Bs = stage_b(s);
+                for (int c = lane; c < Cfg::BK + cols; c += 32) {
+                    if (c < Cfg::BK) {
+                        bulk_copy_g2s(As + c * Cfg::LDA_S, A + (size_t)(k0 + c) * P.lda + m0,
+                                      (uint32_t)rows * Cfg::ESZ, &full[s]);
+                    } else {
+                        int nn = c - Cfg::BK;
+                        bulk_copy_g2s(Bs + nn * Cfg::LDB_S, B + (size_t)(n0 + nn) * P.ldb + k0,
+                                      (uint32_t)Cfg::BK * Cfg::ESZ, &full[s]);
+                    }
+                }
+            }
+        }
+        // Drain: do not leave while copies into this CTA's shared memory are in
+        // flight. The consumers release every stage they read, so waiting for
+        // the last STAGES releases covers every copy issued.
+        if (ok) {
+            for (int r = 0; r < Cfg::STAGES && (uint32_t)r < it; ++r) {
+                uint32_t j = it - 1 - r;
+                int s = j % Cfg::STAGES;
+                if (!mbar_wait_bounded(&empty[s], (j / Cfg::STAGES) & 1, err, kDevTimeoutDrain)) break;
+            }
+        }
+        return;
+    }
+
+    // ------------------------------- consumers -------------------------------
+    const int wm = warp % (Cfg::BM / Cfg::WM);
+    const int wn = warp / (Cfg::BM / Cfg::WM);
+    const int g = lane >> 2;
+    const int t = lane & 3;
+    uint32_t it = 0;
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
+        int local = tile - P.tile_begin;
+        int m0 = (local % P.tiles_m) * Cfg::BM;
+        int n0 = (local / P.tiles_m) * Cfg::BN;
+
+        double acc_re[Cfg::NF][Cfg::MF][4];
+        double acc_im[Cfg::kComplex ? Cfg::NF : 1][Cfg::kComplex ? Cfg::MF : 1][4];
+#pragma unroll
+        for (int i = 0; i < Cfg::NF; ++i)
+#pragma unroll
+            for (int j = 0; j < Cfg::MF; ++j)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    acc_re[i][j][r] = 0.0;
+                    if constexpr (Cfg::kComplex) acc_im[i][j][r] = 0.0;
+                }
+
+        for (int k0 = 0; k0 < P.K; k0 += Cfg::BK, ++it) {
+            int s = it % Cfg::STAGES;
+            if (!mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
+            const E* As = stage_a(s) + wm * Cfg::WM + g;
+            const E* Bs = stage_b(s) + (wn * Cfg::WN + g) * Cfg::LDB_S + t;
+#pragma unroll
+            for (int ks = 0; ks < Cfg::BK; ks += 4) {
+                E fa0[Cfg::NF], fa1[Cfg::NF], fb[Cfg::MF];
+#pragma unroll
+                for (int i = 0; i < Cfg::NF; ++i) {
+                    fa0[i] = Bs[(i * 16) * Cfg::LDB_S + ks];
+                    fa1[i] = Bs[(i * 16 + 8) * Cfg::LDB_S + ks];
+                }
+#pragma unroll
+                for (int j = 0; j < Cfg::MF; ++j) fb[j] = As[(ks + t) * Cfg::LDA_S + j * 8];
+#pragma unroll
+                for (int i = 0; i < Cfg::NF; ++i)
+#pragma unroll
+                    for (int j = 0; j < Cfg::MF; ++j) {
+                        if constexpr (Cfg::kComplex) {
+                            dmma_16x8x4(acc_re[i][j], fa0[i].x, fa1[i].x, fb[j].x);
+                            dmma_16x8x4(acc_re[i][j], -fa0[i].y, -fa1[i].y, fb[j].y);
+                            dmma_16x8x4(acc_im[i][j], fa0[i].x, fa1[i].x, fb[j].y);
+                            dmma_16x8x4(acc_im[i][j], fa0[i].y, fa1[i].y, fb[j].x);
+                        } else {
+                            dmma_16x8x4(acc_re[i][j], fa0[i], fa1[i], fb[j]);
+                        }
+                    }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+
+        // Epilogue: C := beta*C + alpha*acc with the reference's special cases.
+        E* C = reinterpret_cast<E*>(P.C);
+        const double ar = P.alpha_re, ai = P.alpha_im, br = P.beta_re, bi = P.beta_im;
+#pragma unroll
+        for (int i = 0; i < Cfg::NF; ++i)
+#pragma unroll
+            for (int j = 0; j < Cfg::MF; ++j) {
+                int m = m0 + wm * Cfg::WM + j * 8 + 2 * t;
+                if (m >= P.M) continue;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    int n = n0 + wn * Cfg::WN + i * 16 + g + 8 * h;
+                    if (n >= P.N) continue;
+                    E* dst = C + (size_t)n * P.ldc + m;
+                    if constexpr (!Cfg::kComplex) {
+                        double2 cur = make_double2(0.0, 0.0);
+                        if (br != 0.0) {
+                            cur = *reinterpret_cast<const double2*>(dst);
+                            if (br != 1.0) cur = make_double2(mul_rn(cur.x, br), mul_rn(cur.y, br));
+                        }
+                        double2 out;
+                        out.x = fma(ar, acc_re[i][j][2 * h], cur.x);
+                        out.y = fma(ar, acc_re[i][j][2 * h + 1], cur.y);
+                        *reinterpret_cast<double2*>(dst) = out;
+                    } else {
+                        bool unit_alpha = (ar == 1.0 && ai == 0.0);
+                        bool real_alpha = (ai == 0.0);
+                        bool zero_beta = (br == 0.0 && bi == 0.0);
+                        bool unit_beta = (br == 1.0 && bi == 0.0);
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            double p = acc_re[i][j][2 * h + q];
+                            double qq = acc_im[i][j][2 * h + q];
+                            double pr, pi;
+                            if (unit_alpha) {
+                                pr = p;
+                                pi = qq;
+                            } else if (real_alpha) {
+                                pr = mul_rn(ar, p);
+                                pi = mul_rn(ar, qq);
+                            } else {
+                                pr = sub_rn(mul_rn(ar, p), mul_rn(ai, qq));
+                                pi = add_rn(mul_rn(ai, p), mul_rn(ar, qq));
+                            }
+                            double2 o;
+                            if (zero_beta) {
+                                o = make_double2(pr, pi);
+                            } else {
+                                double2 c = dst[q];
+                                if (unit_beta) {
+                                    o = make_double2(add_rn(c.x, pr), add_rn(c.y, pi));
+                                } else {
+                                    double cr = sub_rn(mul_rn(br, c.x), mul_rn(bi, c.y));
+                                    double ci = add_rn(mul_rn(bi, c.x), mul_rn(br, c.y));
+                                    o = make_double2(add_rn(cr, pr), add_rn(ci, pi));
+                                }
+                            }
+                            dst[q] = o;
+                        }
+                    }
+                }
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+namespace {
+
+using RealBig = GemmCfg<false, 4, 2, 4>;     // 128 x 128 tiles, 8 math warps
+using RealSmall = GemmCfg<false, 2, 1, 4>;   // 64 x 64 tiles, 2 math warps
+using CplxBig = GemmCfg<true, 4, 2, 3>;      // 128 x 64 tiles, 8 math warps
+using CplxSmall = GemmCfg<true, 2, 2, 4>;    // 64 x 64 tiles, 4 math warps
+
+template <class Cfg>
+void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
+    static bool configured[64] = {false};
+    int dev = ctx.device;
+    if (!configured[dev]) {
+        TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+        configured[dev] = true;
+    }
+    int total = 0;
+    for (auto& p : probs) {
+        p.tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM;
+        p.tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
+        p.tile_begin = total;
+        total += p.tiles_m * p.tiles_n;
+    }
+    if (total == 0) return;
+    GemmLaunch L{};
+    L.nprob = (int)probs.size();
+    L.total_tiles = total;
+    L.err = ctx.d_err;
+    if (probs.size() <= 4) {
+        for (size_t i = 0; i < probs.size(); ++i) L.inl[i] = probs[i];
+        L.list = nullptr;
+    } else {
+        L.list = ctx.upload_problems(probs);
+    }
+    int ctas_per_sm = 1;
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
+    int grid = std::min(total, std::max(1, ctas_per_sm) * ctx.num_sms);
+    gemm_dmma_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, ctx.stream>>>(L);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
+
+void check_problem(const GemmProblem& p, bool cplx) {
+    int esz = cplx ? 16 : 8;
+    auto aligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    bool ok = p.M >= 0 && p.N >= 0 && p.K >= 0 && (p.M % 2 == 0) && (p.N % 2 == 0) && (p.K % 16 == 0) &&
+              aligned(p.A) && aligned(p.B) && aligned(p.C) && ((size_t)p.lda * esz) % 16 == 0 &&
+              ((size_t)p.ldb * esz) % 16 == 0 && ((size_t)p.ldc * esz) % 16 == 0 && p.lda >= p.M &&
+              p.ldb >= p.K && p.ldc >= p.M;
+    if (!ok) fail(TNS_E_ARGUMENT, "internal GEMM operand violates the bulk-copy layout contract");
+}
+
+}  // namespace
+
+void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
+    std::vector<GemmProblem> work;
+    work.reserve(probs.size());
+    long long flops_big = 0;
+    for (auto& p : probs) {
+        check_problem(p, cplx);
+        if (p.M == 0 || p.N == 0) continue;
+        if (p.K == 0) {
+            // No product: C := beta*C (+ 0). Handled by the scale kernel.
+            scale_inplace(ctx, p.C, p.M, p.N, p.ldc, cplx, p.beta_re, p.beta_im);
+            continue;
+        }
+        work.push_back(p);
+        flops_big += (long long)p.M * p.N * p.K;
+    }
+    if (work.empty()) return;
+    // Big tiles only when they fill the machine.
+    bool big = true;
+    if (cplx) {
+        long long tiles = 0;
+        for (auto& p : work) tiles += (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN);
+        big = tiles >= ctx.num_sms;
+        if (big) launch_cfg<CplxBig>(ctx, work);
+        else launch_cfg<CplxSmall>(ctx, work);
+    } else {
+        long long tiles = 0;
+        for (auto& p : work) tiles += (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
+        big = tiles >= ctx.num_sms;
+        if (big) launch_cfg<RealBig>(ctx, work);
+        else launch_cfg<RealSmall>(ctx, work);
+    }
+    (void)flops_big;
+}
+
+void gemm(Context& ctx, const GemmProblem& p, bool cplx) {
+    std::vector<GemmProblem> v{p};
+    gemm_grouped(ctx, v, cplx);
+}
+
+}  // namespace tns

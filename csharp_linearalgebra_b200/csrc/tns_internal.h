@@ -1,0 +1,177 @@
+// Internal host-side interfaces of the tensile_b200 library: the context
+// (one CUDA stream per workspace), error handling, padded device matrices and
+// the launchers of the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tensile_b200.h"
+
+namespace tns {
+
+// Thrown inside the library, caught at the C ABI and mapped to a status code.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+[[noreturn]] void fail_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define TNS_CUDA(x)                                                  \
+    do {                                                             \
+        cudaError_t e_ = (x);                                        \
+        if (e_ != cudaSuccess) ::tns::fail_cuda(e_, #x, __FILE__, __LINE__); \
+    } while (0)
+
+// Device matrices are zero-padded to multiples of this many rows and columns,
+// which makes every GEMM operand meet the bulk-copy alignment rules and lets
+// the LU and solves work on whole 64-wide blocks.
+constexpr int kPad = 64;
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// One problem of a (grouped) GEMM: C := beta*C + alpha*A*B. lda/ldb/ldc are in
+// elements (complex elements for complex problems).
+struct GemmProblem {
+    const void* A;
+    const void* B;
+    void* C;
+    int lda, ldb, ldc;
+    int M, N, K;
+    int tiles_m, tiles_n, tile_begin;
+    double alpha_re, alpha_im, beta_re, beta_im;
+};
+
+struct Context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    int* d_err = nullptr;           // device-side error flag (bounded waits)
+    long long max_elements = 2147483591LL;
+    std::string last_error;
+    long long kernel_launches = 0;  // kernels launched through this context
+    GemmProblem* d_probs = nullptr;
+    size_t d_probs_cap = 0;
+
+    explicit Context(int dev);
+    ~Context();
+    GemmProblem* upload_problems(const std::vector<GemmProblem>& probs);
+    void sync();                       // stream sync + device error flag check
+    void check_limit(long long elements, const char* purpose) const;
+};
+
+// A padded device matrix owned by the library: rows_p x cols_p with
+// ld = rows_p, zero outside rows x cols. Freed on the context's stream.
+struct DMat {
+    Context* ctx = nullptr;
+    double* p = nullptr;
+    int rows = 0, cols = 0, rows_p = 0, cols_p = 0;
+    bool cplx = false;
+
+    DMat() = default;
+    DMat(Context& c, int r, int k, bool complex_, const char* purpose = "a device matrix");
+    DMat(const DMat&) = delete;
+    DMat& operator=(const DMat&) = delete;
+    DMat(DMat&& o) noexcept { *this = std::move(o); }
+    DMat& operator=(DMat&& o) noexcept;
+    ~DMat();
+    int ld() const { return rows_p; }
+    int esz() const { return cplx ? 16 : 8; }
+    size_t bytes() const { return (size_t)rows_p * cols_p * esz(); }
+    double* col(int j) { return p + (size_t)j * rows_p * (cplx ? 2 : 1); }
+    double* at(int i, int j) { return p + ((size_t)j * rows_p + i) * (cplx ? 2 : 1); }
+    const double* at(int i, int j) const { return p + ((size_t)j * rows_p + i) * (cplx ? 2 : 1); }
+    void zero();
+};
+
+// Scoped device scratch on the context's stream.
+struct DBuf {
+    Context* ctx = nullptr;
+    void* p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(Context& c, size_t b);
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept { *this = std::move(o); }
+    DBuf& operator=(DBuf&& o) noexcept;
+    ~DBuf();
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// ---- transfers -------------------------------------------------------------
+// Copy a rows x cols column-major operand (host or device pointer, ld in
+// elements) into / out of a padded device matrix.
+void copy_in(Context& ctx, DMat& dst, const double* src, int ld, bool src_on_device);
+void copy_out(Context& ctx, const DMat& src, double* dst, int ld, bool dst_on_device);
+void copy_dmat(Context& ctx, DMat& dst, const DMat& src);
+
+// ---- GEMM (gemm.cu) --------------------------------------------------------
+void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx);
+void gemm(Context& ctx, const GemmProblem& p, bool cplx);
+GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, double alpha_im, double beta_re,
+                      double beta_im);
+
+// ---- elementwise and reductions (blas1.cu) ---------------------------------
+void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, double beta_re, double beta_im);
+// dst := src * f (real factor, each part scaled on its own), whole padded extent.
+void scaled_copy(Context& ctx, DMat& dst, const DMat& src, double f);
+// t := t + s * f
+void add_scaled(Context& ctx, DMat& t, const DMat& s, double f);
+// dst := f * I on the valid diagonal, zero elsewhere.
+void set_identity(Context& ctx, DMat& dst, double f);
+// den := v - u, num := v + u
+void pade_split(Context& ctx, DMat& den, DMat& num, const DMat& v, const DMat& u);
+// Norms of the valid rows x cols block, returned to the host (synchronises).
+double norm1(Context& ctx, const DMat& a);
+double norminf(Context& ctx, const DMat& a);
+double normfro(Context& ctx, const DMat& a);
+// ||abs(A)^p||_1 without forming the power (MatrixExponential.cs:468-505).
+double one_norm_abs_power(Context& ctx, const DMat& a, int p);
+// Y := A X or A^H X for an n x t panel of device memory (x, y with leading
+// dimensions ldx, ldy in elements), in the reference's summation order.
+void panel_product(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint);
+// dst := src^H (transpose for real) over the padded extents.
+void conj_transpose(Context& ctx, DMat& dst, const DMat& src);
+// Add delta to the valid diagonal.
+void shift_diagonal(Context& ctx, DMat& a, double dre, double dim);
+// Sum of the valid diagonal, to the host.
+void trace(Context& ctx, const DMat& a, double* re, double* im);
+
+// ---- LU and triangular solves (lu.cu) ------------------------------------
+struct LuResult {
+    int singular_column = -1;
+    double smallest_pivot = 0.0, largest_pivot = 0.0;
+};
+// In-place LU of the valid m x n block of a (padded). d_piv: device int[min(m,n)].
+LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv);
+// B := A^-1 B or A^-H B from factors (valid n x n), in place on the valid rows of b.
+void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
+
+// ---- algorithms (algos.cu) -------------------------------------------------
+struct NormestResult {
+    double value = 0.0;
+    int iterations = 0, products = 0;
+};
+NormestResult normest_power(Context& ctx, const DMat& a, int power, int t, int itmax, int seed);
+NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed);
+
+struct ExpmInfo {
+    int degree = 0, squarings = 0;
+};
+// result := exp(a) for the valid n x n block.
+void expm(Context& ctx, const DMat& a, DMat& result, ExpmInfo* info);
+
+struct ExpmvInfo {
+    int degree = 0, scaling = 0, applications = 0, early_exits = 0;
+};
+void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info);
+
+}  // namespace tns

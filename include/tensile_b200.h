@@ -1,0 +1,189 @@
+/*
+ * tensile_b200 -- C ABI of the B200-native (sm_100a) dense hot path of the
+ * Tensile linear algebra library.
+ *
+ * Every entry point replaces a computation the reference library performs in
+ * managed C# behind its kernel seam (src/Tensile.Kernels/KernelEntry.cs:31-270)
+ * or, for whole algorithms, in src/Tensile (complex products, LU of complex
+ * matrices, normest1, Expm, Expmv). Each declaration names the reference
+ * interface it stands in for (paths relative to the reference project root).
+ *
+ * Conventions
+ *  - Matrices are column-major with a leading dimension (ld >= rows, counted
+ *    in elements), as MatrixShape defines them (src/Tensile/MatrixShape.cs:20-152).
+ *  - Complex matrices are interleaved (re, im) pairs of doubles: the memory
+ *    layout of System.Numerics.Complex, so a pinned Complex[] passes as is.
+ *  - Host-pointer entry points are synchronous: they copy the operands to the
+ *    GPU, compute, copy the results back and return only when the host buffers
+ *    may be unpinned (the reference pins spans for exactly one call,
+ *    src/Tensile.Kernels/KernelEntry.cs:3-30). On failure the destination is
+ *    left untouched (src/Tensile/ComplexKernels.cs:103-106).
+ *  - Entry points ending in _device take device pointers instead and run on the
+ *    context's stream; they also return only when the work has finished.
+ *  - Calls on one context are serialised (one CUDA stream per context, as one
+ *    Workspace serialises its operations on one lock,
+ *    src/Tensile/Workspace.cs:42,136-139). Distinct contexts are independent.
+ *  - Return value: TNS_OK or one of the TNS_E_* codes below; tns_last_error()
+ *    gives the message. The codes map one to one onto the exceptions the
+ *    reference throws for the same conditions.
+ */
+#ifndef TENSILE_B200_H
+#define TENSILE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TNS_OK 0
+#define TNS_E_ARGUMENT 1         /* ArgumentException: shapes disagree, bad ld, not square */
+#define TNS_E_SINGULAR 2         /* InvalidOperationException: exactly zero pivot */
+#define TNS_E_ALLOCATION_LIMIT 3 /* AllocationLimitException (src/Tensile/TensileLimits.cs:59-96) */
+#define TNS_E_OUT_OF_MEMORY 4    /* device allocation failed */
+#define TNS_E_DEVICE 5           /* CUDA runtime error */
+#define TNS_E_TIMEOUT 6          /* a bounded device-side wait gave up */
+#define TNS_E_DISPOSED 7         /* ObjectDisposedException: null or destroyed context */
+#define TNS_E_OUT_OF_RANGE 8     /* ArgumentOutOfRangeException */
+#define TNS_E_NULL 9             /* ArgumentNullException */
+
+typedef struct tns_context tns_context;
+
+/* Workspace(multithreaded) construction and Dispose (src/Tensile/Workspace.cs:52-72, 252-262):
+ * one CUDA stream and the device buffers of one workspace. max_elements is
+ * TensileLimits.MaxElements (src/Tensile/TensileLimits.cs:27-65); <= 0 means
+ * the reference default, Array.MaxLength. */
+int tns_create(int device, long long max_elements, tns_context** out);
+int tns_destroy(tns_context* ctx);
+const char* tns_last_error(const tns_context* ctx);
+int tns_set_max_elements(tns_context* ctx, long long max_elements);
+
+/* ---- products ----------------------------------------------------------- */
+
+/* C := beta*C + alpha*A*B, A m x k, B k x n. beta == 0 overwrites C (NaN in C
+ * does not survive). KernelEntry.Multiply (src/Tensile.Kernels/KernelEntry.cs:34-56)
+ * -> Gemm/ParallelGemm (src/Tensile.Kernels/Gemm.cs:117-203). */
+int tns_dgemm(tns_context* ctx, int m, int n, int k, double alpha, const double* a, int lda,
+              const double* b, int ldb, double beta, double* c, int ldc);
+int tns_dgemm_device(tns_context* ctx, int m, int n, int k, double alpha, const double* a, int lda,
+                     const double* b, int ldb, double beta, double* c, int ldc);
+
+/* Complex C := beta*C + alpha*A*B by the 4M method (four real products, never
+ * 3M) with the reference's alpha/beta special cases. alpha and beta are
+ * (re, im) pairs. ComplexKernels.Multiply (src/Tensile/ComplexKernels.cs:49-108,
+ * Combine :213-240); Workspace.Multiply(Complex) (src/Tensile/Workspace.Complex.cs:37-62). */
+int tns_zgemm(tns_context* ctx, int m, int n, int k, const double* alpha, const double* a, int lda,
+              const double* b, int ldb, const double* beta, double* c, int ldc);
+int tns_zgemm_device(tns_context* ctx, int m, int n, int k, const double* alpha, const double* a,
+                     int lda, const double* b, int ldb, const double* beta, double* c, int ldc);
+
+/* ---- exact norms -------------------------------------------------------- */
+
+/* kind: '1' (largest column sum), 'I' (largest row sum), 'F' (Frobenius,
+ * unscaled). Norms.One/Infinity/Frobenius (src/Tensile.Kernels/Norms.cs:11-66);
+ * complex: ComplexKernels.OneNorm/InfinityNorm (src/Tensile/ComplexKernels.cs:144-180),
+ * moduli by Complex.Abs. */
+int tns_dnorm(tns_context* ctx, char kind, int m, int n, const double* a, int lda, double* out);
+int tns_znorm(tns_context* ctx, char kind, int m, int n, const double* a, int lda, double* out);
+
+/* ---- LU with partial pivoting ------------------------------------------- */
+
+typedef struct {
+    int singular_column;   /* first column with an exactly zero pivot, or -1 */
+    double smallest_pivot; /* min |u_jj| (LuFactorization.SmallestPivot) */
+    double largest_pivot;  /* max |u_jj| */
+    double one_norm;       /* ||A||_1 of the input, captured before factoring */
+} tns_lu_info;
+
+/* In-place P*A = L*U (LAPACK packed form). pivots: min(m,n) 0-based entries,
+ * row k swapped with pivots[k] in increasing k. nb <= 0 selects the reference
+ * default (32 below min(m,n)=1024, else 64). Pivot rule: largest |a| (real) or
+ * |Re|+|Im| (complex), ties to the lowest index.
+ * Lu.Factor (src/Tensile.Kernels/Lu.cs:230-309) via KernelEntry.FactorLu
+ * (src/Tensile.Kernels/KernelEntry.cs:59-67); complex BlockedLu.Factor
+ * (src/Tensile/BlockedLu.cs:45-101) via Workspace.FactorLu(Complex)
+ * (src/Tensile/Workspace.Complex.cs:79-104). */
+int tns_dgetrf(tns_context* ctx, int m, int n, double* a, int lda, int nb, int* pivots,
+               tns_lu_info* info);
+int tns_zgetrf(tns_context* ctx, int m, int n, double* a, int lda, int nb, int* pivots,
+               tns_lu_info* info);
+
+/* Solve A X = B (adjoint = 0) or A^H X = B (adjoint = 1) in place from a
+ * factorization; TNS_E_SINGULAR when singular_column >= 0.
+ * Lu.Solve/SolveTransposed (src/Tensile.Kernels/Lu.cs:336-378) via
+ * KernelEntry.SolveLu/SolveLuTransposed (src/Tensile.Kernels/KernelEntry.cs:70-95);
+ * complex BlockedLu.Solve/SolveAdjoint (src/Tensile/BlockedLu.cs:105-141). */
+int tns_dgetrs(tns_context* ctx, int n, int nrhs, const double* lu, int lda, const int* pivots,
+               int singular_column, double* b, int ldb, int adjoint);
+int tns_zgetrs(tns_context* ctx, int n, int nrhs, const double* lu, int lda, const int* pivots,
+               int singular_column, double* b, int ldb, int adjoint);
+
+/* rcond = 1/(||A||_1 * est ||A^-1||_1), 0 when singular or ||A||_1 == 0.
+ * Condition.ReciprocalOne (src/Tensile/NormEstimate.cs:432-466) over
+ * LuInverseOperator (src/Tensile/LinearOperators.cs:303-350). */
+int tns_dgecon(tns_context* ctx, int n, const double* lu, int lda, const int* pivots,
+               int singular_column, double anorm, double* rcond);
+int tns_zgecon(tns_context* ctx, int n, const double* lu, int lda, const int* pivots,
+               int singular_column, double anorm, double* rcond);
+
+/* ---- block 1-norm estimation -------------------------------------------- */
+
+typedef struct {
+    double value;   /* lower bound on ||A^power||_1 */
+    int iterations;
+    int products;   /* operator applications, counting each probe column */
+} tns_normest_result;
+
+/* NormEstimate.Estimate (src/Tensile/NormEstimate.cs:104-274) over the dense
+ * power operators DenseMatrixOperator / ComplexDenseOperator
+ * (src/Tensile/LinearOperators.cs:89-293). t, itmax and seed as
+ * NormEstimate.Of (defaults 2, 5, 20260915). */
+int tns_dnormest1_power(tns_context* ctx, int n, const double* a, int lda, int power, int t, int itmax,
+                        int seed, tns_normest_result* out);
+int tns_znormest1_power(tns_context* ctx, int n, const double* a, int lda, int power, int t, int itmax,
+                        int seed, tns_normest_result* out);
+
+/* ---- matrix exponential ------------------------------------------------- */
+
+typedef struct {
+    int degree;    /* Pade degree 3, 5, 7, 9 or 13; 0 for n <= 1 */
+    int squarings; /* s */
+} tns_expm_info;
+
+/* exp(A) by Al-Mohy & Higham 2009 scaling and squaring.
+ * MatrixExponential.Expm (src/Tensile/MatrixExponential.cs:136-270;
+ * complex src/Tensile/MatrixExponential.Complex.cs:35-53); info mirrors
+ * ExpmDiagnostics (:575-582). TNS_E_SINGULAR: singular Pade denominator. */
+int tns_dexpm(tns_context* ctx, int n, const double* a, int lda, double* out, int ldo, tns_expm_info* info);
+int tns_zexpm(tns_context* ctx, int n, const double* a, int lda, double* out, int ldo, tns_expm_info* info);
+
+/* A batch of complex exponentials of independent orders: out[i] = exp(a[i]).
+ * The frequency-sweep form of the same algorithm; every decision per matrix
+ * is the one tns_zexpm takes. Host pointers (synchronous) or, for
+ * _device, device pointers. infos may be NULL. */
+int tns_zexpm_batched(tns_context* ctx, int count, const int* orders, const double* const* a,
+                      const int* lda, double* const* out, const int* ldo, tns_expm_info* infos);
+int tns_zexpm_batched_device(tns_context* ctx, int count, const int* orders, const double* const* a,
+                             const int* lda, double* const* out, const int* ldo, tns_expm_info* infos);
+
+/* ---- action of the exponential ------------------------------------------ */
+
+typedef struct {
+    int degree;       /* Taylor degree m (a cap) */
+    int scaling;      /* s >= 1 */
+    int applications; /* operator applications performed */
+    int early_exits;  /* inner loops stopped by the tolerance test */
+} tns_expmv_info;
+
+/* exp(tA)B for dense A (trace shift, sharp ||A^p||^(1/p) bounds, early exit).
+ * MatrixExponentialAction.Expmv (src/Tensile/MatrixExponentialAction.cs:113-320;
+ * complex src/Tensile/MatrixExponentialAction.Complex.cs:34-63); info mirrors
+ * ExpmvDiagnostics (:498-511). TNS_E_OUT_OF_RANGE when the application count
+ * cannot be represented (:386-395). */
+int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
+               double t, double* out, int ldo, tns_expmv_info* info);
+int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
+               double t, double* out, int ldo, tns_expmv_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

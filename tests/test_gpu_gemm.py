@@ -1,0 +1,86 @@
+"""DMMA GEMM (real and fused 4M complex) against the oracle, through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import net_matrix, relfro
+
+pytestmark = pytest.mark.gpu
+
+# GemmTests.cs:31-44 plus the 1024^3 benchmark shape.
+SHAPES = [(1, 1, 1), (1, 1, 64), (8, 6, 4), (16, 8, 16), (17, 9, 5), (31, 33, 7), (48, 48, 48),
+          (64, 64, 64), (65, 63, 66), (100, 37, 129), (129, 130, 2), (300, 257, 511), (1024, 1024, 1024)]
+
+
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_dgemm_matches_oracle(ws, orc, m, n, k):
+    a = net_matrix(orc, m, k, 11) if m * k <= 40000 else np.random.default_rng(1).uniform(-1, 1, (m, k))
+    b = net_matrix(orc, k, n, 12) if k * n <= 40000 else np.random.default_rng(2).uniform(-1, 1, (k, n))
+    c = ws.multiply(a, b)
+    ref = orc.gemm(a, b)
+    assert relfro(c, ref) < 1e-13
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (1.0, 1.0), (-1.0, 1.0), (0.0, 1.0), (2.5, -0.5)])
+def test_dgemm_alpha_beta(ws, orc, alpha, beta):
+    a = net_matrix(orc, 65, 66, 1)
+    b = net_matrix(orc, 66, 63, 2)
+    c0 = net_matrix(orc, 65, 63, 3)
+    c = ws.multiply(a, b, c0, alpha, beta)
+    ref = orc.gemm(a, b, c0, alpha, beta)
+    assert relfro(c, ref) < 1e-13
+
+
+def test_beta_zero_overwrites_nan(ws):
+    a = np.ones((17, 9))
+    b = np.ones((9, 5))
+    c = np.full((17, 5), np.nan)
+    out = ws.multiply(a, b, c, 1.0, 0.0)
+    assert np.array_equal(out, np.full((17, 5), 9.0))
+
+
+def test_padding_is_never_written(ws):
+    """Only the m x n block of a strided C changes (GemmTests.cs:107-129)."""
+    from csharp_linearalgebra_b200 import _native as N
+    import ctypes as C
+    m, n, k, ldc = 10, 7, 5, 13
+    a = np.asfortranarray(np.random.default_rng(3).standard_normal((m, k)))
+    b = np.asfortranarray(np.random.default_rng(4).standard_normal((k, n)))
+    cbuf = np.full((ldc, n), 7.25, order="F")
+    rc = N.load().tns_dgemm(ws.handle, m, n, k, 1.0, a.ctypes.data, m, b.ctypes.data, k, 0.0,
+                            cbuf.ctypes.data, ldc)
+    assert rc == 0
+    assert np.all(cbuf[m:, :] == 7.25)
+    assert relfro(cbuf[:m, :], a @ b) < 1e-14
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (17, 9, 5), (65, 63, 66), (100, 37, 129), (256, 256, 256), (512, 512, 512)])
+def test_zgemm_matches_oracle(ws, orc, m, n, k):
+    rng = np.random.default_rng(m + n + k)
+    a = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    c = ws.multiply(a, b)
+    ref = orc.gemm(a, b)
+    assert relfro(c, ref) < 1e-13
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (1.0, 1.0), (-1.0, 1.0), (2.0 - 1.0j, 0.5 + 0.25j)])
+def test_zgemm_alpha_beta(ws, orc, alpha, beta):
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((33, 31)) + 1j * rng.standard_normal((33, 31))
+    b = rng.standard_normal((31, 29)) + 1j * rng.standard_normal((31, 29))
+    c0 = rng.standard_normal((33, 29)) + 1j * rng.standard_normal((33, 29))
+    c = ws.multiply(a, b, c0, complex(alpha), complex(beta))
+    ref = orc.gemm(a, b, c0, complex(alpha), complex(beta))
+    assert relfro(c, ref) < 1e-13
+
+
+def test_4m_keeps_small_imaginary_parts(ws, orc):
+    """ComplexMultiplyTests.cs:185-212: with tiny imaginary parts the 4M product
+    keeps Im(AB) to relative accuracy (3M would lose it)."""
+    rng = np.random.default_rng(21)
+    n = 64
+    ar, br = rng.standard_normal((n, n)), rng.standard_normal((n, n))
+    ai, bi = 1e-9 * rng.standard_normal((n, n)), 1e-9 * rng.standard_normal((n, n))
+    c = ws.multiply(ar + 1j * ai, br + 1j * bi)
+    im_exact = ar @ bi + ai @ br
+    assert np.linalg.norm(c.imag - im_exact) / np.linalg.norm(im_exact) < 1e-13

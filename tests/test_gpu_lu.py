@@ -1,0 +1,108 @@
+"""LU with partial pivoting, solves and rcond on the GPU against the oracle.
+Pivot sequences must match bit for bit."""
+import numpy as np
+import pytest
+
+from conftest import net_matrix, relfro
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(1, 1), (2, 2), (5, 5), (17, 17), (32, 32), (33, 33), (64, 64), (65, 65), (100, 100),
+          (129, 129), (200, 73), (73, 200), (129, 64), (64, 129), (512, 512)]
+
+
+@pytest.mark.parametrize("m,n", SHAPES)
+@pytest.mark.parametrize("nb", [0, 32, 64])
+def test_real_lu_matches_oracle(ws, orc, m, n, nb):
+    a = net_matrix(orc, m, n, seed=m * 7 + n) if m * n <= 40000 else \
+        np.random.default_rng(m).uniform(-0.5, 0.5, (m, n))
+    lu = ws.factor_lu(a, nb)
+    f, piv, info = orc.getrf(a, nb)
+    assert np.array_equal(lu.pivots, piv)
+    assert lu.singular_column == info["singular_column"] == -1
+    assert relfro(lu.factors, f) < 1e-12
+    assert lu.smallest_pivot == pytest.approx(info["smallest_pivot"], rel=1e-12)
+    assert lu.largest_pivot == pytest.approx(info["largest_pivot"], rel=1e-12)
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (3, 3), (17, 17), (64, 64), (65, 65), (100, 37), (37, 100), (300, 300)])
+def test_complex_lu_matches_oracle(ws, orc, m, n):
+    rng = np.random.default_rng(m * 100 + n)
+    a = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    lu = ws.factor_lu(a)
+    f, piv, info = orc.getrf(a)
+    assert np.array_equal(lu.pivots, piv)
+    assert relfro(lu.factors, f) < 1e-12
+
+
+def test_pivot_maximises_sum_of_absolute_parts(ws):
+    a = np.array([[3.0, 1.0], [2.0 + 2.0j, 1.0]])
+    assert ws.factor_lu(a).pivots[0] == 1
+
+
+def test_pivot_ties_go_to_lowest_index(ws):
+    a = np.array([[1.0 + 1.0j, 1.0], [-2.0, 2.0], [0.5 - 1.5j, 3.0]])
+    assert ws.factor_lu(a).pivots[0] == 0
+
+
+def test_exact_zero_pivot_is_reported(ws, orc):
+    from csharp_linearalgebra_b200 import SingularMatrixError
+    a = net_matrix(orc, 16, 16, 12) + 16 * np.eye(16)
+    a[:, 5] = 0.0
+    lu = ws.factor_lu(a, 16)
+    assert lu.is_singular and lu.singular_column == 5
+    with pytest.raises(SingularMatrixError):
+        lu.solve(np.ones(16))
+    with pytest.raises(SingularMatrixError):
+        lu.solve_adjoint(np.ones(16))
+
+
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (17, 3), (100, 8), (129, 70), (512, 8), (300, 300)])
+def test_solves_match_oracle(ws, orc, n, nrhs):
+    rng = np.random.default_rng(n + nrhs)
+    a = rng.uniform(-0.5, 0.5, (n, n))
+    b = rng.uniform(-0.5, 0.5, (n, nrhs))
+    lu = ws.factor_lu(a)
+    x = lu.solve(b)
+    xt = lu.solve_adjoint(b)
+    f, piv, info = orc.getrf(a)
+    assert relfro(x, orc.getrs(f, piv, b)) < 1e-12
+    assert relfro(xt, orc.getrs(f, piv, b, adjoint=True)) < 1e-12
+    # backward error ||Ax - b||_inf / (||A||_inf ||x||_inf) (LuTests.cs:69-105)
+    assert np.abs(a @ x - b).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max()) < 1e-12
+
+
+@pytest.mark.parametrize("n,nrhs", [(5, 1), (64, 8), (200, 200)])
+def test_complex_solves_match_oracle(ws, orc, n, nrhs):
+    rng = np.random.default_rng(3 * n + nrhs)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    lu = ws.factor_lu(a)
+    f, piv, _ = orc.getrf(a)
+    assert relfro(lu.solve(b), orc.getrs(f, piv, b)) < 1e-12
+    assert relfro(lu.solve_adjoint(b), orc.getrs(f, piv, b, adjoint=True)) < 1e-12
+    x = lu.solve(b)
+    # complex solve backward error (ComplexLuTests.cs:126-133)
+    assert np.abs(a @ x - b).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max()) < 1e-14 * n
+
+
+@pytest.mark.parametrize("n", [10, 64, 200])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_rcond_matches_oracle(ws, orc, n, cplx):
+    rng = np.random.default_rng(n)
+    a = rng.uniform(-0.5, 0.5, (n, n))
+    if cplx:
+        a = a + 1j * rng.uniform(-0.5, 0.5, (n, n))
+    lu = ws.factor_lu(a)
+    f, piv, info = orc.getrf(a)
+    r = lu.reciprocal_condition()
+    ro = orc.gecon(f, piv, -1, orc.norm1(a))
+    assert r == pytest.approx(ro, rel=1e-10)
+    exact = 1.0 / (np.linalg.norm(a, 1) * np.linalg.norm(np.linalg.inv(a), 1))
+    assert exact * (1 - 1e-10) <= r <= 3 * exact
+
+
+def test_determinant(ws):
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal((12, 12))
+    assert ws.factor_lu(a).determinant() == pytest.approx(np.linalg.det(a), rel=1e-12)
