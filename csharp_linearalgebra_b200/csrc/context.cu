@@ -153,6 +153,10 @@ GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, do
     p.alpha_im = alpha_im;
     p.beta_re = beta_re;
     p.beta_im = beta_im;
+    p.kc = 0;  // the reference's KC for this product's true size
+    p.work = (long long)a.rows * b.cols * a.cols;
+    p.W = nullptr;
+    p.ldw = 0;
     return p;
 }
 

@@ -1,4 +1,4 @@
-// FP64 GEMM on the B200 tensor cores (DMMA), real and complex (fused 4M).
+// FP64 GEMM on the B200 tensor cores (DMMA), real and complex (4M).
 //
 // Replaces the reference's BLIS-style CPU GEMM (src/Tensile.Kernels/Gemm.cs:117-203,
 // ParallelGemm.cs:138-229, MicroKernels.cs:57-273) and its 4M complex product
@@ -6,26 +6,32 @@
 //
 // Design
 //  - tcgen05 has no f64 kind, so the math is warp-level mma.sync m16n8k4 f64.
+//    Measured on B200, a DMMA accumulation is bit-identical to a chain of
+//    fused multiply-adds in k order -- the reference micro-kernel's inner loop
+//    -- so the kernel reproduces the reference's result bit for bit by folding
+//    the accumulator into C (c = fma(alpha, acc, c)) at the end of each
+//    KC-deep slab, where the reference writes back, with the reference's KC.
+//  - Complex products keep the reference's 4M order: pass 1 forms
+//    P = Ar*Br and Q = Ar*Bi slab by slab, pass 2 folds in P -= Ai*Bi and
+//    Q += Ai*Br, then P + iQ is combined into C with the reference's alpha and
+//    beta special cases (ComplexKernels.Combine). Both passes stream the same
+//    interleaved tiles; no split copies of A or B are made.
 //  - Operand tiles are staged in shared memory by the TMA engine's bulk copies
 //    (cp.async.bulk, one per tile column) completing on mbarriers; a producer
-//    warp runs STAGES tiles ahead of the consumer (math) warps. Each smem
-//    column is padded so that the DMMA fragment loads are bank-conflict free
-//    (real: A stride = 4 mod 16 doubles, B stride 20; complex: A stride
-//    = 2 mod 8 complex, B stride 20).
+//    warp runs STAGES tiles ahead of the math warps. Smem columns are padded so
+//    the DMMA fragment loads are bank-conflict free (real: A stride = 4 mod 16
+//    doubles, B stride 20; complex: A stride = 2 mod 8 complex, B stride 20).
 //  - The MMA computes C^T = B^T A^T, so a thread's accumulator pair covers two
-//    consecutive rows of column-major C and the epilogue stores 16-byte pairs.
-//  - Complex (interleaved re,im) runs the 4M product inside one kernel: four
-//    real MMAs per fragment pair, Re += Br*Ar - Bi*Ai, Im += Br*Ai + Bi*Ar, so
-//    no split, combine or extra pass over memory.
+//    consecutive rows of column-major C and the epilogue moves 16-byte pairs.
 //  - Persistent CTAs walk a list of problems (grouped GEMM): the same kernel
 //    serves one product, or every matrix of a batch in one launch.
 //  - Every wait is bounded (device_util.cuh): a stuck pipeline records an error
 //    in the context flag and the kernel returns.
 //
 // Operand requirements (checked on the host before every launch): pointers and
-// leading dimensions 16-byte aligned, M and N even, K a multiple of 16. The
-// library's device matrices are zero-padded to multiples of 64, which meets
-// all of them.
+// leading dimensions 16-byte aligned, M and N even, K and KC multiples of 16.
+// The library's device matrices are zero-padded to multiples of 64, which
+// meets all of them.
 
 #include "device_util.cuh"
 #include "tns_internal.h"
@@ -81,13 +87,15 @@ struct GemmLaunch {
 
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid_constant__ GemmLaunch L) {
+    using E = typename std::conditional<Cfg::kComplex, double2, double>::type;
+    constexpr int PASSES = Cfg::kComplex ? 2 : 1;
     const GemmProblem* probs = L.list ? L.list : L.inl;
     const int nprob = L.nprob;
     const int total_tiles = L.total_tiles;
     int* err = L.err;
-    using E = typename std::conditional<Cfg::kComplex, double2, double>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
     uint64_t* empty = full + Cfg::STAGES;
 
@@ -122,7 +130,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
             uint32_t bytes = (uint32_t)(Cfg::BK * rows + cols * Cfg::BK) * Cfg::ESZ;
             const E* A = reinterpret_cast<const E*>(P.A);
             const E* B = reinterpret_cast<const E*>(P.B);
-            for (int k0 = 0; k0 < P.K; k0 += Cfg::BK, ++it) {
+            const int nk = P.K / Cfg::BK;
+            for (int q = 0; q < nk * PASSES; ++q, ++it) {
+                const int k0 = (q % nk) * Cfg::BK;
                 int s = it % Cfg::STAGES;
                 uint32_t round = it / Cfg::STAGES;
                 if (!mbar_wait_bounded(&empty[s], (round & 1) ^ 1, err, kDevTimeoutEmpty)) {
@@ -168,22 +178,31 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
         int local = tile - P.tile_begin;
-        int m0 = (local % P.tiles_m) * Cfg::BM;
-        int n0 = (local / P.tiles_m) * Cfg::BN;
+        const int m0 = (local % P.tiles_m) * Cfg::BM;
+        const int n0 = (local / P.tiles_m) * Cfg::BN;
+        const int nk = P.K / Cfg::BK;
+        const int slab = P.kc / Cfg::BK;  // k-tiles per KC slab
+        const double ar = P.alpha_re, ai = P.alpha_im, br = P.beta_re, bi = P.beta_im;
 
-        double acc_re[Cfg::NF][Cfg::MF][4];
-        double acc_im[Cfg::kComplex ? Cfg::NF : 1][Cfg::kComplex ? Cfg::MF : 1][4];
+        // acc0: real part / P-pass product, acc1 (complex): Q-pass product
+        double acc0[Cfg::NF][Cfg::MF][4];
+        double acc1[Cfg::kComplex ? Cfg::NF : 1][Cfg::kComplex ? Cfg::MF : 1][4];
+        auto zero_acc = [&]() {
 #pragma unroll
-        for (int i = 0; i < Cfg::NF; ++i)
+            for (int i = 0; i < Cfg::NF; ++i)
 #pragma unroll
-            for (int j = 0; j < Cfg::MF; ++j)
+                for (int j = 0; j < Cfg::MF; ++j)
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    acc_re[i][j][r] = 0.0;
-                    if constexpr (Cfg::kComplex) acc_im[i][j][r] = 0.0;
-                }
+                    for (int r = 0; r < 4; ++r) {
+                        acc0[i][j][r] = 0.0;
+                        if constexpr (Cfg::kComplex) acc1[i][j][r] = 0.0;
+                    }
+        };
+        zero_acc();
 
-        for (int k0 = 0; k0 < P.K; k0 += Cfg::BK, ++it) {
+        for (int q = 0; q < nk * PASSES; ++q, ++it) {
+            const int pass = q / nk;
+            const int kt = q % nk;
             int s = it % Cfg::STAGES;
             if (!mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
             const E* As = stage_a(s) + wm * Cfg::WM + g;
@@ -203,81 +222,111 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
 #pragma unroll
                     for (int j = 0; j < Cfg::MF; ++j) {
                         if constexpr (Cfg::kComplex) {
-                            dmma_16x8x4(acc_re[i][j], fa0[i].x, fa1[i].x, fb[j].x);
-                            dmma_16x8x4(acc_re[i][j], -fa0[i].y, -fa1[i].y, fb[j].y);
-                            dmma_16x8x4(acc_im[i][j], fa0[i].x, fa1[i].x, fb[j].y);
-                            dmma_16x8x4(acc_im[i][j], fa0[i].y, fa1[i].y, fb[j].x);
+                            // (A*B)^T = B^T A^T. Pass 0: Ar*Br -> acc0, Ar*Bi -> acc1.
+                            // Pass 1: Ai*Bi -> acc0, Ai*Br -> acc1.
+                            double a_part = pass == 0 ? fb[j].x : fb[j].y;
+                            dmma_16x8x4(acc0[i][j], pass == 0 ? fa0[i].x : fa0[i].y,
+                                        pass == 0 ? fa1[i].x : fa1[i].y, a_part);
+                            dmma_16x8x4(acc1[i][j], pass == 0 ? fa0[i].y : fa0[i].x,
+                                        pass == 0 ? fa1[i].y : fa1[i].x, a_part);
                         } else {
-                            dmma_16x8x4(acc_re[i][j], fa0[i], fa1[i], fb[j]);
+                            dmma_16x8x4(acc0[i][j], fa0[i], fa1[i], fb[j]);
                         }
                     }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
-        }
 
-        // Epilogue: C := beta*C + alpha*acc with the reference's special cases.
-        E* C = reinterpret_cast<E*>(P.C);
-        const double ar = P.alpha_re, ai = P.alpha_im, br = P.beta_re, bi = P.beta_im;
+            const bool slab_end = ((kt + 1) % slab == 0) || (kt + 1 == nk);
+            if (!slab_end) continue;
+            const bool first = (kt + 1) <= slab;  // first slab of this pass
+            const bool last = (kt + 1 == nk) && (pass == PASSES - 1);
+
+            // Fold the slab into C (real) or into P + iQ (complex).
 #pragma unroll
-        for (int i = 0; i < Cfg::NF; ++i)
+            for (int i = 0; i < Cfg::NF; ++i)
 #pragma unroll
-            for (int j = 0; j < Cfg::MF; ++j) {
-                int m = m0 + wm * Cfg::WM + j * 8 + 2 * t;
-                if (m >= P.M) continue;
+                for (int j = 0; j < Cfg::MF; ++j) {
+                    int m = m0 + wm * Cfg::WM + j * 8 + 2 * t;
+                    if (m >= P.M) continue;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    int n = n0 + wn * Cfg::WN + i * 16 + g + 8 * h;
-                    if (n >= P.N) continue;
-                    E* dst = C + (size_t)n * P.ldc + m;
-                    if constexpr (!Cfg::kComplex) {
-                        double2 cur = make_double2(0.0, 0.0);
-                        if (br != 0.0) {
-                            cur = *reinterpret_cast<const double2*>(dst);
-                            if (br != 1.0) cur = make_double2(mul_rn(cur.x, br), mul_rn(cur.y, br));
-                        }
-                        double2 out;
-                        out.x = fma(ar, acc_re[i][j][2 * h], cur.x);
-                        out.y = fma(ar, acc_re[i][j][2 * h + 1], cur.y);
-                        *reinterpret_cast<double2*>(dst) = out;
-                    } else {
-                        bool unit_alpha = (ar == 1.0 && ai == 0.0);
-                        bool real_alpha = (ai == 0.0);
-                        bool zero_beta = (br == 0.0 && bi == 0.0);
-                        bool unit_beta = (br == 1.0 && bi == 0.0);
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            double p = acc_re[i][j][2 * h + q];
-                            double qq = acc_im[i][j][2 * h + q];
-                            double pr, pi;
-                            if (unit_alpha) {
-                                pr = p;
-                                pi = qq;
-                            } else if (real_alpha) {
-                                pr = mul_rn(ar, p);
-                                pi = mul_rn(ar, qq);
-                            } else {
-                                pr = sub_rn(mul_rn(ar, p), mul_rn(ai, qq));
-                                pi = add_rn(mul_rn(ai, p), mul_rn(ar, qq));
-                            }
-                            double2 o;
-                            if (zero_beta) {
-                                o = make_double2(pr, pi);
-                            } else {
-                                double2 c = dst[q];
-                                if (unit_beta) {
-                                    o = make_double2(add_rn(c.x, pr), add_rn(c.y, pi));
-                                } else {
-                                    double cr = sub_rn(mul_rn(br, c.x), mul_rn(bi, c.y));
-                                    double ci = add_rn(mul_rn(bi, c.x), mul_rn(br, c.y));
-                                    o = make_double2(add_rn(cr, pr), add_rn(ci, pi));
+                    for (int h = 0; h < 2; ++h) {
+                        int n = n0 + wn * Cfg::WN + i * 16 + g + 8 * h;
+                        if (n >= P.N) continue;
+                        if constexpr (!Cfg::kComplex) {
+                            double* dst = reinterpret_cast<double*>(P.C) + (size_t)n * P.ldc + m;
+                            double2 cur;
+                            if (first) {
+                                // ScaleC (Gemm.cs:187-203): beta == 0 overwrites.
+                                cur = make_double2(0.0, 0.0);
+                                if (br != 0.0) {
+                                    cur = *reinterpret_cast<const double2*>(dst);
+                                    if (br != 1.0) cur = make_double2(mul_rn(cur.x, br), mul_rn(cur.y, br));
                                 }
+                            } else {
+                                cur = *reinterpret_cast<const double2*>(dst);
                             }
-                            dst[q] = o;
+                            double2 out;
+                            out.x = fma(ar, acc0[i][j][2 * h], cur.x);
+                            out.y = fma(ar, acc0[i][j][2 * h + 1], cur.y);
+                            *reinterpret_cast<double2*>(dst) = out;
+                        } else {
+                            double2* W = reinterpret_cast<double2*>(P.W ? P.W : P.C) + (size_t)n * (P.W ? P.ldw : P.ldc) + m;
+                            double2* C = reinterpret_cast<double2*>(P.C) + (size_t)n * P.ldc + m;
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                double pacc = acc0[i][j][2 * h + e];
+                                double qacc = acc1[i][j][2 * h + e];
+                                double2 pq;
+                                if (pass == 0) {
+                                    // real = Ar*Br (alpha 1, beta 0), imag = Ar*Bi (alpha 1, beta 0)
+                                    double2 prev = first ? make_double2(0.0, 0.0) : W[e];
+                                    pq = make_double2(fma(1.0, pacc, prev.x), fma(1.0, qacc, prev.y));
+                                } else {
+                                    // real += -1 * Ai*Bi, imag += 1 * Ai*Br (beta 1)
+                                    double2 prev = W[e];
+                                    pq = make_double2(fma(-1.0, pacc, prev.x), fma(1.0, qacc, prev.y));
+                                }
+                                if (!last) {
+                                    W[e] = pq;
+                                    continue;
+                                }
+                                // Combine (ComplexKernels.cs:213-240).
+                                const bool unit_alpha = (ar == 1.0 && ai == 0.0);
+                                const bool real_alpha = (ai == 0.0);
+                                const bool zero_beta = (br == 0.0 && bi == 0.0);
+                                const bool unit_beta = (br == 1.0 && bi == 0.0);
+                                double pr, pi;
+                                if (unit_alpha) {
+                                    pr = pq.x;
+                                    pi = pq.y;
+                                } else if (real_alpha) {
+                                    pr = mul_rn(ar, pq.x);
+                                    pi = mul_rn(ar, pq.y);
+                                } else {
+                                    pr = sub_rn(mul_rn(ar, pq.x), mul_rn(ai, pq.y));
+                                    pi = add_rn(mul_rn(ai, pq.x), mul_rn(ar, pq.y));
+                                }
+                                double2 o;
+                                if (zero_beta) {
+                                    o = make_double2(pr, pi);
+                                } else {
+                                    double2 c = C[e];
+                                    if (unit_beta) {
+                                        o = make_double2(add_rn(c.x, pr), add_rn(c.y, pi));
+                                    } else {
+                                        double cr = sub_rn(mul_rn(br, c.x), mul_rn(bi, c.y));
+                                        double ci = add_rn(mul_rn(bi, c.x), mul_rn(br, c.y));
+                                        o = make_double2(add_rn(cr, pr), add_rn(ci, pi));
+                                    }
+                                }
+                                C[e] = o;
+                            }
                         }
                     }
                 }
-            }
+            zero_acc();
+        }
     }
 }
 
@@ -287,10 +336,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
 
 namespace {
 
-using RealBig = GemmCfg<false, 4, 2, 4>;     // 128 x 128 tiles, 8 math warps
-using RealSmall = GemmCfg<false, 2, 1, 4>;   // 64 x 64 tiles, 2 math warps
-using CplxBig = GemmCfg<true, 4, 2, 3>;      // 128 x 64 tiles, 8 math warps
-using CplxSmall = GemmCfg<true, 2, 2, 4>;    // 64 x 64 tiles, 4 math warps
+using RealBig = GemmCfg<false, 4, 2, 4>;    // 128 x 128 tiles, 8 math warps
+using RealSmall = GemmCfg<false, 2, 1, 4>;  // 64 x 64 tiles, 2 math warps
+using CplxBig = GemmCfg<true, 4, 2, 3>;     // 128 x 64 tiles, 8 math warps
+using CplxSmall = GemmCfg<true, 2, 2, 4>;   // 64 x 64 tiles, 4 math warps
 
 template <class Cfg>
 void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
@@ -330,9 +379,9 @@ void check_problem(const GemmProblem& p, bool cplx) {
     int esz = cplx ? 16 : 8;
     auto aligned = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     bool ok = p.M >= 0 && p.N >= 0 && p.K >= 0 && (p.M % 2 == 0) && (p.N % 2 == 0) && (p.K % 16 == 0) &&
-              aligned(p.A) && aligned(p.B) && aligned(p.C) && ((size_t)p.lda * esz) % 16 == 0 &&
-              ((size_t)p.ldb * esz) % 16 == 0 && ((size_t)p.ldc * esz) % 16 == 0 && p.lda >= p.M &&
-              p.ldb >= p.K && p.ldc >= p.M;
+              p.kc > 0 && (p.kc % 16 == 0) && aligned(p.A) && aligned(p.B) && aligned(p.C) &&
+              ((size_t)p.lda * esz) % 16 == 0 && ((size_t)p.ldb * esz) % 16 == 0 && ((size_t)p.ldc * esz) % 16 == 0 &&
+              p.lda >= p.M && p.ldb >= p.K && p.ldc >= p.M && (!p.W || (aligned(p.W) && p.ldw >= p.M));
     if (!ok) fail(TNS_E_ARGUMENT, "internal GEMM operand violates the bulk-copy layout contract");
 }
 
@@ -341,35 +390,40 @@ void check_problem(const GemmProblem& p, bool cplx) {
 void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
     std::vector<GemmProblem> work;
     work.reserve(probs.size());
-    long long flops_big = 0;
-    for (auto& p : probs) {
+    std::vector<DBuf> scratch;
+    for (auto& p0 : probs) {
+        GemmProblem p = p0;
+        if (p.kc <= 0) p.kc = reference_kc(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
         check_problem(p, cplx);
         if (p.M == 0 || p.N == 0) continue;
         if (p.K == 0) {
-            // No product: C := beta*C (+ 0). Handled by the scale kernel.
+            // No product: C := beta*C.
             scale_inplace(ctx, p.C, p.M, p.N, p.ldc, cplx, p.beta_re, p.beta_im);
             continue;
         }
+        if (cplx && !p.W && !(p.alpha_re == 1.0 && p.alpha_im == 0.0 && p.beta_re == 0.0 && p.beta_im == 0.0)) {
+            // P + iQ need their own storage when the combine is not a plain copy.
+            scratch.emplace_back(ctx, (size_t)p.M * p.N * 16);
+            p.W = scratch.back().p;
+            p.ldw = p.M;
+        }
         work.push_back(p);
-        flops_big += (long long)p.M * p.N * p.K;
     }
     if (work.empty()) return;
     // Big tiles only when they fill the machine.
-    bool big = true;
     if (cplx) {
         long long tiles = 0;
-        for (auto& p : work) tiles += (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN);
-        big = tiles >= ctx.num_sms;
-        if (big) launch_cfg<CplxBig>(ctx, work);
+        for (auto& p : work)
+            tiles += (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN);
+        if (tiles >= ctx.num_sms) launch_cfg<CplxBig>(ctx, work);
         else launch_cfg<CplxSmall>(ctx, work);
     } else {
         long long tiles = 0;
-        for (auto& p : work) tiles += (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
-        big = tiles >= ctx.num_sms;
-        if (big) launch_cfg<RealBig>(ctx, work);
+        for (auto& p : work)
+            tiles += (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
+        if (tiles >= ctx.num_sms) launch_cfg<RealBig>(ctx, work);
         else launch_cfg<RealSmall>(ctx, work);
     }
-    (void)flops_big;
 }
 
 void gemm(Context& ctx, const GemmProblem& p, bool cplx) {

@@ -341,14 +341,12 @@ __global__ void pivot_range_kernel(const double* a, int ld, int limit, double* o
 __global__ void init_int_kernel(int* p, int v) { *p = v; }
 
 // The 64 x 64 complex block needs 64 KB of dynamic shared memory, above the
-// default 48 KB, so both triangular kernels opt in once per device.
+// default 48 KB, so the triangular kernels opt in before each launch (the
+// attribute is per kernel; real and complex instances share a signature, so
+// no static flag can tell them apart).
 template <class K>
-void allow_64k_smem(Context& ctx, K kernel) {
-    static bool done[64] = {false};
-    if (!done[ctx.device]) {
-        TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 16));
-        done[ctx.device] = true;
-    }
+void allow_64k_smem(Context&, K kernel) {
+    TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 16));
 }
 
 template <bool CPLX>

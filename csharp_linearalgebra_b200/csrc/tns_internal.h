@@ -38,6 +38,13 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 // One problem of a (grouped) GEMM: C := beta*C + alpha*A*B. lda/ldb/ldc are in
 // elements (complex elements for complex problems).
+//
+// kc is the reference's KC slab depth (Gemm.cs / ParallelGemm.cs): the
+// accumulator is folded into C as c = fma(alpha, acc, c) at the end of every
+// kc-deep slab of K, exactly where the reference's micro-kernel writes back.
+// 0 lets gemm() choose the reference's rule for the problem's true size.
+// W (complex only): scratch for the 4M partial products P + iQ, M x N with
+// leading dimension ldw; null when the result can be written straight into C.
 struct GemmProblem {
     const void* A;
     const void* B;
@@ -46,7 +53,16 @@ struct GemmProblem {
     int M, N, K;
     int tiles_m, tiles_n, tile_begin;
     double alpha_re, alpha_im, beta_re, beta_im;
+    int kc;
+    void* W;
+    int ldw;
+    long long work;  // m*n*k of the unpadded product, for the KC rule
 };
+
+// The reference's KC rule (GemmDispatch.cs:45,109; Gemm.cs:62; ParallelGemm):
+// the default multithreaded workspace runs products of at least 2^24 work
+// threaded with KC = 256, smaller ones serially with KC = 384.
+inline int reference_kc(long long work) { return work >= (1LL << 24) ? 256 : 384; }
 
 struct Context {
     int device = 0;
