@@ -1,0 +1,325 @@
+"""Benchmark: batched complex matrix exponential over a frequency sweep.
+
+Workload (one "step"): exp(A_k) for a sweep of 256 complex matrices
+A_k = -(G_k + i w_k C_k), orders n_k uniform in [64, 1024], G_k nonsymmetric
+N(0,1)/sqrt(n), C_k = Q^T D Q SPD with D log-uniform in [1e-3, 1], w_k
+log-spaced 1e2..1e6 -- seeded synthetic data with the shapes and value
+distributions of the batching configuration. Metric: expm/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank runs its own sweep
+(weak scaling, independent matrices, no collective on the data path); the
+time is the max over ranks.
+
+`value` has the inputs resident in HBM (device entry point); `e2e` goes
+through the host-buffer entry point with pinned buffers, so every step copies
+each matrix in and each exponential out. The roofline figure is the DMMA GEMM
+kernel's algorithmic FLOP rate (CUDA events on the library's stream) against
+cuBLAS DGEMM measured in the same process. `--impl reference` times the CPU
+restatement of the reference's algorithm (the oracle) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched complex expm/s: split-prec vs plain FP64 GPU at ≤1e-12 rel err; vs CPU"
+WORKLOAD = ("frequency sweep of 256 complex128 matrices A_k = -(G + i w_k C), n_k ~ U{64..1024}, "
+            "G ~ N(0,1)/sqrt(n), C = Q^T D Q (D log-uniform [1e-3,1]), w_k log-spaced 1e2..1e6; Expm of each")
+
+
+def make_sweep(count: int, seed: int):
+    """The seeded synthetic sweep: list of (n, complex128 Fortran array)."""
+    rng = np.random.default_rng(seed)
+    orders = rng.integers(64, 1025, size=count)
+    omegas = np.logspace(2.0, 6.0, count)
+    mats = []
+    for n, w in zip(orders, omegas):
+        n = int(n)
+        g = rng.standard_normal((n, n)) / math.sqrt(n)
+        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        d = np.exp(rng.uniform(math.log(1e-3), 0.0, n))
+        c = (q.T * d) @ q
+        c = 0.5 * (c + c.T)
+        mats.append(np.asfortranarray(-(g + 1j * w * c)))
+    return [int(n) for n in orders], mats
+
+
+def cpu_sample(orders, budget):
+    """Indices of a bounded, representative CPU sample: sweep order until the
+    summed n^3 reaches `budget`."""
+    idx, acc = [], 0.0
+    for i, n in enumerate(orders):
+        idx.append(i)
+        acc += float(n) ** 3
+        if acc >= budget:
+            break
+    return idx
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reference_arm(args, world, rank):
+    """The reference's algorithm on the host cores (the oracle restatement)."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    oracle.lib()
+    threads = oracle.threads()
+    orders, mats = make_sweep(args.count, args.seed)
+    sample = cpu_sample(orders, args.ref_budget)
+    def step():
+        for i in sample:
+            oracle.expm(mats[i])
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = len(sample) / dt
+    line = {"metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic, seeded",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "count": args.count, "seed": args.seed,
+                       "sample": f"first {len(sample)} matrices of the sweep per step (sum n^3 >= {args.ref_budget:.1e})"},
+            "cpu_baseline": {"value": value, "unit": "expm/s", "cores": threads, "kind": "port",
+                             "sample": f"first {len(sample)} matrices of the sweep, orders {[orders[i] for i in sample]}"},
+            "e2e": {"value": value, "unit": "expm/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def measured_fp64_peak(torch):
+    """cuBLAS DGEMM TFLOP/s (burst) on this GPU, the FP64 denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def ours(args, world, rank, local, dist):
+    import torch
+    torch.cuda.set_device(local)
+    from csharp_linearalgebra_b200 import Workspace
+
+    peak = measured_fp64_peak(torch)
+    orders, mats = make_sweep(args.count, args.seed + 1000 * rank)
+    count = len(mats)
+    # device-resident inputs and outputs
+    dev_in = [torch.from_numpy(m.T.copy()).to("cuda") for m in mats]  # row-major of A^T == column-major A
+    dev_out = [torch.empty_like(t) for t in dev_in]
+    a_ptrs = [t.data_ptr() for t in dev_in]
+    o_ptrs = [t.data_ptr() for t in dev_out]
+    in_bytes = sum(n * n * 16 for n in orders)
+    # pinned host buffers for the end-to-end path
+    host_in = [torch.from_numpy(m.T.copy()).pin_memory() for m in mats]
+    host_out = [torch.empty_like(t).pin_memory() for t in host_in]
+    hi_ptrs = [t.data_ptr() for t in host_in]
+    ho_ptrs = [t.data_ptr() for t in host_out]
+
+    ws = Workspace(local)
+    stream = torch.cuda.ExternalStream(ws.stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def step_device():
+        return ws.expm_batched_device(count, orders, a_ptrs, orders, o_ptrs, orders)
+
+    for _ in range(args.warmup):
+        diags = step_device()
+    torch.cuda.synchronize()
+
+    # timed region, inputs resident in HBM
+    ws.reset_stats()
+    ws.set_timing(True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            diags = step_device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    ws.set_timing(False)
+    st = ws.stats()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * count / (ms * 1e-3)
+
+    # end to end through the host-buffer entry point
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * count / (ms_e2e * 1e-3)
+
+    # CPU baseline (rank 0, N = 1 only): the oracle on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+        oracle.lib()
+        sample = cpu_sample(orders, args.cpu_budget)
+        t0 = time.perf_counter()
+        for i in sample:
+            oracle.expm(mats[i])
+        dt = time.perf_counter() - t0
+        cpu = {"value": len(sample) / dt, "unit": "expm/s", "cores": oracle.threads(), "kind": "port",
+               "sample": f"first {len(sample)} matrices of this sweep (orders {[orders[i] for i in sample]}), "
+                         f"{dt:.1f} s, C++ restatement of the reference, all host threads"}
+
+    achieved = st["gemm_flops"] / (st["gemm_ms"] * 1e-3) / 1e12 if st["gemm_ms"] > 0 else None
+    degrees = sorted(set((d.degree, d.squarings) for d in diags))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (complex128, FP64 DMMA)", "data": "synthetic, seeded",
+            "config": {"workload": WORKLOAD, "count": count, "seed": args.seed, "form": "plain FP64 (DMMA)",
+                       "l2": f"inputs larger than L2: {in_bytes / 1e9:.2f} GB of matrices per step per GPU",
+                       "parallelism": f"independent matrices; {world} rank(s), each its own sweep",
+                       "squarings_range": [min(s for _, s in degrees), max(s for _, s in degrees)]},
+            "e2e": {"value": e2e_value, "unit": "expm/s", "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": in_bytes},
+            "roofline": {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA, complex 4M)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (MEASURED_PEAKS.json has no FP64 figure)",
+                         "traffic": None,
+                         "gemm_share_of_step": st["gemm_ms"] / (ms * args.steps) if ms > 0 else None},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": int(st["kernel_launches"]),
+        }
+        print(json.dumps(line), flush=True)
+    ws.dispose()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--count", type=int, default=256)
+    p.add_argument("--seed", type=int, default=20260915)
+    p.add_argument("--cpu-budget", type=float, default=6e9, help="sum of n^3 in the CPU-baseline sample")
+    p.add_argument("--ref-budget", type=float, default=2e9, help="sum of n^3 per reference-arm step")
+    p.add_argument("--no-cpu", action="store_true")
+    args = p.parse_args()
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        else:
+            ours(args, world, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -148,6 +148,49 @@ class Workspace:
     def set_max_elements(self, value: int):
         self._call("tns_set_max_elements", int(value))
 
+    # -- diagnostics --------------------------------------------------------
+    def stats(self) -> dict:
+        s = N.Stats()
+        self._call("tns_get_stats", C.byref(s))
+        return {k: getattr(s, k) for k, _ in N.Stats._fields_}
+
+    def reset_stats(self):
+        self._call("tns_reset_stats")
+
+    def set_timing(self, enabled: bool):
+        self._call("tns_set_timing", int(bool(enabled)))
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t this workspace issues its work on."""
+        s = C.c_void_p()
+        self._call("tns_get_stream", C.byref(s))
+        return s.value or 0
+
+    def expm_batched_device(self, count, orders, a_ptrs, lds, out_ptrs, ldos):
+        """Batched complex exp over device-resident matrices (raw device
+        pointers, e.g. from torch tensors). Returns the diagnostics."""
+        orders_c = (C.c_int * count)(*orders)
+        lda_c = (C.c_int * count)(*lds)
+        ldo_c = (C.c_int * count)(*ldos)
+        ap = (C.c_void_p * count)(*a_ptrs)
+        op = (C.c_void_p * count)(*out_ptrs)
+        infos = (N.ExpmInfo * count)()
+        self._call("tns_zexpm_batched_device", count, orders_c, ap, lda_c, op, ldo_c, infos)
+        return [ExpmDiagnostics(i.degree, i.squarings) for i in infos]
+
+    def expm_batched_host(self, count, orders, a_ptrs, lds, out_ptrs, ldos):
+        """Batched complex exp over host buffers given by address (pinned or
+        pageable); the copies to and from the device happen inside the call."""
+        orders_c = (C.c_int * count)(*orders)
+        lda_c = (C.c_int * count)(*lds)
+        ldo_c = (C.c_int * count)(*ldos)
+        ap = (C.c_void_p * count)(*a_ptrs)
+        op = (C.c_void_p * count)(*out_ptrs)
+        infos = (N.ExpmInfo * count)()
+        self._call("tns_zexpm_batched", count, orders_c, ap, lda_c, op, ldo_c, infos)
+        return [ExpmDiagnostics(i.degree, i.squarings) for i in infos]
+
     # -- products -----------------------------------------------------------
     def multiply(self, a, b, c=None, alpha=1.0, beta=0.0):
         """C := beta*C + alpha*A*B (Workspace.Multiply). Returns C."""

@@ -42,6 +42,11 @@ class ExpmvInfo(C.Structure):
                 ("early_exits", C.c_int)]
 
 
+class Stats(C.Structure):
+    _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
+                ("gemm_flops", C.c_double), ("gemm_ms", C.c_double)]
+
+
 # name -> (restype, argtypes)
 _P, _I, _D, _LL, _CH = C.c_void_p, C.c_int, C.c_double, C.c_longlong, C.c_char
 SIGNATURES = {
@@ -69,6 +74,10 @@ SIGNATURES = {
     "tns_zexpm_batched_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "tns_dexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_get_stats": (_I, [_P, C.POINTER(Stats)]),
+    "tns_reset_stats": (_I, [_P]),
+    "tns_set_timing": (_I, [_P, _I]),
+    "tns_get_stream": (_I, [_P, C.POINTER(_P)]),
 }
 
 _lib = None

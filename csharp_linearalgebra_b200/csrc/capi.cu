@@ -416,6 +416,35 @@ int tns_zexpm_batched_device(tns_context* c, int count, const int* orders, const
                              double* const* out, const int* ldo, tns_expm_info* infos) {
     return zexpm_batched_entry(c, true, count, orders, a, lda, out, ldo, infos);
 }
+int tns_get_stats(tns_context* c, tns_stats* out) {
+    return guarded(c, [&](Context& ctx) {
+        require(out != nullptr, TNS_E_NULL, "out is null");
+        ctx.drain_events();
+        out->kernel_launches = ctx.kernel_launches;
+        out->gemm_launches = ctx.gemm_launches;
+        out->gemm_flops = ctx.gemm_flops;
+        out->gemm_ms = ctx.gemm_ms_done;
+    });
+}
+int tns_reset_stats(tns_context* c) {
+    return guarded(c, [&](Context& ctx) {
+        ctx.drain_events();
+        ctx.kernel_launches = 0;
+        ctx.gemm_launches = 0;
+        ctx.gemm_flops = 0.0;
+        ctx.gemm_ms_done = 0.0;
+    });
+}
+int tns_set_timing(tns_context* c, int enabled) {
+    return guarded(c, [&](Context& ctx) { ctx.timing = enabled != 0; });
+}
+int tns_get_stream(tns_context* c, void** stream) {
+    return guarded(c, [&](Context& ctx) {
+        require(stream != nullptr, TNS_E_NULL, "stream is null");
+        *stream = reinterpret_cast<void*>(ctx.stream);
+    });
+}
+
 int tns_dexpmv(tns_context* c, int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
                double* out, int ldo, tns_expmv_info* info) {
     return expmv_entry(c, false, n, a, lda, ncols, b, ldb, t, out, ldo, info);

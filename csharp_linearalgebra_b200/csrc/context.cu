@@ -30,9 +30,38 @@ Context::Context(int dev) : device(dev) {
     TNS_CUDA(cudaMemset(d_err, 0, sizeof(int)));
 }
 
+cudaEvent_t Context::take_event() {
+    if (event_pool.empty()) {
+        cudaEvent_t e;
+        TNS_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    cudaEvent_t e = event_pool.back();
+    event_pool.pop_back();
+    return e;
+}
+
+void Context::drain_events() {
+    if (gemm_events.empty()) return;
+    TNS_CUDA(cudaStreamSynchronize(stream));
+    for (auto& pr : gemm_events) {
+        float ms = 0.f;
+        TNS_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        gemm_ms_done += ms;
+        event_pool.push_back(pr.first);
+        event_pool.push_back(pr.second);
+    }
+    gemm_events.clear();
+}
+
 Context::~Context() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    for (auto& pr : gemm_events) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
     if (d_probs) cudaFree(d_probs);
     if (d_err) cudaFree(d_err);
     if (stream) cudaStreamDestroy(stream);

@@ -370,9 +370,22 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     int ctas_per_sm = 1;
     TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
     int grid = std::min(total, std::max(1, ctas_per_sm) * ctx.num_sms);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx.timing) {
+        e0 = ctx.take_event();
+        e1 = ctx.take_event();
+        TNS_CUDA(cudaEventRecord(e0, ctx.stream));
+    }
     gemm_dmma_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, ctx.stream>>>(L);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
+    ctx.gemm_launches++;
+    for (auto& p : probs) ctx.gemm_flops += (Cfg::kComplex ? 8.0 : 2.0) * (double)(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
+    if (ctx.timing) {
+        TNS_CUDA(cudaEventRecord(e1, ctx.stream));
+        ctx.gemm_events.emplace_back(e0, e1);
+        if (ctx.gemm_events.size() > 4096) ctx.drain_events();
+    }
 }
 
 void check_problem(const GemmProblem& p, bool cplx) {

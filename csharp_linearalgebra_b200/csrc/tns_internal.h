@@ -75,6 +75,17 @@ struct Context {
     GemmProblem* d_probs = nullptr;
     size_t d_probs_cap = 0;
 
+    // Optional per-launch timing of the GEMM kernel (CUDA events on this
+    // context's stream), for the roofline report.
+    bool timing = false;
+    long long gemm_launches = 0;
+    double gemm_flops = 0.0;  // algorithmic: 2mnk real, 8mnk complex (4M), true sizes
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_events;
+    std::vector<cudaEvent_t> event_pool;
+    double gemm_ms_done = 0.0;  // elapsed time of events already drained
+    cudaEvent_t take_event();
+    void drain_events();        // sums finished event pairs into gemm_ms_done
+
     explicit Context(int dev);
     ~Context();
     GemmProblem* upload_problems(const std::vector<GemmProblem>& probs);

@@ -183,6 +183,27 @@ int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, con
 int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
                double t, double* out, int ldo, tns_expmv_info* info);
 
+/* ---- diagnostics --------------------------------------------------------- */
+
+/* Counters of the work a context has issued, the device-side counterpart of
+ * the reference's LuPhaseTimings / ExpmDiagnostics observers
+ * (src/Tensile.Kernels/Lu.cs:92-164, src/Tensile/MatrixExponential.cs:575-582).
+ * gemm_ms is the summed CUDA-event duration of the GEMM kernel launches made
+ * while timing was enabled; gemm_flops counts 2mnk (real) or 8mnk (complex 4M)
+ * at the products' true sizes. */
+typedef struct {
+    long long kernel_launches; /* every kernel this context launched */
+    long long gemm_launches;
+    double gemm_flops;
+    double gemm_ms;
+} tns_stats;
+
+int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
+int tns_reset_stats(tns_context* ctx);
+int tns_set_timing(tns_context* ctx, int enabled);
+/* The CUDA stream (cudaStream_t) the context issues its work on. */
+int tns_get_stream(tns_context* ctx, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

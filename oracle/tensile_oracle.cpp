@@ -25,6 +25,8 @@
 #include <utility>
 #include <vector>
 
+#include <immintrin.h>
+
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -289,18 +291,56 @@ int threads_now() {
 // ===========================================================================
 constexpr int MR = 8, NR = 6, MC = 144, NC = 4096;
 
+// The 8x6 AVX2/FMA register tile (the reference's Avx2Kernel8x6 geometry):
+// 12 accumulators, each lane a k-ordered fused multiply-add chain.
 inline void micro_kernel(int kc, double alpha, const double* ap, const double* bp, double* c,
                          int ldc, int mrb, int nrb) {
-    double acc[NR][MR];
-    for (int j = 0; j < NR; j++)
-        for (int i = 0; i < MR; i++) acc[j][i] = 0.0;
+    __m256d c00 = _mm256_setzero_pd(), c10 = _mm256_setzero_pd();
+    __m256d c01 = _mm256_setzero_pd(), c11 = _mm256_setzero_pd();
+    __m256d c02 = _mm256_setzero_pd(), c12 = _mm256_setzero_pd();
+    __m256d c03 = _mm256_setzero_pd(), c13 = _mm256_setzero_pd();
+    __m256d c04 = _mm256_setzero_pd(), c14 = _mm256_setzero_pd();
+    __m256d c05 = _mm256_setzero_pd(), c15 = _mm256_setzero_pd();
     for (int p = 0; p < kc; p++) {
-        const double* a = ap + p * MR;
-        const double* b = bp + p * NR;
+        __m256d a0 = _mm256_loadu_pd(ap);
+        __m256d a1 = _mm256_loadu_pd(ap + 4);
+        ap += MR;
+        __m256d b;
+        b = _mm256_broadcast_sd(bp + 0);
+        c00 = _mm256_fmadd_pd(a0, b, c00);
+        c10 = _mm256_fmadd_pd(a1, b, c10);
+        b = _mm256_broadcast_sd(bp + 1);
+        c01 = _mm256_fmadd_pd(a0, b, c01);
+        c11 = _mm256_fmadd_pd(a1, b, c11);
+        b = _mm256_broadcast_sd(bp + 2);
+        c02 = _mm256_fmadd_pd(a0, b, c02);
+        c12 = _mm256_fmadd_pd(a1, b, c12);
+        b = _mm256_broadcast_sd(bp + 3);
+        c03 = _mm256_fmadd_pd(a0, b, c03);
+        c13 = _mm256_fmadd_pd(a1, b, c13);
+        b = _mm256_broadcast_sd(bp + 4);
+        c04 = _mm256_fmadd_pd(a0, b, c04);
+        c14 = _mm256_fmadd_pd(a1, b, c14);
+        b = _mm256_broadcast_sd(bp + 5);
+        c05 = _mm256_fmadd_pd(a0, b, c05);
+        c15 = _mm256_fmadd_pd(a1, b, c15);
+        bp += NR;
+    }
+    __m256d lo[NR] = {c00, c01, c02, c03, c04, c05};
+    __m256d hi[NR] = {c10, c11, c12, c13, c14, c15};
+    __m256d va = _mm256_set1_pd(alpha);
+    if (mrb == MR && nrb == NR) {
         for (int j = 0; j < NR; j++) {
-            double bj = b[j];
-            for (int i = 0; i < MR; i++) acc[j][i] = __builtin_fma(a[i], bj, acc[j][i]);
+            double* col = c + (size_t)j * ldc;
+            _mm256_storeu_pd(col, _mm256_fmadd_pd(va, lo[j], _mm256_loadu_pd(col)));
+            _mm256_storeu_pd(col + 4, _mm256_fmadd_pd(va, hi[j], _mm256_loadu_pd(col + 4)));
         }
+        return;
+    }
+    alignas(32) double acc[NR][MR];
+    for (int j = 0; j < NR; j++) {
+        _mm256_store_pd(&acc[j][0], lo[j]);
+        _mm256_store_pd(&acc[j][4], hi[j]);
     }
     for (int j = 0; j < nrb; j++) {
         double* col = c + (size_t)j * ldc;

@@ -18,6 +18,8 @@ def test_dgemm_matches_oracle(ws, orc, m, n, k):
     c = ws.multiply(a, b)
     ref = orc.gemm(a, b)
     assert relfro(c, ref) < 1e-13
+    # DMMA accumulates as the reference's FMA chain and the fold points match its KC slabs
+    assert np.array_equal(c, ref)
 
 
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (1.0, 1.0), (-1.0, 1.0), (0.0, 1.0), (2.5, -0.5)])
@@ -28,6 +30,8 @@ def test_dgemm_alpha_beta(ws, orc, alpha, beta):
     c = ws.multiply(a, b, c0, alpha, beta)
     ref = orc.gemm(a, b, c0, alpha, beta)
     assert relfro(c, ref) < 1e-13
+    # DMMA accumulates as the reference's FMA chain and the fold points match its KC slabs
+    assert np.array_equal(c, ref)
 
 
 def test_beta_zero_overwrites_nan(ws):
@@ -61,6 +65,8 @@ def test_zgemm_matches_oracle(ws, orc, m, n, k):
     c = ws.multiply(a, b)
     ref = orc.gemm(a, b)
     assert relfro(c, ref) < 1e-13
+    # DMMA accumulates as the reference's FMA chain and the fold points match its KC slabs
+    assert np.array_equal(c, ref)
 
 
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (1.0, 1.0), (-1.0, 1.0), (2.0 - 1.0j, 0.5 + 0.25j)])
@@ -72,6 +78,8 @@ def test_zgemm_alpha_beta(ws, orc, alpha, beta):
     c = ws.multiply(a, b, c0, complex(alpha), complex(beta))
     ref = orc.gemm(a, b, c0, complex(alpha), complex(beta))
     assert relfro(c, ref) < 1e-13
+    # DMMA accumulates as the reference's FMA chain and the fold points match its KC slabs
+    assert np.array_equal(c, ref)
 
 
 def test_4m_keeps_small_imaginary_parts(ws, orc):

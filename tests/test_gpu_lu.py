@@ -21,6 +21,7 @@ def test_real_lu_matches_oracle(ws, orc, m, n, nb):
     assert np.array_equal(lu.pivots, piv)
     assert lu.singular_column == info["singular_column"] == -1
     assert relfro(lu.factors, f) < 1e-12
+    assert np.array_equal(lu.factors, f)  # bit for bit
     assert lu.smallest_pivot == pytest.approx(info["smallest_pivot"], rel=1e-12)
     assert lu.largest_pivot == pytest.approx(info["largest_pivot"], rel=1e-12)
 
@@ -33,6 +34,7 @@ def test_complex_lu_matches_oracle(ws, orc, m, n):
     f, piv, info = orc.getrf(a)
     assert np.array_equal(lu.pivots, piv)
     assert relfro(lu.factors, f) < 1e-12
+    assert np.array_equal(lu.factors, f)  # bit for bit
 
 
 def test_pivot_maximises_sum_of_absolute_parts(ws):
