@@ -190,7 +190,7 @@ def ours(args, world, rank, local, dist):
     torch.cuda.set_device(local)
     from csharp_linearalgebra_b200 import Workspace
 
-    peak = measured_fp64_peak(torch)
+    peak = None if args.no_peak else measured_fp64_peak(torch)
     orders, mats = make_sweep(args.count, args.seed + 1000 * rank)
     count = len(mats)
     # device-resident inputs and outputs
@@ -242,20 +242,22 @@ def ours(args, world, rank, local, dist):
     value = world * count / (ms * 1e-3)
 
     # end to end through the host-buffer entry point
-    barrier()
-    torch.cuda.synchronize()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = e2.elapsed_time(e3) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e_value = world * count / (ms_e2e * 1e-3)
+    e2e_value = None
+    if not args.no_e2e:
+        barrier()
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e2.elapsed_time(e3) / args.steps
+        if dist is not None:
+            t = torch.tensor([ms_e2e], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        e2e_value = world * count / (ms_e2e * 1e-3)
 
     # CPU baseline (rank 0, N = 1 only): the oracle on a bounded sample
     cpu = None
@@ -286,7 +288,7 @@ def ours(args, world, rank, local, dist):
                     "d2h_bytes_per_step": in_bytes},
             "roofline": {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA, complex 4M)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if achieved else None,
+                         "frac": (achieved / peak) if (achieved and peak) else None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (MEASURED_PEAKS.json has no FP64 figure)",
                          "traffic": None,
                          "gemm_share_of_step": st["gemm_ms"] / (ms * args.steps) if ms > 0 else None},
@@ -308,7 +310,9 @@ def main():
     p.add_argument("--seed", type=int, default=20260915)
     p.add_argument("--cpu-budget", type=float, default=6e9, help="sum of n^3 in the CPU-baseline sample")
     p.add_argument("--ref-budget", type=float, default=2e9, help="sum of n^3 per reference-arm step")
-    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS DGEMM peak (profiling runs)")
     args = p.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
