@@ -157,6 +157,10 @@ class Workspace:
     def reset_stats(self):
         self._call("tns_reset_stats")
 
+    def set_workers(self, workers: int):
+        """How many matrices of a batch run concurrently (streams)."""
+        self._call("tns_set_workers", int(workers))
+
     def set_timing(self, enabled: bool):
         self._call("tns_set_timing", int(bool(enabled)))
 

@@ -173,121 +173,185 @@ __global__ void fill_kernel(double* p, size_t count, double v) {
         p[e] = v;
 }
 
-// Y := A X, axpy order: y[i] accumulates x[j] * a[i, j] for j = 0..n-1, skipping
-// x[j] == 0 as the reference's PanelProduct.Apply does. Real: one thread per
-// (row, column). Complex operator (LinearOperators.cs:262-282): four real sums
-// pr = Ar*xr, pi = Ar*xi, qr = Ai*xr, qi = Ai*xi, then (pr - qi, pi + qr).
-__global__ void panel_apply_kernel(const double* __restrict__ a, int n, int ld, bool cplx, const double* __restrict__ x,
-                                   int ldx, double* __restrict__ y, int ldy, int t) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int c = blockIdx.y;
-    if (i >= n || c >= t) return;
-    if (!cplx) {
-        const double* xc = x + (size_t)c * ldx;
-        double sum = 0.0;
-        for (int j = 0; j < n; ++j) {
-            double s = xc[j];
-            if (s != 0.0) sum = add_rn(sum, mul_rn(s, a[(size_t)j * ld + i]));
+// Y := A X in the axpy order of PanelProduct.Apply (PanelProduct.cs:25-41):
+// y[i] accumulates x[j] * a[i, j] for j = 0..n-1 with two roundings per term,
+// skipping x[j] == 0. The skip is kept exactly: a skipped term adds +0.0 to a
+// sum that is never -0.0, which changes nothing, and it keeps 0 * inf out.
+// Complex operator (LinearOperators.cs:262-282): four real sums per column,
+// pr = Ar xr, pi = Ar xi, qr = Ai xr, qi = Ai xi, then (pr - qi, pi + qr).
+// One thread per row covers all t <= TMAX columns, so A is read once per
+// product; x is staged through shared memory.
+template <int TMAX, bool CPLX>
+__global__ void __launch_bounds__(128) panel_apply_kernel(const double* __restrict__ a, int n, int ld,
+                                                          const double* __restrict__ x, int ldx,
+                                                          double* __restrict__ y, int ldy, int t) {
+    constexpr int CH = 64;  // rows of x staged per chunk
+    constexpr int ES = CPLX ? 2 : 1;
+    __shared__ double sx[CH * TMAX * ES];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool row_ok = i < n;
+    double acc[TMAX][CPLX ? 4 : 1];
+#pragma unroll
+    for (int c = 0; c < TMAX; ++c)
+#pragma unroll
+        for (int q = 0; q < (CPLX ? 4 : 1); ++q) acc[c][q] = 0.0;
+    for (int j0 = 0; j0 < n; j0 += CH) {
+        const int len = min(CH, n - j0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < len * t * ES; e += blockDim.x) {
+            int c = e / (len * ES), r = e % (len * ES);
+            sx[(c * CH) * ES + r] = x[((size_t)c * ldx + j0) * ES + r];
         }
-        y[(size_t)c * ldy + i] = sum;
-    } else {
-        const double2* xc = reinterpret_cast<const double2*>(x) + (size_t)c * ldx;
-        const double2* A = reinterpret_cast<const double2*>(a);
-        double pr = 0.0, pi = 0.0, qr = 0.0, qi = 0.0;
-        for (int j = 0; j < n; ++j) {
-            double2 s = xc[j];
-            double2 aij = A[(size_t)j * ld + i];
-            if (s.x != 0.0) {
-                pr = add_rn(pr, mul_rn(s.x, aij.x));
-                qr = add_rn(qr, mul_rn(s.x, aij.y));
-            }
-            if (s.y != 0.0) {
-                pi = add_rn(pi, mul_rn(s.y, aij.x));
-                qi = add_rn(qi, mul_rn(s.y, aij.y));
+        __syncthreads();
+        if (!row_ok) continue;
+        for (int jj = 0; jj < len; ++jj) {
+            const size_t idx = (size_t)(j0 + jj) * ld + i;
+            if (!CPLX) {
+                const double aij = a[idx];
+#pragma unroll
+                for (int c = 0; c < TMAX; ++c) {
+                    if (c < t) {
+                        double s = sx[c * CH + jj];
+                        double term = s != 0.0 ? mul_rn(s, aij) : 0.0;
+                        acc[c][0] = add_rn(acc[c][0], term);
+                    }
+                }
+            } else {
+                const double2 aij = reinterpret_cast<const double2*>(a)[idx];
+#pragma unroll
+                for (int c = 0; c < TMAX; ++c) {
+                    if (c < t) {
+                        double sr = sx[(c * CH + jj) * 2], si = sx[(c * CH + jj) * 2 + 1];
+                        bool nr = sr != 0.0, ni = si != 0.0;
+                        acc[c][0] = add_rn(acc[c][0], nr ? mul_rn(sr, aij.x) : 0.0);  // pr
+                        acc[c][2] = add_rn(acc[c][2], nr ? mul_rn(sr, aij.y) : 0.0);  // qr
+                        acc[c][1] = add_rn(acc[c][1], ni ? mul_rn(si, aij.x) : 0.0);  // pi
+                        acc[c][3] = add_rn(acc[c][3], ni ? mul_rn(si, aij.y) : 0.0);  // qi
+                    }
+                }
             }
         }
-        reinterpret_cast<double2*>(y)[(size_t)c * ldy + i] = make_double2(sub_rn(pr, qi), add_rn(pi, qr));
+    }
+    if (!row_ok) return;
+#pragma unroll
+    for (int c = 0; c < TMAX; ++c) {
+        if (c >= t) continue;
+        if (!CPLX) {
+            y[(size_t)c * ldy + i] = acc[c][0];
+        } else {
+            reinterpret_cast<double2*>(y)[(size_t)c * ldy + i] =
+                make_double2(sub_rn(acc[c][0], acc[c][3]), add_rn(acc[c][1], acc[c][2]));
+        }
     }
 }
 
-// ColumnOps.Dot with .NET's 256-bit Vector<double>: partial L (0..15) sums the
-// elements i = L mod 16 below the last full 16-block in index order; then the
-// remaining full 4-blocks go to partials 0..3; s[l] = (a0+a1)+(a2+a3) per lane
-// l; total = (s0+s1)+(s2+s3); then the scalar tail in order. Computed by a
-// half-warp: lane L of the half owns partial L.
-__device__ __forceinline__ double netdot_half(const double* __restrict__ u, const double* __restrict__ v, int n,
-                                              int L, unsigned mask, int src_base) {
+// Lane L (0..15) of a half-warp has accumulated the 16-lane partial sums of
+// .NET's ColumnOps.Dot with 256-bit Vector<double> (ColumnOps.cs:35-65):
+// partial L holds the terms i = L mod 16 below the last whole 16-block, in
+// index order, and partials 0..3 then take the remaining whole 4-blocks.
+// Combine them as the reference does: s[l] = (a0[l] + a1[l]) + (a2[l] + a3[l]),
+// total = (s0 + s1) + (s2 + s3).
+__device__ __forceinline__ double netdot_combine(double acc, int L, int base) {
+    const unsigned mask = 0xffffffffu;
+    double a0 = __shfl_sync(mask, acc, base + (L & 3));
+    double a1 = __shfl_sync(mask, acc, base + 4 + (L & 3));
+    double a2 = __shfl_sync(mask, acc, base + 8 + (L & 3));
+    double a3 = __shfl_sync(mask, acc, base + 12 + (L & 3));
+    double s = add_rn(add_rn(a0, a1), add_rn(a2, a3));
+    double s0 = __shfl_sync(mask, s, base + 0);
+    double s1 = __shfl_sync(mask, s, base + 1);
+    double s2 = __shfl_sync(mask, s, base + 2);
+    double s3 = __shfl_sync(mask, s, base + 3);
+    return add_rn(add_rn(s0, s1), add_rn(s2, s3));
+}
+
+// Y := A^T X (real) or A^H X (complex operator: pr = Ar^T xr, pi = Ar^T xi,
+// qr = Ai^T xr, qi = Ai^T xi, then (pr + qi, pi - qr)), PanelProduct.ApplyTranspose
+// (PanelProduct.cs:44-55): y[j] = Dot(a[:, j], x) in ColumnOps.Dot's order.
+// One half-warp per output row j, covering all t <= TMAX columns, reading the
+// interleaved complex data directly.
+template <int TMAX, bool CPLX>
+__global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld, const double* __restrict__ x,
+                                     int ldx, double* __restrict__ y, int ldy, int t) {
+    constexpr int NQ = CPLX ? 4 : 1;
+    const long long half = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const int L = threadIdx.x & 15;
+    const int base = threadIdx.x & 16;  // lane offset of this half in the warp
+    // Inactive halves compute row 0 and drop it, so every shuffle sees a
+    // converged warp.
+    const bool active = half < n;
+    const int j = active ? (int)half : 0;
+    double acc[TMAX][NQ];
+#pragma unroll
+    for (int c = 0; c < TMAX; ++c)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) acc[c][q] = 0.0;
     const int W = 4;
-    double total = 0.0;
-    int i16 = 0;
+    const int n16 = (n / (4 * W)) * (4 * W);
+    const int n4 = n >= W ? n16 + ((n - n16) / W) * W : 0;
+    auto add_term = [&](int i) {
+        if (!CPLX) {
+            double aij = a[(size_t)j * ld + i];
+#pragma unroll
+            for (int c = 0; c < TMAX; ++c)
+                if (c < t) acc[c][0] = add_rn(acc[c][0], mul_rn(aij, x[(size_t)c * ldx + i]));
+        } else {
+            double2 aij = reinterpret_cast<const double2*>(a)[(size_t)j * ld + i];
+#pragma unroll
+            for (int c = 0; c < TMAX; ++c)
+                if (c < t) {
+                    double2 xc = reinterpret_cast<const double2*>(x)[(size_t)c * ldx + i];
+                    acc[c][0] = add_rn(acc[c][0], mul_rn(aij.x, xc.x));  // pr
+                    acc[c][1] = add_rn(acc[c][1], mul_rn(aij.x, xc.y));  // pi
+                    acc[c][2] = add_rn(acc[c][2], mul_rn(aij.y, xc.x));  // qr
+                    acc[c][3] = add_rn(acc[c][3], mul_rn(aij.y, xc.y));  // qi
+                }
+        }
+    };
+    double res[TMAX][NQ];
     if (n >= W) {
-        int n16 = (n / (4 * W)) * (4 * W);
-        double acc = 0.0;
-        for (int i = L; i < n16; i += 16) acc = add_rn(acc, mul_rn(u[i], v[i]));
-        // remaining whole 4-blocks into a0 (partials 0..3)
-        int n4 = n16 + ((n - n16) / W) * W;
+        for (int i = L; i < n16; i += 16) add_term(i);
         if (L < W)
-            for (int i = n16 + L; i < n4; i += W) acc = add_rn(acc, mul_rn(u[i], v[i]));
-        i16 = n4;
-        // combine: s[l] = (a0[l]+a1[l]) + (a2[l]+a3[l]) where a_k[l] is partial 4k+l
-        double a0 = __shfl_sync(mask, acc, src_base + (L & 3));
-        double a1 = __shfl_sync(mask, acc, src_base + 4 + (L & 3));
-        double a2 = __shfl_sync(mask, acc, src_base + 8 + (L & 3));
-        double a3 = __shfl_sync(mask, acc, src_base + 12 + (L & 3));
-        double s = add_rn(add_rn(a0, a1), add_rn(a2, a3));
-        double s0 = __shfl_sync(mask, s, src_base + 0);
-        double s1 = __shfl_sync(mask, s, src_base + 1);
-        double s2 = __shfl_sync(mask, s, src_base + 2);
-        double s3 = __shfl_sync(mask, s, src_base + 3);
-        total = add_rn(add_rn(s0, s1), add_rn(s2, s3));
-    }
-    for (int i = i16; i < n; ++i) total = add_rn(total, mul_rn(u[i], v[i]));
-    return total;
-}
-
-// Y := A^T X (real) or A^H X (complex operator: pr = Ar^T xr etc., then
-// (pr + qi, pi - qr)). One half-warp per (output row j, column c).
-__global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld, bool cplx, const double* __restrict__ x,
-                                     int ldx, double* __restrict__ y, int ldy, int t, double* __restrict__ scratch) {
-    long long half = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
-    int L = threadIdx.x & 15;
-    int lane = threadIdx.x & 31;
-    int src_base = lane & 16;
-    // Every lane runs the same dot (inactive halves on row 0, column 0, result
-    // dropped) so that the shuffles inside see a converged warp.
-    bool active = half < (long long)n * t;
-    int j = active ? (int)(half % n) : 0;
-    int c = active ? (int)(half / n) : 0;
-    unsigned mask = 0xffffffffu;
-    if (!cplx) {
-        double r = netdot_half(a + (size_t)j * ld, x + (size_t)c * ldx, n, L, mask, src_base);
-        if (active && L == 0) y[(size_t)c * ldy + j] = r;
+            for (int i = n16 + L; i < n4; i += W) add_term(i);
+#pragma unroll
+        for (int c = 0; c < TMAX; ++c)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) res[c][q] = netdot_combine(acc[c][q], L, base);
     } else {
-        // The split parts of A and of x live in scratch (planar), so the dots
-        // read contiguous doubles: [Ar | Ai] (n x n each, ld n), then [xr | xi]
-        // (n x t each).
-        const double* Ar = scratch;
-        const double* Ai = scratch + (size_t)n * n;
-        const double* xr = scratch + 2 * (size_t)n * n;
-        const double* xi = xr + (size_t)n * t;
-        double pr = netdot_half(Ar + (size_t)j * n, xr + (size_t)c * n, n, L, mask, src_base);
-        double pi = netdot_half(Ar + (size_t)j * n, xi + (size_t)c * n, n, L, mask, src_base);
-        double qr = netdot_half(Ai + (size_t)j * n, xr + (size_t)c * n, n, L, mask, src_base);
-        double qi = netdot_half(Ai + (size_t)j * n, xi + (size_t)c * n, n, L, mask, src_base);
-        if (active && L == 0)
-            reinterpret_cast<double2*>(y)[(size_t)c * ldy + j] = make_double2(add_rn(pr, qi), sub_rn(pi, qr));
+#pragma unroll
+        for (int c = 0; c < TMAX; ++c)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) res[c][q] = 0.0;
     }
-}
-
-// Planar split of an interleaved rows x cols block (ld) into compact re / im.
-__global__ void split_planar_kernel(const double* __restrict__ a, int rows, int cols, int ld, double* __restrict__ re,
-                                    double* __restrict__ im) {
-    size_t total = (size_t)rows * cols;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(e % rows), j = (int)(e / rows);
-        double2 z = reinterpret_cast<const double2*>(a)[(size_t)j * ld + i];
-        re[e] = z.x;
-        im[e] = z.y;
+    if (!active || L != 0) return;
+    // scalar tail, in order, by one lane
+    for (int i = n4; i < n; ++i) {
+        if (!CPLX) {
+            double aij = a[(size_t)j * ld + i];
+#pragma unroll
+            for (int c = 0; c < TMAX; ++c)
+                if (c < t) res[c][0] = add_rn(res[c][0], mul_rn(aij, x[(size_t)c * ldx + i]));
+        } else {
+            double2 aij = reinterpret_cast<const double2*>(a)[(size_t)j * ld + i];
+#pragma unroll
+            for (int c = 0; c < TMAX; ++c)
+                if (c < t) {
+                    double2 xc = reinterpret_cast<const double2*>(x)[(size_t)c * ldx + i];
+                    res[c][0] = add_rn(res[c][0], mul_rn(aij.x, xc.x));
+                    res[c][1] = add_rn(res[c][1], mul_rn(aij.x, xc.y));
+                    res[c][2] = add_rn(res[c][2], mul_rn(aij.y, xc.x));
+                    res[c][3] = add_rn(res[c][3], mul_rn(aij.y, xc.y));
+                }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < TMAX; ++c) {
+        if (c >= t) continue;
+        if (!CPLX)
+            y[(size_t)c * ldy + j] = res[c][0];
+        else
+            reinterpret_cast<double2*>(y)[(size_t)c * ldy + j] =
+                make_double2(add_rn(res[c][0], res[c][3]), sub_rn(res[c][1], res[c][2]));
     }
 }
 
@@ -423,31 +487,41 @@ double one_norm_abs_power(Context& ctx, const DMat& a, int p) {
     return fetch_scalar(ctx, vecs.as<double>() + 2 * (size_t)n);
 }
 
-void panel_product(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
+namespace {
+template <int TMAX, bool CPLX>
+void launch_panel(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
     int n = a.rows;
-    if (n == 0 || t == 0) return;
     if (!adjoint) {
-        dim3 grid((n + 127) / 128, t);
-        panel_apply_kernel<<<grid, 128, 0, ctx.stream>>>(a.p, n, a.ld(), a.cplx, x, ldx, y, ldy, t);
-        TNS_CUDA(cudaGetLastError());
-        ctx.kernel_launches++;
-        return;
-    }
-    long long halves = (long long)n * t;
-    int blocks = (int)((halves * 16 + 255) / 256);
-    if (!a.cplx) {
-        panel_apply_t_kernel<<<blocks, 256, 0, ctx.stream>>>(a.p, n, a.ld(), false, x, ldx, y, ldy, t, nullptr);
-        ctx.kernel_launches++;
+        panel_apply_kernel<TMAX, CPLX><<<(n + 127) / 128, 128, 0, ctx.stream>>>(a.p, n, a.ld(), x, ldx, y, ldy, t);
     } else {
-        DBuf scratch(ctx, sizeof(double) * (2 * (size_t)n * n + 2 * (size_t)n * t));
-        double* s = scratch.as<double>();
-        split_planar_kernel<<<blocks_for((long long)n * n), kThreads, 0, ctx.stream>>>(a.p, n, n, a.ld(), s, s + (size_t)n * n);
-        split_planar_kernel<<<blocks_for((long long)n * t), kThreads, 0, ctx.stream>>>(
-            x, n, t, ldx, s + 2 * (size_t)n * n, s + 2 * (size_t)n * n + (size_t)n * t);
-        panel_apply_t_kernel<<<blocks, 256, 0, ctx.stream>>>(a.p, n, a.ld(), true, x, ldx, y, ldy, t, s);
-        ctx.kernel_launches += 3;
+        long long threads = (long long)n * 16;
+        panel_apply_t_kernel<TMAX, CPLX><<<(int)((threads + 255) / 256), 256, 0, ctx.stream>>>(a.p, n, a.ld(), x, ldx, y,
+                                                                                               ldy, t);
     }
     TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
+template <bool CPLX>
+void panel_dispatch(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
+    if (t <= 2) launch_panel<2, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
+    else if (t <= 4) launch_panel<4, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
+    else if (t <= 8) launch_panel<8, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
+    else launch_panel<16, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
+}
+}  // namespace
+
+void panel_product(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
+    if (a.rows == 0 || t == 0) return;
+    // Wider panels run as successive blocks of 16 columns; each column's
+    // arithmetic is independent of the others.
+    for (int c0 = 0; c0 < t; c0 += 16) {
+        int tc = std::min(16, t - c0);
+        size_t es = a.cplx ? 2 : 1;
+        const double* xc = x + (size_t)c0 * ldx * es;
+        double* yc = y + (size_t)c0 * ldy * es;
+        if (a.cplx) panel_dispatch<true>(ctx, a, xc, ldx, yc, ldy, tc, adjoint);
+        else panel_dispatch<false>(ctx, a, xc, ldx, yc, ldy, tc, adjoint);
+    }
 }
 
 void shift_diagonal(Context& ctx, DMat& a, double dre, double dim) {

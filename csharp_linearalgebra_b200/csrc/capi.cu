@@ -6,9 +6,12 @@
 #include "tns_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <sstream>
+#include <thread>
 #include <vector>
 
 struct tns_context {
@@ -277,31 +280,113 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             check_operand(a[i], orders[i], orders[i], lda[i], "A[i]");
             check_operand(out[i], orders[i], orders[i], ldo[i], "out[i]");
         }
-        for (int i = 0; i < count; ++i) {
+        // Largest first (longest-processing-time order), so that the tail of
+        // the batch is made of short jobs.
+        std::vector<int> order(count);
+        for (int i = 0; i < count; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return orders[x] > orders[y]; });
+        std::vector<tns_expm_info> results(count, tns_expm_info{0, 0});
+
+        auto run_one = [&](Context& wc, int i) {
             int n = orders[i];
-            tns_expm_info inf{0, 0};
             if (n == 1) {
+                double h[2], r[2];
                 if (dev) {
-                    double h[2], r[2];
-                    TNS_CUDA(cudaMemcpy(h, a[i], 16, cudaMemcpyDeviceToHost));
+                    TNS_CUDA(cudaMemcpyAsync(h, a[i], 16, cudaMemcpyDeviceToHost, wc.stream));
+                    wc.sync();
                     scalar_exp(h, r, true);
-                    TNS_CUDA(cudaMemcpy(out[i], r, 16, cudaMemcpyHostToDevice));
+                    TNS_CUDA(cudaMemcpyAsync(out[i], r, 16, cudaMemcpyHostToDevice, wc.stream));
+                    wc.sync();
                 } else {
                     scalar_exp(a[i], out[i], true);
                 }
             } else if (n > 1) {
-                DMat A = upload(ctx, a[i], n, n, lda[i], true, dev, "a matrix to exponentiate");
+                DMat A = upload(wc, a[i], n, n, lda[i], true, dev, "a matrix to exponentiate");
                 DMat R;
                 tns::ExpmInfo ei;
-                tns::expm(ctx, A, R, &ei);
-                tns::copy_out(ctx, R, out[i], ldo[i], dev);
-                inf.degree = ei.degree;
-                inf.squarings = ei.squarings;
+                tns::expm(wc, A, R, &ei);
+                tns::copy_out(wc, R, out[i], ldo[i], dev);
+                wc.sync();
+                results[i] = tns_expm_info{ei.degree, ei.squarings};
             }
-            if (infos) infos[i] = inf;
+        };
+
+        int nworkers = std::max(1, std::min(count, ctx.max_workers));
+        while ((int)ctx.workers.size() < nworkers) ctx.workers.emplace_back(new Context(ctx.device));
+        std::atomic<int> next{0};
+        std::atomic<bool> stop{false};
+        std::mutex mu;
+        int err_code = TNS_OK;
+        std::string err_msg;
+        auto worker = [&](int w) {
+            Context& wc = *ctx.workers[w];
+            wc.max_elements = ctx.max_elements;
+            wc.timing = ctx.timing;
+            try {
+                TNS_CUDA(cudaSetDevice(ctx.device));
+                while (!stop.load()) {
+                    int k = next.fetch_add(1);
+                    if (k >= count) break;
+                    run_one(wc, order[k]);
+                }
+                check_device_flag(wc);
+            } catch (const Error& e) {
+                std::lock_guard<std::mutex> g(mu);
+                if (err_code == TNS_OK) {
+                    err_code = e.code;
+                    err_msg = e.what();
+                }
+                stop = true;
+                cudaStreamSynchronize(wc.stream);
+            } catch (const std::exception& e) {
+                std::lock_guard<std::mutex> g(mu);
+                if (err_code == TNS_OK) {
+                    err_code = TNS_E_DEVICE;
+                    err_msg = e.what();
+                }
+                stop = true;
+                cudaStreamSynchronize(wc.stream);
+            }
+        };
+        if (nworkers == 1) {
+            worker(0);
+        } else {
+            std::vector<std::thread> threads;
+            threads.reserve(nworkers);
+            for (int w = 0; w < nworkers; ++w) threads.emplace_back(worker, w);
+            for (auto& th : threads) th.join();
         }
-        ctx.sync();
+        if (err_code != TNS_OK) fail(err_code, err_msg);
+        if (infos)
+            for (int i = 0; i < count; ++i) infos[i] = results[i];
     });
+}
+
+// Sum of a context's counters and those of its batch workers.
+void collect_stats(Context& ctx, tns_stats* out) {
+    ctx.drain_events();
+    out->kernel_launches = ctx.kernel_launches;
+    out->gemm_launches = ctx.gemm_launches;
+    out->gemm_flops = ctx.gemm_flops;
+    out->gemm_ms = ctx.gemm_ms_done;
+    for (auto& w : ctx.workers) {
+        w->drain_events();
+        out->kernel_launches += w->kernel_launches;
+        out->gemm_launches += w->gemm_launches;
+        out->gemm_flops += w->gemm_flops;
+        out->gemm_ms += w->gemm_ms_done;
+    }
+}
+
+void reset_stats(Context& ctx) {
+    ctx.drain_events();
+    ctx.kernel_launches = ctx.gemm_launches = 0;
+    ctx.gemm_flops = ctx.gemm_ms_done = 0.0;
+    for (auto& w : ctx.workers) {
+        w->drain_events();
+        w->kernel_launches = w->gemm_launches = 0;
+        w->gemm_flops = w->gemm_ms_done = 0.0;
+    }
 }
 
 }  // namespace
@@ -419,20 +504,16 @@ int tns_zexpm_batched_device(tns_context* c, int count, const int* orders, const
 int tns_get_stats(tns_context* c, tns_stats* out) {
     return guarded(c, [&](Context& ctx) {
         require(out != nullptr, TNS_E_NULL, "out is null");
-        ctx.drain_events();
-        out->kernel_launches = ctx.kernel_launches;
-        out->gemm_launches = ctx.gemm_launches;
-        out->gemm_flops = ctx.gemm_flops;
-        out->gemm_ms = ctx.gemm_ms_done;
+        collect_stats(ctx, out);
     });
 }
 int tns_reset_stats(tns_context* c) {
+    return guarded(c, [&](Context& ctx) { reset_stats(ctx); });
+}
+int tns_set_workers(tns_context* c, int workers) {
     return guarded(c, [&](Context& ctx) {
-        ctx.drain_events();
-        ctx.kernel_launches = 0;
-        ctx.gemm_launches = 0;
-        ctx.gemm_flops = 0.0;
-        ctx.gemm_ms_done = 0.0;
+        require(workers >= 1 && workers <= 128, TNS_E_OUT_OF_RANGE, "workers must be in [1, 128]");
+        ctx.max_workers = workers;
     });
 }
 int tns_set_timing(tns_context* c, int enabled) {

@@ -28,6 +28,13 @@ Context::Context(int dev) : device(dev) {
     TNS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     TNS_CUDA(cudaMalloc(&d_err, sizeof(int)));
     TNS_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    // Keep freed blocks in the stream-ordered pool instead of handing them back
+    // to the driver at every synchronisation: the algorithms allocate and free
+    // work matrices between host-side decisions.
+    cudaMemPool_t pool;
+    TNS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = ~0ull;
+    TNS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
 }
 
 cudaEvent_t Context::take_event() {
@@ -55,6 +62,7 @@ void Context::drain_events() {
 }
 
 Context::~Context() {
+    workers.clear();
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     for (auto& pr : gemm_events) {

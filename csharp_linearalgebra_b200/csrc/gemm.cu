@@ -37,6 +37,7 @@
 #include "tns_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 namespace tns {
@@ -343,11 +344,11 @@ using CplxSmall = GemmCfg<true, 2, 2, 4>;   // 64 x 64 tiles, 4 math warps
 
 template <class Cfg>
 void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
-    static bool configured[64] = {false};
+    static std::atomic<bool> configured[64];
     int dev = ctx.device;
-    if (!configured[dev]) {
+    if (!configured[dev].load(std::memory_order_acquire)) {
         TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
-        configured[dev] = true;
+        configured[dev].store(true, std::memory_order_release);
     }
     int total = 0;
     for (auto& p : probs) {

@@ -317,25 +317,44 @@ __global__ void trsm_block_kernel(const double* t, int ldt, double* b, int ldb, 
     }
 }
 
-// min / max |u_jj| over the diagonal (RecordPivotRange, Lu.cs:312-329), with
-// Math.Min/Math.Max semantics, sequentially.
+// min / max |u_jj| over the diagonal (RecordPivotRange, Lu.cs:312-329). The
+// values are moduli (never -0), so Math.Min/Math.Max fold to the plain min and
+// max unless a NaN is present, which then wins; in that form the fold is
+// order-independent and a block reduction gives the reference's result.
 template <bool CPLX>
 __global__ void pivot_range_kernel(const double* a, int ld, int limit, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double smallest = __longlong_as_double(0x7ff0000000000000ll), largest = 0.0;
-    for (int j = 0; j < limit; ++j) {
+    __shared__ double s_lo[32], s_hi[32];
+    __shared__ int s_nan;
+    if (threadIdx.x == 0) s_nan = 0;
+    __syncthreads();
+    double lo = __longlong_as_double(0x7ff0000000000000ll), hi = 0.0;
+    bool nan = false;
+    for (int j = threadIdx.x; j < limit; j += blockDim.x) {
         const double* e = a + ((size_t)j * ld + j) * (CPLX ? 2 : 1);
         double v = CPLX ? cabs_net(e[0], e[1]) : fabs(e[0]);
-        // Math.Min
-        if (smallest != v) {
-            if (!isnan(smallest)) smallest = smallest < v ? smallest : v;
-        } else if (!signbit(smallest)) {
-            smallest = v;
-        }
-        largest = net_max(largest, v);
+        if (isnan(v)) nan = true;
+        lo = fmin(lo, v);
+        hi = fmax(hi, v);
     }
-    out[0] = smallest;
-    out[1] = largest;
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (nan) atomicOr(&s_nan, 1);
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[threadIdx.x >> 5] = lo;
+        s_hi[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            lo = fmin(lo, s_lo[w]);
+            hi = fmax(hi, s_hi[w]);
+        }
+        double qnan = __longlong_as_double(0x7ff8000000000000ll);
+        out[0] = s_nan ? qnan : lo;
+        out[1] = s_nan ? qnan : hi;
+    }
 }
 
 __global__ void init_int_kernel(int* p, int v) { *p = v; }
@@ -456,9 +475,9 @@ LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
         }
     }
     if (cplx)
-        pivot_range_kernel<true><<<1, 32, 0, ctx.stream>>>(a.p, ld, limit, d_range);
+        pivot_range_kernel<true><<<1, 256, 0, ctx.stream>>>(a.p, ld, limit, d_range);
     else
-        pivot_range_kernel<false><<<1, 32, 0, ctx.stream>>>(a.p, ld, limit, d_range);
+        pivot_range_kernel<false><<<1, 256, 0, ctx.stream>>>(a.p, ld, limit, d_range);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
     int h_sing = INT_MAX;

@@ -86,6 +86,12 @@ struct Context {
     cudaEvent_t take_event();
     void drain_events();        // sums finished event pairs into gemm_ms_done
 
+    // Batched work runs on worker contexts (one host thread and one stream
+    // each), created on first use, so that independent matrices overlap on
+    // the GPU. Their counters are summed into this context's statistics.
+    int max_workers = 16;
+    std::vector<std::unique_ptr<Context>> workers;
+
     explicit Context(int dev);
     ~Context();
     GemmProblem* upload_problems(const std::vector<GemmProblem>& probs);
