@@ -1,5 +1,6 @@
 // Streaming kernels: elementwise updates, exact norms, the ell test's
-// abs-power chain, and the narrow panel products behind normest1.
+// abs-power chain, and the narrow panel products behind normest1. Every
+// kernel takes a Batch<D>: one launch serves one matrix or a whole batch.
 //
 // All of these are HBM/L2-bound O(n^2) work. Where a result steers one of the
 // reference's integer decisions (norms feeding d4/d6, the ell chain, the panel
@@ -14,10 +15,12 @@
 //   A^T*X (dot form) PanelProduct.ApplyTranspose :44-55 with ColumnOps.Dot's
 //                    four 4-lane accumulators (src/Tensile.Kernels/ColumnOps.cs:35-65)
 
+#include "batch.cuh"
 #include "device_util.cuh"
 #include "tns_internal.h"
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 namespace tns {
@@ -26,15 +29,17 @@ namespace {
 
 constexpr int kThreads = 256;
 
-inline int blocks_for(long long n, int threads = kThreads) {
+inline int blocks_for(long long n, int threads = kThreads, int cap = 148 * 16) {
     long long b = (n + threads - 1) / threads;
-    return (int)std::max(1LL, std::min(b, 148LL * 16));
+    return (int)std::max(1LL, std::min(b, (long long)cap));
 }
 
 __device__ __forceinline__ double mag(const double* a, size_t idx, bool cplx) {
     if (cplx) return cabs_net(a[2 * idx], a[2 * idx + 1]);
     return fabs(a[idx]);
 }
+
+// ---- elementwise ------------------------------------------------------------
 
 // Scale: c := beta*c (beta == 0 overwrites), complex beta by the naive product.
 __global__ void scale_kernel(double* c, int m, int n, int ldc, bool cplx, double br, double bi) {
@@ -57,58 +62,63 @@ __global__ void scale_kernel(double* c, int m, int n, int ldc, bool cplx, double
     }
 }
 
-// dst := src * f over a flat range of doubles (each complex part on its own,
-// ComplexKernels.Scale, src/Tensile/ComplexKernels.cs:132).
-__global__ void scaled_copy_kernel(double* __restrict__ dst, const double* __restrict__ src, size_t count, double f) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
-        dst[e] = mul_rn(src[e], f);
-}
+// Elementwise operations over a matrix's whole padded extent (zeros in the
+// padding stay zero):
+//   kScaledCopy  dst = s1 * f          (Scaled, MatrixExponential.cs:528-543;
+//                                       complex parts scaled on their own)
+//   kAddScaled   dst = dst + s1 * f    (AddScaled, :546-558)
+//   kIdentity    dst = f I on the valid diagonal (Identity, :518-525)
+//   kPadeSplit   dst = s1 - s2, dst2 = s1 + s2 (SolvePade, :381-393)
+enum EwOp : int { kScaledCopy = 0, kAddScaled = 1, kIdentity = 2, kPadeSplit = 3 };
 
-// t := t + s * f (AddScaled, src/Tensile/MatrixExponential.cs:546-558).
-__global__ void add_scaled_kernel(double* __restrict__ t, const double* __restrict__ s, size_t count, double f) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
-        t[e] = add_rn(t[e], mul_rn(s[e], f));
-}
-
-__global__ void identity_kernel(double* dst, int rows_p, int cols_p, int n, bool cplx, double f) {
-    size_t total = (size_t)rows_p * cols_p * (cplx ? 2 : 1);
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        size_t el = cplx ? e / 2 : e;
-        int i = (int)(el % rows_p), j = (int)(el / rows_p);
-        bool re = !cplx || (e % 2 == 0);
-        dst[e] = (i == j && i < n && re) ? f : 0.0;
+__global__ void ew_kernel(const __grid_constant__ Batch<EwDesc> b) {
+    const EwDesc& d = batch_item(b, blockIdx.y);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < d.count; e += stride) {
+        switch (d.op) {
+            case kScaledCopy: d.dst[e] = mul_rn(d.s1[e], d.f); break;
+            case kAddScaled: d.dst[e] = add_rn(d.dst[e], mul_rn(d.s1[e], d.f)); break;
+            case kIdentity: {
+                size_t el = d.cplx ? e / 2 : e;
+                int i = (int)(el % d.rows_p), j = (int)(el / d.rows_p);
+                bool re = !d.cplx || (e % 2 == 0);
+                d.dst[e] = (i == j && i < d.n && re) ? d.f : 0.0;
+                break;
+            }
+            case kPadeSplit:
+                d.dst[e] = sub_rn(d.s1[e], d.s2[e]);
+                d.dst2[e] = add_rn(d.s1[e], d.s2[e]);
+                break;
+        }
     }
 }
 
-__global__ void pade_split_kernel(double* __restrict__ den, double* __restrict__ num, const double* __restrict__ v,
-                                  const double* __restrict__ u, size_t count) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
-        den[e] = sub_rn(v[e], u[e]);
-        num[e] = add_rn(v[e], u[e]);
-    }
-}
+// ---- norms ------------------------------------------------------------------
 
 // One thread per column: sequential sum of moduli in row order.
-__global__ void col_abs_sums_kernel(const double* __restrict__ a, int m, int n, int ld, bool cplx, double* __restrict__ out) {
+template <bool CPLX>
+__global__ void col_abs_sums_kernel(const __grid_constant__ Batch<SumDesc> b) {
+    const SumDesc& d = batch_item(b, blockIdx.y);
     int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const double* col = a + (size_t)j * ld * (cplx ? 2 : 1);
+    if (j >= d.n) return;
+    const double* col = d.a + (size_t)j * d.ld * (CPLX ? 2 : 1);
     double sum = 0.0;
-    for (int i = 0; i < m; ++i) sum = add_rn(sum, mag(col, i, cplx));
-    out[j] = sum;
+    for (int i = 0; i < d.m; ++i) sum = add_rn(sum, mag(col, i, CPLX));
+    d.out[j] = sum;
 }
 
 // One thread per row: sequential sum over columns in column order.
-__global__ void row_abs_sums_kernel(const double* __restrict__ a, int m, int n, int ld, bool cplx, double* __restrict__ out) {
+template <bool CPLX>
+__global__ void row_abs_sums_kernel(const __grid_constant__ Batch<SumDesc> b) {
+    const SumDesc& d = batch_item(b, blockIdx.y);
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
+    if (i >= d.m) return;
     double sum = 0.0;
-    for (int j = 0; j < n; ++j) sum = add_rn(sum, mag(a, (size_t)j * ld + i, cplx));
-    out[i] = sum;
+    for (int j = 0; j < d.n; ++j) sum = add_rn(sum, mag(d.a, (size_t)j * d.ld + i, CPLX));
+    d.out[i] = sum;
 }
 
-// Sum of squares per column (the reference's Frobenius accumulates one running
-// total; this path is used only for diagnostics, not decisions).
+// Sum of squares per column (diagnostic Frobenius only; no decision uses it).
 __global__ void col_sq_sums_kernel(const double* __restrict__ a, int m, int n, int ld, bool cplx, double* __restrict__ out) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -118,60 +128,64 @@ __global__ void col_sq_sums_kernel(const double* __restrict__ a, int m, int n, i
     out[j] = sum;
 }
 
-// Math.Max fold in index order (NaN propagates), single block.
-__global__ void max_fold_kernel(const double* __restrict__ v, int n, double* __restrict__ out) {
+// Math.Max fold of non-negative sums (NaN propagates): a tree reduction gives
+// the sequential fold's result, since max is order-independent here. One
+// block per item.
+__global__ void max_fold_kernel(const __grid_constant__ Batch<SumDesc> b) {
+    const SumDesc& d = batch_item(b, blockIdx.x);
     __shared__ double part[32];
-    // Order-independent except for NaN and signed zero; v holds sums of
-    // non-negative terms, so a tree with NaN propagation is exact.
+    __shared__ int any_nan;
+    if (threadIdx.x == 0) any_nan = 0;
+    __syncthreads();
     double best = 0.0;
     bool nan = false;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double x = v[i];
+    for (int i = threadIdx.x; i < d.n; i += blockDim.x) {
+        double x = d.a[i];
         if (isnan(x)) nan = true;
         else if (x > best) best = x;
     }
     for (int o = 16; o > 0; o >>= 1) {
         double other = __shfl_xor_sync(0xffffffffu, best, o);
         best = other > best ? other : best;
-        nan = __any_sync(0xffffffffu, nan);
     }
-    __shared__ int any_nan;
-    if (threadIdx.x == 0) any_nan = 0;
-    __syncthreads();
-    if (nan && (threadIdx.x & 31) == 0) any_nan = 1;
+    if (nan) atomicOr(&any_nan, 1);
     if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = best;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double b = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = part[w] > b ? part[w] : b;
-        out[0] = any_nan ? __longlong_as_double(0x7ff8000000000000ll) : b;
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = part[w] > r ? part[w] : r;
+        d.out[0] = any_nan ? __longlong_as_double(0x7ff8000000000000ll) : r;
     }
 }
 
-// |A| as a real n x n matrix (ld = n_p).
-__global__ void moduli_kernel(const double* __restrict__ a, int n, int ld, bool cplx, double* __restrict__ mags) {
-    size_t total = (size_t)ld * n;
+// ---- the ell test's chain -----------------------------------------------------
+
+// |A| as a real matrix (ld = n_p); row := ones.
+template <bool CPLX>
+__global__ void moduli_kernel(const __grid_constant__ Batch<ChainDesc> b) {
+    const ChainDesc& d = batch_item(b, blockIdx.y);
+    size_t total = (size_t)d.ld * d.n;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(e % ld);
-        mags[e] = i < n ? mag(a, e, cplx) : 0.0;
+        int i = (int)(e % d.ld);
+        d.mags[e] = i < d.n ? mag(d.a, e, CPLX) : 0.0;
+        if (e < (size_t)d.n) d.row[e] = 1.0;
     }
 }
 
-// One pass of the chain: next[j] = sum_i row[i] * mags[i, j], sequential in i.
-__global__ void abs_power_step_kernel(const double* __restrict__ mags, int n, int ld, const double* __restrict__ row,
-                                      double* __restrict__ next) {
+// One pass: next[j] = sum_i row[i] * mags[i, j], sequential in i.
+__global__ void abs_power_step_kernel(const __grid_constant__ Batch<ChainDesc> b, int parity) {
+    const ChainDesc& d = batch_item(b, blockIdx.y);
     int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const double* col = mags + (size_t)j * ld;
+    if (j >= d.n) return;
+    const double* row = parity ? d.next : d.row;
+    double* out = parity ? d.row : d.next;
+    const double* col = d.mags + (size_t)j * d.ld;
     double sum = 0.0;
-    for (int i = 0; i < n; ++i) sum = add_rn(sum, mul_rn(row[i], col[i]));
-    next[j] = sum;
+    for (int i = 0; i < d.n; ++i) sum = add_rn(sum, mul_rn(row[i], col[i]));
+    out[j] = sum;
 }
 
-__global__ void fill_kernel(double* p, size_t count, double v) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
-        p[e] = v;
-}
+// ---- normest1 panel products ------------------------------------------------
 
 // Y := A X in the axpy order of PanelProduct.Apply (PanelProduct.cs:25-41):
 // y[i] accumulates x[j] * a[i, j] for j = 0..n-1 with two roundings per term,
@@ -182,10 +196,11 @@ __global__ void fill_kernel(double* p, size_t count, double v) {
 // One thread per row covers all t <= TMAX columns, so A is read once per
 // product; x is staged through shared memory.
 template <int TMAX, bool CPLX>
-__global__ void __launch_bounds__(128) panel_apply_kernel(const double* __restrict__ a, int n, int ld,
-                                                          const double* __restrict__ x, int ldx,
-                                                          double* __restrict__ y, int ldy, int t) {
-    constexpr int CH = 64;  // rows of x staged per chunk
+__global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant__ Batch<PanelDesc> b) {
+    const PanelDesc& d = batch_item(b, blockIdx.y);
+    const int n = d.n, t = d.t;
+    if ((int)(blockIdx.x * blockDim.x) >= n) return;  // whole block past this item
+    constexpr int CH = 64;                              // rows of x staged per chunk
     constexpr int ES = CPLX ? 2 : 1;
     __shared__ double sx[CH * TMAX * ES];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -200,14 +215,14 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const double* __restri
         __syncthreads();
         for (int e = threadIdx.x; e < len * t * ES; e += blockDim.x) {
             int c = e / (len * ES), r = e % (len * ES);
-            sx[(c * CH) * ES + r] = x[((size_t)c * ldx + j0) * ES + r];
+            sx[(c * CH) * ES + r] = d.x[((size_t)c * d.ldx + j0) * ES + r];
         }
         __syncthreads();
         if (!row_ok) continue;
         for (int jj = 0; jj < len; ++jj) {
-            const size_t idx = (size_t)(j0 + jj) * ld + i;
+            const size_t idx = (size_t)(j0 + jj) * d.ld + i;
             if (!CPLX) {
-                const double aij = a[idx];
+                const double aij = d.a[idx];
 #pragma unroll
                 for (int c = 0; c < TMAX; ++c) {
                     if (c < t) {
@@ -217,7 +232,7 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const double* __restri
                     }
                 }
             } else {
-                const double2 aij = reinterpret_cast<const double2*>(a)[idx];
+                const double2 aij = reinterpret_cast<const double2*>(d.a)[idx];
 #pragma unroll
                 for (int c = 0; c < TMAX; ++c) {
                     if (c < t) {
@@ -237,9 +252,9 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const double* __restri
     for (int c = 0; c < TMAX; ++c) {
         if (c >= t) continue;
         if (!CPLX) {
-            y[(size_t)c * ldy + i] = acc[c][0];
+            d.y[(size_t)c * d.ldy + i] = acc[c][0];
         } else {
-            reinterpret_cast<double2*>(y)[(size_t)c * ldy + i] =
+            reinterpret_cast<double2*>(d.y)[(size_t)c * d.ldy + i] =
                 make_double2(sub_rn(acc[c][0], acc[c][3]), add_rn(acc[c][1], acc[c][2]));
         }
     }
@@ -271,8 +286,10 @@ __device__ __forceinline__ double netdot_combine(double acc, int L, int base) {
 // One half-warp per output row j, covering all t <= TMAX columns, reading the
 // interleaved complex data directly.
 template <int TMAX, bool CPLX>
-__global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld, const double* __restrict__ x,
-                                     int ldx, double* __restrict__ y, int ldy, int t) {
+__global__ void panel_apply_t_kernel(const __grid_constant__ Batch<PanelDesc> b) {
+    const PanelDesc& d = batch_item(b, blockIdx.y);
+    const int n = d.n, t = d.t;
+    if ((long long)blockIdx.x * blockDim.x >= (long long)n * 16) return;  // whole block past this item
     constexpr int NQ = CPLX ? 4 : 1;
     const long long half = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     const int L = threadIdx.x & 15;
@@ -281,6 +298,9 @@ __global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld
     // converged warp.
     const bool active = half < n;
     const int j = active ? (int)half : 0;
+    const double* a = d.a;
+    const double* x = d.x;
+    const int ld = d.ld, ldx = d.ldx;
     double acc[TMAX][NQ];
 #pragma unroll
     for (int c = 0; c < TMAX; ++c)
@@ -289,30 +309,30 @@ __global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld
     const int W = 4;
     const int n16 = (n / (4 * W)) * (4 * W);
     const int n4 = n >= W ? n16 + ((n - n16) / W) * W : 0;
-    auto add_term = [&](int i) {
+    auto add_term = [&](double (&r)[TMAX][NQ], int i) {
         if (!CPLX) {
             double aij = a[(size_t)j * ld + i];
 #pragma unroll
             for (int c = 0; c < TMAX; ++c)
-                if (c < t) acc[c][0] = add_rn(acc[c][0], mul_rn(aij, x[(size_t)c * ldx + i]));
+                if (c < t) r[c][0] = add_rn(r[c][0], mul_rn(aij, x[(size_t)c * ldx + i]));
         } else {
             double2 aij = reinterpret_cast<const double2*>(a)[(size_t)j * ld + i];
 #pragma unroll
             for (int c = 0; c < TMAX; ++c)
                 if (c < t) {
                     double2 xc = reinterpret_cast<const double2*>(x)[(size_t)c * ldx + i];
-                    acc[c][0] = add_rn(acc[c][0], mul_rn(aij.x, xc.x));  // pr
-                    acc[c][1] = add_rn(acc[c][1], mul_rn(aij.x, xc.y));  // pi
-                    acc[c][2] = add_rn(acc[c][2], mul_rn(aij.y, xc.x));  // qr
-                    acc[c][3] = add_rn(acc[c][3], mul_rn(aij.y, xc.y));  // qi
+                    r[c][0] = add_rn(r[c][0], mul_rn(aij.x, xc.x));  // pr
+                    r[c][1] = add_rn(r[c][1], mul_rn(aij.x, xc.y));  // pi
+                    r[c][2] = add_rn(r[c][2], mul_rn(aij.y, xc.x));  // qr
+                    r[c][3] = add_rn(r[c][3], mul_rn(aij.y, xc.y));  // qi
                 }
         }
     };
     double res[TMAX][NQ];
     if (n >= W) {
-        for (int i = L; i < n16; i += 16) add_term(i);
+        for (int i = L; i < n16; i += 16) add_term(acc, i);
         if (L < W)
-            for (int i = n16 + L; i < n4; i += W) add_term(i);
+            for (int i = n16 + L; i < n4; i += W) add_term(acc, i);
 #pragma unroll
         for (int c = 0; c < TMAX; ++c)
 #pragma unroll
@@ -324,36 +344,19 @@ __global__ void panel_apply_t_kernel(const double* __restrict__ a, int n, int ld
             for (int q = 0; q < NQ; ++q) res[c][q] = 0.0;
     }
     if (!active || L != 0) return;
-    // scalar tail, in order, by one lane
-    for (int i = n4; i < n; ++i) {
-        if (!CPLX) {
-            double aij = a[(size_t)j * ld + i];
-#pragma unroll
-            for (int c = 0; c < TMAX; ++c)
-                if (c < t) res[c][0] = add_rn(res[c][0], mul_rn(aij, x[(size_t)c * ldx + i]));
-        } else {
-            double2 aij = reinterpret_cast<const double2*>(a)[(size_t)j * ld + i];
-#pragma unroll
-            for (int c = 0; c < TMAX; ++c)
-                if (c < t) {
-                    double2 xc = reinterpret_cast<const double2*>(x)[(size_t)c * ldx + i];
-                    res[c][0] = add_rn(res[c][0], mul_rn(aij.x, xc.x));
-                    res[c][1] = add_rn(res[c][1], mul_rn(aij.x, xc.y));
-                    res[c][2] = add_rn(res[c][2], mul_rn(aij.y, xc.x));
-                    res[c][3] = add_rn(res[c][3], mul_rn(aij.y, xc.y));
-                }
-        }
-    }
+    for (int i = n4; i < n; ++i) add_term(res, i);  // scalar tail, in order
 #pragma unroll
     for (int c = 0; c < TMAX; ++c) {
         if (c >= t) continue;
         if (!CPLX)
-            y[(size_t)c * ldy + j] = res[c][0];
+            d.y[(size_t)c * d.ldy + j] = res[c][0];
         else
-            reinterpret_cast<double2*>(y)[(size_t)c * ldy + j] =
+            reinterpret_cast<double2*>(d.y)[(size_t)c * d.ldy + j] =
                 make_double2(add_rn(res[c][0], res[c][3]), sub_rn(res[c][1], res[c][2]));
     }
 }
+
+// ---- small single-matrix helpers ----------------------------------------------
 
 __global__ void shift_diag_kernel(double* a, int n, int ld, bool cplx, double dre, double dim) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -384,15 +387,226 @@ __global__ void trace_kernel(const double* a, int n, int ld, bool cplx, double* 
     out[1] = im;
 }
 
-double fetch_scalar(Context& ctx, const double* d) {
-    double h = 0.0;
-    TNS_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
-    ctx.sync();
-    return h;
+template <int TMAX, bool CPLX>
+void launch_panel(Context& ctx, std::vector<PanelDesc>& v, bool adjoint) {
+    int nmax = 0;
+    for (auto& d : v) nmax = std::max(nmax, d.n);
+    if (nmax == 0) return;
+    Batch<PanelDesc> b = make_batch(ctx, v);
+    if (!adjoint) {
+        dim3 grid((nmax + 127) / 128, b.count);
+        panel_apply_kernel<TMAX, CPLX><<<grid, 128, 0, ctx.stream>>>(b);
+    } else {
+        long long threads = (long long)nmax * 16;
+        dim3 grid((unsigned)((threads + 255) / 256), b.count);
+        panel_apply_t_kernel<TMAX, CPLX><<<grid, 256, 0, ctx.stream>>>(b);
+    }
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
 }
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Batched host entry points
+// ---------------------------------------------------------------------------
+
+void ew_batch(Context& ctx, std::vector<EwDesc>& v) {
+    if (v.empty()) return;
+    long long maxc = 0;
+    for (auto& d : v) maxc = std::max(maxc, (long long)d.count);
+    if (maxc == 0) return;
+    Batch<EwDesc> b = make_batch(ctx, v);
+    int bx = blocks_for(maxc, kThreads, std::max(1, 148 * 8 / (int)v.size()) + 1);
+    ew_kernel<<<dim3(bx, b.count), kThreads, 0, ctx.stream>>>(b);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
+
+EwDesc ew_scaled_copy(DMat& dst, const DMat& src, double f) {
+    EwDesc d{};
+    d.op = kScaledCopy;
+    d.dst = dst.p;
+    d.s1 = src.p;
+    d.count = src.bytes() / 8;
+    d.f = f;
+    return d;
+}
+EwDesc ew_add_scaled(DMat& t, const DMat& s, double f) {
+    EwDesc d{};
+    d.op = kAddScaled;
+    d.dst = t.p;
+    d.s1 = s.p;
+    d.count = s.bytes() / 8;
+    d.f = f;
+    return d;
+}
+EwDesc ew_identity(DMat& dst, double f) {
+    EwDesc d{};
+    d.op = kIdentity;
+    d.dst = dst.p;
+    d.count = dst.bytes() / 8;
+    d.f = f;
+    d.rows_p = dst.rows_p;
+    d.n = dst.rows;
+    d.cplx = dst.cplx ? 1 : 0;
+    return d;
+}
+EwDesc ew_pade_split(DMat& den, DMat& num, const DMat& v, const DMat& u) {
+    EwDesc d{};
+    d.op = kPadeSplit;
+    d.dst = den.p;
+    d.dst2 = num.p;
+    d.s1 = v.p;
+    d.s2 = u.p;
+    d.count = v.bytes() / 8;
+    return d;
+}
+
+std::vector<double> norm1_batch(Context& ctx, const std::vector<const DMat*>& mats) {
+    std::vector<double> out(mats.size(), 0.0);
+    if (mats.empty()) return out;
+    bool cplx = mats[0]->cplx;
+    size_t total = 0;
+    for (auto* m : mats) total += (size_t)m->cols + 1;
+    DBuf buf(ctx, sizeof(double) * std::max<size_t>(total, 1));
+    std::vector<SumDesc> sums, folds;
+    size_t off = 0;
+    int nmax = 0;
+    for (auto* m : mats) {
+        double* base = buf.as<double>() + off;
+        sums.push_back(SumDesc{m->p, m->rows, m->cols, m->ld(), base});
+        folds.push_back(SumDesc{base, 0, m->cols, 0, base + m->cols});
+        off += (size_t)m->cols + 1;
+        nmax = std::max(nmax, m->cols);
+    }
+    Batch<SumDesc> bs = make_batch(ctx, sums);
+    dim3 grid((nmax + 127) / 128, bs.count);
+    if (cplx) col_abs_sums_kernel<true><<<grid, 128, 0, ctx.stream>>>(bs);
+    else col_abs_sums_kernel<false><<<grid, 128, 0, ctx.stream>>>(bs);
+    Batch<SumDesc> bf = make_batch(ctx, folds);
+    max_fold_kernel<<<bf.count, 256, 0, ctx.stream>>>(bf);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches += 2;
+    std::vector<double> host(total);
+    TNS_CUDA(cudaMemcpyAsync(host.data(), buf.p, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    off = 0;
+    for (size_t k = 0; k < mats.size(); ++k) {
+        out[k] = (mats[k]->rows == 0 || mats[k]->cols == 0) ? 0.0 : host[off + mats[k]->cols];
+        off += (size_t)mats[k]->cols + 1;
+    }
+    return out;
+}
+
+std::vector<double> norminf_batch(Context& ctx, const std::vector<const DMat*>& mats) {
+    std::vector<double> out(mats.size(), 0.0);
+    if (mats.empty()) return out;
+    bool cplx = mats[0]->cplx;
+    size_t total = 0;
+    for (auto* m : mats) total += (size_t)m->rows + 1;
+    DBuf buf(ctx, sizeof(double) * std::max<size_t>(total, 1));
+    std::vector<SumDesc> sums, folds;
+    size_t off = 0;
+    int mmax = 0;
+    for (auto* m : mats) {
+        double* base = buf.as<double>() + off;
+        sums.push_back(SumDesc{m->p, m->rows, m->cols, m->ld(), base});
+        folds.push_back(SumDesc{base, 0, m->rows, 0, base + m->rows});
+        off += (size_t)m->rows + 1;
+        mmax = std::max(mmax, m->rows);
+    }
+    Batch<SumDesc> bs = make_batch(ctx, sums);
+    dim3 grid((mmax + 127) / 128, bs.count);
+    if (cplx) row_abs_sums_kernel<true><<<grid, 128, 0, ctx.stream>>>(bs);
+    else row_abs_sums_kernel<false><<<grid, 128, 0, ctx.stream>>>(bs);
+    Batch<SumDesc> bf = make_batch(ctx, folds);
+    max_fold_kernel<<<bf.count, 256, 0, ctx.stream>>>(bf);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches += 2;
+    std::vector<double> host(total);
+    TNS_CUDA(cudaMemcpyAsync(host.data(), buf.p, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    off = 0;
+    for (size_t k = 0; k < mats.size(); ++k) {
+        out[k] = (mats[k]->rows == 0 || mats[k]->cols == 0) ? 0.0 : host[off + mats[k]->rows];
+        off += (size_t)mats[k]->rows + 1;
+    }
+    return out;
+}
+
+std::vector<double> abs_power_batch(Context& ctx, const std::vector<const DMat*>& mats, int p) {
+    std::vector<double> out(mats.size(), 0.0);
+    if (mats.empty()) return out;
+    bool cplx = mats[0]->cplx;
+    size_t mag_total = 0, vec_total = 0;
+    for (auto* m : mats) {
+        mag_total += (size_t)m->ld() * m->rows;
+        vec_total += 2 * (size_t)m->rows + 1;
+    }
+    DBuf mags(ctx, sizeof(double) * std::max<size_t>(mag_total, 1));
+    DBuf vecs(ctx, sizeof(double) * vec_total);
+    std::vector<ChainDesc> chains;
+    std::vector<SumDesc> folds;
+    size_t mo = 0, vo = 0;
+    int nmax = 0;
+    long long emax = 0;
+    for (auto* m : mats) {
+        double* row = vecs.as<double>() + vo;
+        ChainDesc c{m->p, m->rows, m->ld(), mags.as<double>() + mo, row, row + m->rows};
+        chains.push_back(c);
+        // after p passes the result sits in row (p even) or next (p odd)
+        folds.push_back(SumDesc{(p % 2 == 0) ? row : row + m->rows, 0, m->rows, 0, row + 2 * m->rows});
+        mo += (size_t)m->ld() * m->rows;
+        vo += 2 * (size_t)m->rows + 1;
+        nmax = std::max(nmax, m->rows);
+        emax = std::max(emax, (long long)m->ld() * m->rows);
+    }
+    Batch<ChainDesc> bc = make_batch(ctx, chains);
+    dim3 g0(blocks_for(emax, kThreads, std::max(1, 148 * 8 / (int)mats.size()) + 1), bc.count);
+    if (cplx) moduli_kernel<true><<<g0, kThreads, 0, ctx.stream>>>(bc);
+    else moduli_kernel<false><<<g0, kThreads, 0, ctx.stream>>>(bc);
+    ctx.kernel_launches++;
+    dim3 g1((nmax + 127) / 128, bc.count);
+    for (int step = 0; step < p; ++step) {
+        abs_power_step_kernel<<<g1, 128, 0, ctx.stream>>>(bc, step & 1);
+        ctx.kernel_launches++;
+    }
+    Batch<SumDesc> bf = make_batch(ctx, folds);
+    max_fold_kernel<<<bf.count, 256, 0, ctx.stream>>>(bf);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+    std::vector<double> host(vec_total);
+    TNS_CUDA(cudaMemcpyAsync(host.data(), vecs.p, sizeof(double) * vec_total, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    vo = 0;
+    for (size_t k = 0; k < mats.size(); ++k) {
+        out[k] = host[vo + 2 * (size_t)mats[k]->rows];
+        vo += 2 * (size_t)mats[k]->rows + 1;
+    }
+    return out;
+}
+
+void panel_product_batch(Context& ctx, std::vector<PanelDesc>& v, bool cplx, bool adjoint) {
+    if (v.empty()) return;
+    int tmax = 0;
+    for (auto& d : v) tmax = std::max(tmax, d.t);
+    if (tmax > 16) fail(TNS_E_ARGUMENT, "internal panel product wider than 16 columns");
+    if (cplx) {
+        if (tmax <= 2) launch_panel<2, true>(ctx, v, adjoint);
+        else if (tmax <= 4) launch_panel<4, true>(ctx, v, adjoint);
+        else if (tmax <= 8) launch_panel<8, true>(ctx, v, adjoint);
+        else launch_panel<16, true>(ctx, v, adjoint);
+    } else {
+        if (tmax <= 2) launch_panel<2, false>(ctx, v, adjoint);
+        else if (tmax <= 4) launch_panel<4, false>(ctx, v, adjoint);
+        else if (tmax <= 8) launch_panel<8, false>(ctx, v, adjoint);
+        else launch_panel<16, false>(ctx, v, adjoint);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Single-matrix host entry points (one-item batches)
 // ---------------------------------------------------------------------------
 
 void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, double br, double bi) {
@@ -404,53 +618,28 @@ void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, doub
 }
 
 void scaled_copy(Context& ctx, DMat& dst, const DMat& src, double f) {
-    size_t count = src.bytes() / 8;
-    scaled_copy_kernel<<<blocks_for((long long)count), kThreads, 0, ctx.stream>>>(dst.p, src.p, count, f);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
+    std::vector<EwDesc> v{ew_scaled_copy(dst, src, f)};
+    ew_batch(ctx, v);
 }
 
 void add_scaled(Context& ctx, DMat& t, const DMat& s, double f) {
-    size_t count = s.bytes() / 8;
-    add_scaled_kernel<<<blocks_for((long long)count), kThreads, 0, ctx.stream>>>(t.p, s.p, count, f);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
+    std::vector<EwDesc> v{ew_add_scaled(t, s, f)};
+    ew_batch(ctx, v);
 }
 
 void set_identity(Context& ctx, DMat& dst, double f) {
-    size_t total = dst.bytes() / 8;
-    identity_kernel<<<blocks_for((long long)total), kThreads, 0, ctx.stream>>>(dst.p, dst.rows_p, dst.cols_p, dst.rows,
-                                                                               dst.cplx, f);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
+    std::vector<EwDesc> v{ew_identity(dst, f)};
+    ew_batch(ctx, v);
 }
 
 void pade_split(Context& ctx, DMat& den, DMat& num, const DMat& v, const DMat& u) {
-    size_t count = v.bytes() / 8;
-    pade_split_kernel<<<blocks_for((long long)count), kThreads, 0, ctx.stream>>>(den.p, num.p, v.p, u.p, count);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
+    std::vector<EwDesc> d{ew_pade_split(den, num, v, u)};
+    ew_batch(ctx, d);
 }
 
-double norm1(Context& ctx, const DMat& a) {
-    if (a.rows == 0 || a.cols == 0) return 0.0;
-    DBuf sums(ctx, sizeof(double) * (a.cols + 1));
-    col_abs_sums_kernel<<<(a.cols + 127) / 128, 128, 0, ctx.stream>>>(a.p, a.rows, a.cols, a.ld(), a.cplx, sums.as<double>());
-    max_fold_kernel<<<1, 256, 0, ctx.stream>>>(sums.as<double>(), a.cols, sums.as<double>() + a.cols);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches += 2;
-    return fetch_scalar(ctx, sums.as<double>() + a.cols);
-}
+double norm1(Context& ctx, const DMat& a) { return norm1_batch(ctx, {&a})[0]; }
 
-double norminf(Context& ctx, const DMat& a) {
-    if (a.rows == 0 || a.cols == 0) return 0.0;
-    DBuf sums(ctx, sizeof(double) * (a.rows + 1));
-    row_abs_sums_kernel<<<(a.rows + 127) / 128, 128, 0, ctx.stream>>>(a.p, a.rows, a.cols, a.ld(), a.cplx, sums.as<double>());
-    max_fold_kernel<<<1, 256, 0, ctx.stream>>>(sums.as<double>(), a.rows, sums.as<double>() + a.rows);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches += 2;
-    return fetch_scalar(ctx, sums.as<double>() + a.rows);
-}
+double norminf(Context& ctx, const DMat& a) { return norminf_batch(ctx, {&a})[0]; }
 
 double normfro(Context& ctx, const DMat& a) {
     if (a.rows == 0 || a.cols == 0) return 0.0;
@@ -466,49 +655,7 @@ double normfro(Context& ctx, const DMat& a) {
     return std::sqrt(total);
 }
 
-double one_norm_abs_power(Context& ctx, const DMat& a, int p) {
-    int n = a.rows;
-    int ld = a.ld();
-    DBuf mags(ctx, sizeof(double) * (size_t)ld * n);
-    DBuf vecs(ctx, sizeof(double) * (2 * (size_t)n + 1));
-    double* row = vecs.as<double>();
-    double* next = row + n;
-    moduli_kernel<<<blocks_for((long long)ld * n), kThreads, 0, ctx.stream>>>(a.p, n, ld, a.cplx, mags.as<double>());
-    fill_kernel<<<blocks_for(n), kThreads, 0, ctx.stream>>>(row, n, 1.0);
-    ctx.kernel_launches += 2;
-    for (int step = 0; step < p; ++step) {
-        abs_power_step_kernel<<<(n + 127) / 128, 128, 0, ctx.stream>>>(mags.as<double>(), n, ld, row, next);
-        std::swap(row, next);
-        ctx.kernel_launches++;
-    }
-    max_fold_kernel<<<1, 256, 0, ctx.stream>>>(row, n, vecs.as<double>() + 2 * (size_t)n);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
-    return fetch_scalar(ctx, vecs.as<double>() + 2 * (size_t)n);
-}
-
-namespace {
-template <int TMAX, bool CPLX>
-void launch_panel(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
-    int n = a.rows;
-    if (!adjoint) {
-        panel_apply_kernel<TMAX, CPLX><<<(n + 127) / 128, 128, 0, ctx.stream>>>(a.p, n, a.ld(), x, ldx, y, ldy, t);
-    } else {
-        long long threads = (long long)n * 16;
-        panel_apply_t_kernel<TMAX, CPLX><<<(int)((threads + 255) / 256), 256, 0, ctx.stream>>>(a.p, n, a.ld(), x, ldx, y,
-                                                                                               ldy, t);
-    }
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
-}
-template <bool CPLX>
-void panel_dispatch(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
-    if (t <= 2) launch_panel<2, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
-    else if (t <= 4) launch_panel<4, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
-    else if (t <= 8) launch_panel<8, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
-    else launch_panel<16, CPLX>(ctx, a, x, ldx, y, ldy, t, adjoint);
-}
-}  // namespace
+double one_norm_abs_power(Context& ctx, const DMat& a, int p) { return abs_power_batch(ctx, {&a}, p)[0]; }
 
 void panel_product(Context& ctx, const DMat& a, const double* x, int ldx, double* y, int ldy, int t, bool adjoint) {
     if (a.rows == 0 || t == 0) return;
@@ -517,10 +664,9 @@ void panel_product(Context& ctx, const DMat& a, const double* x, int ldx, double
     for (int c0 = 0; c0 < t; c0 += 16) {
         int tc = std::min(16, t - c0);
         size_t es = a.cplx ? 2 : 1;
-        const double* xc = x + (size_t)c0 * ldx * es;
-        double* yc = y + (size_t)c0 * ldy * es;
-        if (a.cplx) panel_dispatch<true>(ctx, a, xc, ldx, yc, ldy, tc, adjoint);
-        else panel_dispatch<false>(ctx, a, xc, ldx, yc, ldy, tc, adjoint);
+        PanelDesc d{a.p, a.rows, a.ld(), x + (size_t)c0 * ldx * es, ldx, y + (size_t)c0 * ldy * es, ldy, tc};
+        std::vector<PanelDesc> v{d};
+        panel_product_batch(ctx, v, a.cplx, adjoint);
     }
 }
 

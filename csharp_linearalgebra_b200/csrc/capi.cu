@@ -280,40 +280,58 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             check_operand(a[i], orders[i], orders[i], lda[i], "A[i]");
             check_operand(out[i], orders[i], orders[i], ldo[i], "out[i]");
         }
-        // Largest first (longest-processing-time order), so that the tail of
-        // the batch is made of short jobs.
-        std::vector<int> order(count);
-        for (int i = 0; i < count; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return orders[x] > orders[y]; });
         std::vector<tns_expm_info> results(count, tns_expm_info{0, 0});
-
-        auto run_one = [&](Context& wc, int i) {
+        // Orders 0 and 1 need no device work (MatrixExponential.cs:158-175).
+        std::vector<int> big;
+        for (int i = 0; i < count; ++i) {
             int n = orders[i];
-            if (n == 1) {
+            if (n >= 2) {
+                big.push_back(i);
+            } else if (n == 1) {
                 double h[2], r[2];
                 if (dev) {
-                    TNS_CUDA(cudaMemcpyAsync(h, a[i], 16, cudaMemcpyDeviceToHost, wc.stream));
-                    wc.sync();
+                    TNS_CUDA(cudaMemcpyAsync(h, a[i], 16, cudaMemcpyDeviceToHost, ctx.stream));
+                    ctx.sync();
                     scalar_exp(h, r, true);
-                    TNS_CUDA(cudaMemcpyAsync(out[i], r, 16, cudaMemcpyHostToDevice, wc.stream));
-                    wc.sync();
+                    TNS_CUDA(cudaMemcpyAsync(out[i], r, 16, cudaMemcpyHostToDevice, ctx.stream));
+                    ctx.sync();
                 } else {
                     scalar_exp(a[i], out[i], true);
                 }
-            } else if (n > 1) {
-                DMat A = upload(wc, a[i], n, n, lda[i], true, dev, "a matrix to exponentiate");
-                DMat R;
-                tns::ExpmInfo ei;
-                tns::expm(wc, A, R, &ei);
-                tns::copy_out(wc, R, out[i], ldo[i], dev);
-                wc.sync();
-                results[i] = tns_expm_info{ei.degree, ei.squarings};
             }
+        }
+        // Split the rest into cost-balanced groups (largest first onto the
+        // lightest group, n^3 as the cost); each group runs the batched
+        // algorithm on its own worker stream, so one group's host-side
+        // decisions and copies overlap another group's kernels.
+        int ngroups = std::max(1, std::min((int)big.size(), ctx.max_workers));
+        std::stable_sort(big.begin(), big.end(), [&](int x, int y) { return orders[x] > orders[y]; });
+        std::vector<std::vector<int>> groups(ngroups);
+        std::vector<double> load(ngroups, 0.0);
+        for (int i : big) {
+            int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            groups[g].push_back(i);
+            load[g] += std::pow((double)orders[i], 3.0);
+        }
+        auto run_group = [&](Context& wc, const std::vector<int>& idx) {
+            if (idx.empty()) return;
+            std::vector<DMat> in;
+            in.reserve(idx.size());
+            for (int i : idx) in.push_back(upload(wc, a[i], orders[i], orders[i], lda[i], true, dev, "a matrix to exponentiate"));
+            std::vector<const DMat*> ptrs;
+            for (auto& m : in) ptrs.push_back(&m);
+            std::vector<DMat> res;
+            std::vector<tns::ExpmInfo> infs;
+            tns::expm_batch(wc, ptrs, res, infs);
+            for (size_t k = 0; k < idx.size(); ++k) {
+                tns::copy_out(wc, res[k], out[idx[k]], ldo[idx[k]], dev);
+                results[idx[k]] = tns_expm_info{infs[k].degree, infs[k].squarings};
+            }
+            wc.sync();
         };
 
-        int nworkers = std::max(1, std::min(count, ctx.max_workers));
+        int nworkers = ngroups;
         while ((int)ctx.workers.size() < nworkers) ctx.workers.emplace_back(new Context(ctx.device));
-        std::atomic<int> next{0};
         std::atomic<bool> stop{false};
         std::mutex mu;
         int err_code = TNS_OK;
@@ -324,11 +342,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             wc.timing = ctx.timing;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
-                while (!stop.load()) {
-                    int k = next.fetch_add(1);
-                    if (k >= count) break;
-                    run_one(wc, order[k]);
-                }
+                run_group(wc, groups[w]);
                 check_device_flag(wc);
             } catch (const Error& e) {
                 std::lock_guard<std::mutex> g(mu);

@@ -70,27 +70,36 @@ Context::~Context() {
         cudaEventDestroy(pr.second);
     }
     for (auto e : event_pool) cudaEventDestroy(e);
-    if (d_probs) cudaFree(d_probs);
+    if (h_ring) cudaFreeHost(h_ring);
+    if (d_ring) cudaFree(d_ring);
     if (d_err) cudaFree(d_err);
     if (stream) cudaStreamDestroy(stream);
 }
 
-GemmProblem* Context::upload_problems(const std::vector<GemmProblem>& probs) {
-    size_t bytes = sizeof(GemmProblem) * probs.size();
-    if (bytes > d_probs_cap) {
-        if (d_probs) {
-            TNS_CUDA(cudaStreamSynchronize(stream));
-            TNS_CUDA(cudaFree(d_probs));
-            d_probs = nullptr;
-        }
-        size_t cap = std::max(bytes, sizeof(GemmProblem) * 256);
-        TNS_CUDA(cudaMalloc(&d_probs, cap));
-        d_probs_cap = cap;
+const void* Context::upload(const void* src, size_t bytes) {
+    size_t need = (bytes + 255) & ~size_t(255);
+    if (need > ring_cap) {
+        // Grow: everything already queued must finish with the old ring.
+        TNS_CUDA(cudaStreamSynchronize(stream));
+        if (h_ring) TNS_CUDA(cudaFreeHost(h_ring));
+        if (d_ring) TNS_CUDA(cudaFree(d_ring));
+        h_ring = nullptr;
+        d_ring = nullptr;
+        ring_cap = std::max(need, size_t(4) << 20);
+        TNS_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_ring), ring_cap, cudaHostAllocDefault));
+        TNS_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_ring), ring_cap));
+        ring_pos = 0;
     }
-    // A pageable source: the copy is staged before this call returns, so the
-    // vector may go away; the device buffer is reused in stream order.
-    TNS_CUDA(cudaMemcpyAsync(d_probs, probs.data(), bytes, cudaMemcpyHostToDevice, stream));
-    return d_probs;
+    if (ring_pos + need > ring_cap) {
+        // Wrap around: the copies and kernels still reading the ring finish first.
+        TNS_CUDA(cudaStreamSynchronize(stream));
+        ring_pos = 0;
+    }
+    std::memcpy(h_ring + ring_pos, src, bytes);
+    TNS_CUDA(cudaMemcpyAsync(d_ring + ring_pos, h_ring + ring_pos, bytes, cudaMemcpyHostToDevice, stream));
+    const void* out = d_ring + ring_pos;
+    ring_pos += need;
+    return out;
 }
 
 void Context::sync() { TNS_CUDA(cudaStreamSynchronize(stream)); }

@@ -1,0 +1,474 @@
+// Al-Mohy & Higham 2009 scaling and squaring (MatrixExponential.ScalingAndSquaring,
+// src/Tensile/MatrixExponential.cs:181-270) for a batch of independent
+// matrices of any orders, one launch per phase.
+//
+// Every matrix takes exactly the decisions the reference takes for it: the
+// Pade degree ladder (3, 5, 7, 9 against eta1/eta3 and the ell test, then 13),
+// d8/d10 from its own normest1 run, s = max(ceil(log2(eta5/4.25)), 0) plus
+// ell on the scaled matrix. What is batched is the work between decisions:
+// the powers A^2, A^4, A^6 are three grouped GEMM launches for the whole
+// batch; the norms, the ell chains and every normest1 product step are one
+// launch each for all matrices in that stage; the Pade evaluation is a few
+// elementwise launches and three grouped GEMMs; the LU of the denominators
+// advances all matrices block step by block step; the solve and each round
+// of squarings are grouped GEMMs over the matrices still squaring. A single
+// matrix is a batch of one.
+
+#include "estimator.h"
+#include "tns_internal.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace tns {
+
+namespace {
+
+// Constants, src/Tensile/MatrixExponential.cs:50-110, 441-449.
+const double kTheta3 = 1.495585217958292e-2;
+const double kTheta5 = 2.539398330063230e-1;
+const double kTheta7 = 9.504178996162932e-1;
+const double kTheta9 = 2.097847961257068e0;
+const double kScalingThreshold = 4.25;
+const double kUnitRoundoff = 1.1102230246251565e-16;
+const double kPade3[] = {120, 60, 12, 1};
+const double kPade5[] = {30240, 15120, 3360, 420, 30, 1};
+const double kPade7[] = {17297280, 8648640, 1995840, 277200, 25200, 1512, 56, 1};
+const double kPade9[] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0, 30270240.0,
+                         2162160.0,     110880.0,     3960.0,       90.0,        1.0};
+const double kPade13[] = {64764752532480000.0, 32382376266240000.0, 7771770303897600.0, 1187353796428800.0,
+                          129060195264000.0,   10559470521600.0,    670442572800.0,     33522128640.0,
+                          1323241920.0,        40840800.0,          960960.0,           16380.0,
+                          182.0,               1.0};
+const int kSeed = 20260915;
+
+double abs_coeff_reciprocal(int m) {
+    switch (m) {
+        case 3: return 100800.0;
+        case 5: return 10059033600.0;
+        case 7: return 4487938430976000.0;
+        case 9: return 5914384781877411840000.0;
+        default: return 113250775606021113483283660800000000.0;
+    }
+}
+
+struct Job {
+    const DMat* a = nullptr;
+    int n = 0;
+    DMat a2, a4, a6, a8;
+    double d4 = 0, d6 = 0, d8 = 0, d10 = 0, eta1 = 0, eta3 = 0;
+    int degree = 0, s = 0;
+    DMat result;
+};
+
+DMat like(Context& ctx, const DMat& a) { return DMat(ctx, a.rows, a.cols, a.cplx, "an exponential work matrix"); }
+
+// Ell (:416-430) for a set of matrices at one Pade degree m.
+std::vector<int> ell_batch(Context& ctx, const std::vector<const DMat*>& mats, int m) {
+    std::vector<int> out(mats.size(), 0);
+    if (mats.empty()) return out;
+    std::vector<double> anorm = norm1_batch(ctx, mats);
+    std::vector<double> apn = abs_power_batch(ctx, mats, 2 * m + 1);
+    for (size_t k = 0; k < mats.size(); ++k) {
+        if (anorm[k] == 0.0 || apn[k] == 0.0) continue;
+        double alpha = apn[k] / (anorm[k] * abs_coeff_reciprocal(m));
+        int value = (int)std::ceil(std::log2(alpha / kUnitRoundoff) / (2 * m));
+        out[k] = std::max(value, 0);
+    }
+    return out;
+}
+
+// normest1 of A^p (t = 2, itmax = 5, the default seed) for a set of matrices:
+// every estimator's products of one round run in one launch per power step.
+template <class TE>
+std::vector<double> power_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+    using Est = Estimator<TE>;
+    const size_t cnt = mats.size();
+    std::vector<double> out(cnt, 0.0);
+    if (cnt == 0) return out;
+    std::vector<std::unique_ptr<Est>> est;
+    std::vector<size_t> offs(cnt);
+    size_t total = 0;
+    for (size_t k = 0; k < cnt; ++k) {
+        est.emplace_back(new Est(mats[k]->rows, 2, 5, kSeed));
+        offs[k] = total;
+        total += (size_t)mats[k]->rows * est[k]->t() * TE::kDoubles;
+    }
+    DBuf d0(ctx, sizeof(double) * std::max<size_t>(total, 1));
+    DBuf d1(ctx, sizeof(double) * std::max<size_t>(total, 1));
+    std::vector<double> host(total);
+    const bool cplx = TE::kDoubles == 2;
+    for (;;) {
+        for (int phase = 0; phase < 2; ++phase) {
+            const bool adjoint = phase == 1;
+            std::vector<size_t> live;
+            for (size_t k = 0; k < cnt; ++k)
+                if (est[k]->need() == (adjoint ? Est::kAdjoint : Est::kApply)) live.push_back(k);
+            if (live.empty()) continue;
+            for (size_t k : live) {
+                const double* src = reinterpret_cast<const double*>(adjoint ? est[k]->s() : est[k]->x());
+                std::copy(src, src + (size_t)mats[k]->rows * est[k]->t() * TE::kDoubles, host.data() + offs[k]);
+            }
+            TNS_CUDA(cudaMemcpyAsync(d0.p, host.data(), sizeof(double) * total, cudaMemcpyHostToDevice, ctx.stream));
+            double* src = d0.as<double>();
+            double* dst = d1.as<double>();
+            for (int step = 0; step < power; ++step) {
+                std::vector<PanelDesc> v;
+                for (size_t k : live) {
+                    int n = mats[k]->rows;
+                    v.push_back(PanelDesc{mats[k]->p, n, mats[k]->ld(), src + offs[k], n, dst + offs[k], n, est[k]->t()});
+                }
+                panel_product_batch(ctx, v, cplx, adjoint);
+                std::swap(src, dst);
+            }
+            TNS_CUDA(cudaMemcpyAsync(host.data(), src, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();
+            for (size_t k : live) {
+                double* dstp = reinterpret_cast<double*>(adjoint ? est[k]->z() : est[k]->y());
+                const double* from = host.data() + offs[k];
+                std::copy(from, from + (size_t)mats[k]->rows * est[k]->t() * TE::kDoubles, dstp);
+                if (adjoint) est[k]->adjointed();
+                else est[k]->applied();
+            }
+        }
+        bool done = true;
+        for (auto& e : est)
+            if (e->need() != Est::kDone) done = false;
+        if (done) break;
+    }
+    for (size_t k = 0; k < cnt; ++k) out[k] = est[k]->value();
+    return out;
+}
+
+std::vector<double> power_norms(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+    if (mats.empty()) return {};
+    return mats[0]->cplx ? power_estimates<CplxE>(ctx, mats, power) : power_estimates<RealE>(ctx, mats, power);
+}
+
+void product_batch(Context& ctx, std::vector<std::pair<const DMat*, const DMat*>> ab, std::vector<DMat*> c,
+                   double beta) {
+    if (ab.empty()) return;
+    std::vector<GemmProblem> probs;
+    for (size_t k = 0; k < ab.size(); ++k) probs.push_back(make_gemm(*ab[k].first, *ab[k].second, *c[k], 1.0, 0.0, beta, 0.0));
+    gemm_grouped(ctx, probs, ab[0].first->cplx);
+}
+
+}  // namespace
+
+void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,
+                std::vector<ExpmInfo>& infos) {
+    const size_t cnt = inputs.size();
+    results.clear();
+    results.resize(cnt);
+    infos.assign(cnt, ExpmInfo{});
+    if (cnt == 0) return;
+    std::vector<Job> jobs(cnt);
+    for (size_t k = 0; k < cnt; ++k) {
+        jobs[k].a = inputs[k];
+        jobs[k].n = inputs[k]->rows;
+    }
+    // A^2, A^4, A^6 (:190-192).
+    {
+        std::vector<std::pair<const DMat*, const DMat*>> ab;
+        std::vector<DMat*> c;
+        for (auto& j : jobs) {
+            j.a2 = like(ctx, *j.a);
+            ab.push_back({j.a, j.a});
+            c.push_back(&j.a2);
+        }
+        product_batch(ctx, ab, c, 0.0);
+        ab.clear();
+        c.clear();
+        for (auto& j : jobs) {
+            j.a4 = like(ctx, *j.a);
+            ab.push_back({&j.a2, &j.a2});
+            c.push_back(&j.a4);
+        }
+        product_batch(ctx, ab, c, 0.0);
+        ab.clear();
+        c.clear();
+        for (auto& j : jobs) {
+            j.a6 = like(ctx, *j.a);
+            ab.push_back({&j.a2, &j.a4});
+            c.push_back(&j.a6);
+        }
+        product_batch(ctx, ab, c, 0.0);
+    }
+    // d4, d6 exact (:198-199).
+    {
+        std::vector<const DMat*> m4, m6;
+        for (auto& j : jobs) {
+            m4.push_back(&j.a4);
+            m6.push_back(&j.a6);
+        }
+        std::vector<double> n4 = norm1_batch(ctx, m4), n6 = norm1_batch(ctx, m6);
+        for (size_t k = 0; k < cnt; ++k) {
+            jobs[k].d4 = std::pow(n4[k], 1.0 / 4.0);
+            jobs[k].d6 = std::pow(n6[k], 1.0 / 6.0);
+            jobs[k].eta1 = net::max(jobs[k].d4, jobs[k].d6);
+        }
+    }
+    // The low-degree ladder (:202-231), stage by stage over the undecided.
+    auto stage_ell = [&](int m, auto&& eligible) {
+        std::vector<Job*> js;
+        std::vector<const DMat*> mats;
+        for (auto& j : jobs)
+            if (j.degree == 0 && eligible(j)) {
+                js.push_back(&j);
+                mats.push_back(j.a);
+            }
+        std::vector<int> e = ell_batch(ctx, mats, m);
+        for (size_t k = 0; k < js.size(); ++k)
+            if (e[k] == 0) js[k]->degree = m;
+    };
+    stage_ell(3, [](const Job& j) { return j.eta1 < kTheta3; });
+    stage_ell(5, [](const Job& j) { return j.eta1 < kTheta5; });
+    {
+        std::vector<Job*> js;
+        std::vector<const DMat*> mats;
+        for (auto& j : jobs)
+            if (j.degree == 0) {
+                js.push_back(&j);
+                mats.push_back(j.a);
+            }
+        std::vector<double> e8 = power_norms(ctx, mats, 8);
+        for (size_t k = 0; k < js.size(); ++k) {
+            js[k]->d8 = std::pow(e8[k], 1.0 / 8.0);
+            js[k]->eta3 = net::max(js[k]->d6, js[k]->d8);
+        }
+    }
+    stage_ell(7, [](const Job& j) { return j.eta3 < kTheta7; });
+    stage_ell(9, [](const Job& j) { return j.eta3 < kTheta9; });
+    // Degree 13: d10, eta5, s and the ell correction on the scaled matrix (:233-247).
+    std::vector<Job*> top;
+    for (auto& j : jobs)
+        if (j.degree == 0) top.push_back(&j);
+    if (!top.empty()) {
+        std::vector<const DMat*> mats;
+        for (auto* j : top) mats.push_back(j->a);
+        std::vector<double> e10 = power_norms(ctx, mats, 10);
+        std::vector<DMat> scaled;
+        std::vector<EwDesc> ew;
+        scaled.reserve(top.size());
+        for (size_t k = 0; k < top.size(); ++k) {
+            Job& j = *top[k];
+            j.d10 = std::pow(e10[k], 1.0 / 10.0);
+            double eta4 = net::max(j.d8, j.d10);
+            double eta5 = net::min(j.eta3, eta4);
+            j.s = eta5 == 0.0 ? 0 : std::max((int)std::ceil(std::log2(eta5 / kScalingThreshold)), 0);
+            j.degree = 13;
+            scaled.push_back(like(ctx, *j.a));
+            ew.push_back(ew_scaled_copy(scaled.back(), *j.a, std::ldexp(1.0, -j.s)));
+        }
+        ew_batch(ctx, ew);
+        std::vector<const DMat*> sm;
+        for (auto& m : scaled) sm.push_back(&m);
+        std::vector<int> e13 = ell_batch(ctx, sm, 13);
+        for (size_t k = 0; k < top.size(); ++k) top[k]->s += e13[k];
+    }
+
+    // Evaluation (:251-259, EvaluateLowDegree :284-315, EvaluateDegree13 :323-360).
+    // Per job: u (numerator odd part times A) and v (even part); then
+    // den = v - u, num = v + u.
+    struct Eval {
+        DMat b, b2, b4, b6, inner, inner_even, w, u, v;
+    };
+    std::vector<Eval> ev(cnt);
+    {
+        std::vector<EwDesc> ew;
+        for (size_t k = 0; k < cnt; ++k) {
+            Job& j = jobs[k];
+            Eval& e = ev[k];
+            if (j.degree == 9) {
+                j.a8 = like(ctx, *j.a);
+            }
+            if (j.degree == 13) {
+                double f = std::ldexp(1.0, -j.s);
+                e.b = like(ctx, *j.a);
+                e.b2 = like(ctx, *j.a);
+                e.b4 = like(ctx, *j.a);
+                e.b6 = like(ctx, *j.a);
+                ew.push_back(ew_scaled_copy(e.b, *j.a, f));
+                ew.push_back(ew_scaled_copy(e.b2, j.a2, f * f));
+                ew.push_back(ew_scaled_copy(e.b4, j.a4, std::pow(f, 4)));
+                ew.push_back(ew_scaled_copy(e.b6, j.a6, std::pow(f, 6)));
+            }
+        }
+        ew_batch(ctx, ew);
+        // A^8 for degree 9 (:229).
+        std::vector<std::pair<const DMat*, const DMat*>> ab;
+        std::vector<DMat*> c;
+        for (auto& j : jobs)
+            if (j.degree == 9) {
+                ab.push_back({&j.a4, &j.a4});
+                c.push_back(&j.a8);
+            }
+        product_batch(ctx, ab, c, 0.0);
+        // The powers of degree-13 jobs are no longer needed.
+        for (auto& j : jobs)
+            if (j.degree == 13) {
+                j.a2 = DMat();
+                j.a4 = DMat();
+                j.a6 = DMat();
+            }
+    }
+    {
+        // Elementwise assembly, in the reference's order of operations.
+        std::vector<EwDesc> s1, s2, s3, s4;  // sequential rounds (each op in a round touches distinct targets)
+        for (size_t k = 0; k < cnt; ++k) {
+            Job& j = jobs[k];
+            Eval& e = ev[k];
+            e.w = like(ctx, *j.a);
+            e.v = like(ctx, *j.a);
+            if (j.degree == 13) {
+                const double* b = kPade13;
+                e.inner = like(ctx, *j.a);
+                e.inner_even = like(ctx, *j.a);
+                // inner = b13 B6 + b11 B4 + b9 B2; w = b1 I + b3 B2 + b5 B4 + b7 B6;
+                // inner_even = b12 B6 + b10 B4 + b8 B2; v = b0 I + b2 B2 + b4 B4 + b6 B6.
+                s1.push_back(ew_scaled_copy(e.inner, e.b6, b[13]));
+                s1.push_back(ew_identity(e.w, b[1]));
+                s1.push_back(ew_scaled_copy(e.inner_even, e.b6, b[12]));
+                s1.push_back(ew_identity(e.v, b[0]));
+                s2.push_back(ew_add_scaled(e.inner, e.b4, b[11]));
+                s2.push_back(ew_add_scaled(e.w, e.b2, b[3]));
+                s2.push_back(ew_add_scaled(e.inner_even, e.b4, b[10]));
+                s2.push_back(ew_add_scaled(e.v, e.b2, b[2]));
+                s3.push_back(ew_add_scaled(e.inner, e.b2, b[9]));
+                s3.push_back(ew_add_scaled(e.w, e.b4, b[5]));
+                s3.push_back(ew_add_scaled(e.inner_even, e.b2, b[8]));
+                s3.push_back(ew_add_scaled(e.v, e.b4, b[4]));
+                s4.push_back(ew_add_scaled(e.w, e.b6, b[7]));
+                s4.push_back(ew_add_scaled(e.v, e.b6, b[6]));
+            } else {
+                const double* b = j.degree == 3 ? kPade3 : j.degree == 5 ? kPade5 : j.degree == 7 ? kPade7 : kPade9;
+                int m = j.degree;
+                s1.push_back(ew_identity(e.w, b[1]));
+                s1.push_back(ew_identity(e.v, b[0]));
+                s2.push_back(ew_add_scaled(e.w, j.a2, b[3]));
+                s2.push_back(ew_add_scaled(e.v, j.a2, b[2]));
+                if (m >= 5) {
+                    s3.push_back(ew_add_scaled(e.w, j.a4, b[5]));
+                    s3.push_back(ew_add_scaled(e.v, j.a4, b[4]));
+                }
+                if (m >= 7) {
+                    s4.push_back(ew_add_scaled(e.w, j.a6, b[7]));
+                    s4.push_back(ew_add_scaled(e.v, j.a6, b[6]));
+                }
+            }
+        }
+        ew_batch(ctx, s1);
+        ew_batch(ctx, s2);
+        ew_batch(ctx, s3);
+        ew_batch(ctx, s4);
+        std::vector<EwDesc> s5;
+        for (auto& j : jobs)
+            if (j.degree == 9) {
+                size_t k = &j - jobs.data();
+                s5.push_back(ew_add_scaled(ev[k].w, j.a8, kPade9[9]));
+                s5.push_back(ew_add_scaled(ev[k].v, j.a8, kPade9[8]));
+            }
+        ew_batch(ctx, s5);
+        // w += B6 inner; v += B6 inner_even (degree 13, beta = 1).
+        std::vector<std::pair<const DMat*, const DMat*>> ab;
+        std::vector<DMat*> c;
+        for (size_t k = 0; k < cnt; ++k)
+            if (jobs[k].degree == 13) {
+                ab.push_back({&ev[k].b6, &ev[k].inner});
+                c.push_back(&ev[k].w);
+                ab.push_back({&ev[k].b6, &ev[k].inner_even});
+                c.push_back(&ev[k].v);
+            }
+        product_batch(ctx, ab, c, 1.0);
+        // u = A w (B w for degree 13).
+        ab.clear();
+        c.clear();
+        for (size_t k = 0; k < cnt; ++k) {
+            ev[k].u = like(ctx, *jobs[k].a);
+            ab.push_back({jobs[k].degree == 13 ? &ev[k].b : jobs[k].a, &ev[k].w});
+            c.push_back(&ev[k].u);
+        }
+        product_batch(ctx, ab, c, 0.0);
+    }
+    // SolvePade (:372-405): den = v - u, num = v + u, LU of den, solve.
+    std::vector<DMat> den(cnt), num(cnt);
+    {
+        std::vector<EwDesc> ew;
+        for (size_t k = 0; k < cnt; ++k) {
+            den[k] = like(ctx, *jobs[k].a);
+            num[k] = like(ctx, *jobs[k].a);
+            ew.push_back(ew_pade_split(den[k], num[k], ev[k].v, ev[k].u));
+        }
+        ew_batch(ctx, ew);
+        for (auto& e : ev) e = Eval();  // release the evaluation buffers
+        for (auto& j : jobs) {
+            j.a2 = DMat();
+            j.a4 = DMat();
+            j.a6 = DMat();
+            j.a8 = DMat();
+        }
+        size_t piv_total = 0;
+        for (auto& j : jobs) piv_total += (size_t)j.n;
+        DBuf pivs(ctx, sizeof(int) * (piv_total + cnt));
+        std::vector<LuItem> lus;
+        std::vector<SolveItem> solves;
+        size_t po = 0;
+        for (size_t k = 0; k < cnt; ++k) {
+            int n = jobs[k].n;
+            int* piv = pivs.as<int>() + po;
+            int* sing = pivs.as<int>() + piv_total + k;
+            lus.push_back(LuItem{&den[k], n, n, 0, piv, sing});
+            solves.push_back(SolveItem{&den[k], piv, &num[k], n});
+            po += (size_t)n;
+        }
+        getrf_batch(ctx, lus);
+        std::vector<int> sing(cnt);
+        TNS_CUDA(cudaMemcpyAsync(sing.data(), pivs.as<int>() + piv_total, sizeof(int) * cnt, cudaMemcpyDeviceToHost,
+                                 ctx.stream));
+        ctx.sync();
+        for (size_t k = 0; k < cnt; ++k)
+            if (sing[k] != INT_MAX)
+                fail(TNS_E_SINGULAR, "The Pade denominator is exactly singular at column " + std::to_string(sing[k]) +
+                                         ", which indicates a non-finite input rather than a property of the algorithm.");
+        getrs_batch(ctx, solves, false);
+    }
+    // Squarings (:262-267): round r squares every matrix with s > r.
+    {
+        std::vector<DMat> sq(cnt);
+        int max_s = 0;
+        for (auto& j : jobs) max_s = std::max(max_s, j.s);
+        for (size_t k = 0; k < cnt; ++k)
+            if (jobs[k].s > 0) sq[k] = like(ctx, *jobs[k].a);
+        for (int r = 0; r < max_s; ++r) {
+            std::vector<std::pair<const DMat*, const DMat*>> ab;
+            std::vector<DMat*> c;
+            for (size_t k = 0; k < cnt; ++k)
+                if (jobs[k].s > r) {
+                    ab.push_back({&num[k], &num[k]});
+                    c.push_back(&sq[k]);
+                }
+            product_batch(ctx, ab, c, 0.0);
+            for (size_t k = 0; k < cnt; ++k)
+                if (jobs[k].s > r) std::swap(num[k], sq[k]);
+        }
+    }
+    for (size_t k = 0; k < cnt; ++k) {
+        results[k] = std::move(num[k]);
+        infos[k].degree = jobs[k].degree;
+        infos[k].squarings = jobs[k].degree == 13 ? jobs[k].s : 0;
+    }
+}
+
+void expm(Context& ctx, const DMat& a, DMat& result, ExpmInfo* info) {
+    std::vector<DMat> results;
+    std::vector<ExpmInfo> infos;
+    expm_batch(ctx, {&a}, results, infos);
+    result = std::move(results[0]);
+    if (info) *info = infos[0];
+}
+
+}  // namespace tns

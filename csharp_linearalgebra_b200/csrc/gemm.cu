@@ -366,7 +366,7 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
         for (size_t i = 0; i < probs.size(); ++i) L.inl[i] = probs[i];
         L.list = nullptr;
     } else {
-        L.list = ctx.upload_problems(probs);
+        L.list = static_cast<const GemmProblem*>(ctx.upload(probs.data(), sizeof(GemmProblem) * probs.size()));
     }
     int ctas_per_sm = 1;
     TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));

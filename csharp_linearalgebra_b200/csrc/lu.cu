@@ -1,23 +1,25 @@
-// LU with partial pivoting and the triangular solves, on the GPU.
+// LU with partial pivoting and the triangular solves, on the GPU, for one
+// matrix or a batch of independent matrices advanced in lockstep.
 //
 // Right-looking blocked getrf as the reference runs it (src/Tensile.Kernels/Lu.cs:230-309
 // for real, src/Tensile/BlockedLu.cs:45-101 for complex): per block of nb
 // columns
-//   1. panel factorization (one CTA; pivot = first index of the largest |a|,
-//      or |Re|+|Im| for complex; reciprocal multiply unless |pivot| < SafeMin;
-//      rank-1 updates y + (-m)*x with two roundings),
+//   1. panel factorization (one CTA per matrix; pivot = first index of the
+//      largest |a|, or |Re|+|Im| for complex; reciprocal multiply unless
+//      |pivot| < SafeMin; rank-1 updates y + (-m)*x with two roundings),
 //   2. the panel's row interchanges applied to the columns either side,
 //   3. U12 := L11^-1 A12 (one warp per column, the reference's update order),
-//   4. A22 := A22 - A21*U12 on the DMMA GEMM.
-// The per-element arithmetic of steps 1-3 is the reference's, so the pivot
-// sequence can only differ from the reference through the trailing GEMM's
-// summation order.
+//   4. A22 := A22 - A21*U12 on the DMMA GEMM (bit-identical to the
+//      reference's product, gemm.cu).
+// Every step's arithmetic is the reference's, so the factors and pivots match
+// the reference bit for bit. In a batch, step k of every matrix runs in one
+// launch per phase (a grouped GEMM for the trailing updates).
 //
-// Solves: few right-hand sides use one CTA per column (substitution with the
-// reference's update order); many right-hand sides (the Pade solve, n RHS)
-// use 64-row diagonal-block substitution plus DMMA GEMM updates, a blocked
-// TRSM (the reference's own planned next step, GEMM-based TRSM).
+// Solves: 64-row diagonal-block substitution plus DMMA GEMM updates of the
+// rows below (a blocked, GEMM-based TRSM -- the reference's own planned next
+// step for its n-RHS solves).
 
+#include "batch.cuh"
 #include "device_util.cuh"
 #include "tns_internal.h"
 
@@ -58,10 +60,18 @@ __device__ __forceinline__ Z zdiv(Z l, Z r) {
 
 // ---------------------------------------------------------------------------
 // Panel factorization: rows [r0, m) x columns [r0, r0 + w) of a (ld elements),
-// one CTA. pivots land as global 0-based rows in piv[r0 + j].
+// one CTA per item. Pivots land as global 0-based rows in piv[r0 + j].
 // ---------------------------------------------------------------------------
+struct PanelFactorDesc {
+    double* a;
+    int ld, m, r0, w;
+    int* piv;
+    int* singular;
+};
+
 template <bool CPLX>
-__global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, int r0, int w, int* piv, int* singular) {
+__global__ void __launch_bounds__(512) panel_kernel(const __grid_constant__ Batch<PanelFactorDesc> b) {
+    const PanelFactorDesc& d = batch_item(b, blockIdx.x);
     constexpr int ES = CPLX ? 2 : 1;
     __shared__ double s_val[32];
     __shared__ int s_idx[32];
@@ -69,9 +79,10 @@ __global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, in
     __shared__ double s_prow[2 * 64];
     const int tid = threadIdx.x;
     const int nthreads = blockDim.x;
-    const int M = m - r0;  // rows in the panel
+    const int ld = d.ld, w = d.w, r0 = d.r0;
+    const int M = d.m - r0;  // rows in the panel
     const int limit = min(M, w);
-    double* P = a + ((size_t)r0 * ld + r0) * ES;  // panel origin
+    double* P = d.a + ((size_t)r0 * ld + r0) * ES;  // panel origin
 
     for (int j = 0; j < limit; ++j) {
         // a. first index of the largest pivot measure in column j, rows j..M-1
@@ -109,7 +120,7 @@ __global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, in
             // A column of NaNs (no comparison succeeds) keeps the diagonal.
             if (bi == INT_MAX) bi = j;
             s_p = bi;
-            piv[r0 + j] = r0 + bi;
+            d.piv[r0 + j] = r0 + bi;
         }
         __syncthreads();
         const int p = s_p;
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, in
         if (!CPLX) {
             double value = s_prow[2 * j];
             if (value == 0.0) {
-                if (tid == 0) atomicMin(singular, r0 + j);
+                if (tid == 0) atomicMin(d.singular, r0 + j);
             }
             bool recip = fabs(value) >= kSafeMin;
             double r = __ddiv_rn(1.0, value);
@@ -159,7 +170,7 @@ __global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, in
         } else {
             Z value{s_prow[2 * j], s_prow[2 * j + 1]};
             bool zero = value.re == 0.0 && value.im == 0.0;
-            if (zero && tid == 0) atomicMin(singular, r0 + j);
+            if (zero && tid == 0) atomicMin(d.singular, r0 + j);
             bool recip = cabs_net(value.re, value.im) >= kSafeMin;
             Z r = zdiv(Z{1.0, 0.0}, value);
             for (int i = j + 1 + tid; i < M; i += nthreads) {
@@ -183,16 +194,25 @@ __global__ void __launch_bounds__(512) panel_kernel(double* a, int ld, int m, in
 }
 
 // Row interchanges rows k <-> piv[k] for k in [k0, k1), applied in increasing
-// k, to columns [c0, c1). One thread per column (SwapRows, Lu.cs:430-448).
+// k (or decreasing, to undo), to columns [c0, c1). One thread per column
+// (SwapRows / UnswapRows, Lu.cs:430-478).
+struct LaswpDesc {
+    double* a;
+    int ld, c0, c1;
+    const int* piv;
+    int k0, k1, reverse;
+};
+
 template <bool CPLX>
-__global__ void laswp_kernel(double* a, int ld, int c0, int c1, const int* piv, int k0, int k1, bool reverse) {
+__global__ void laswp_kernel(const __grid_constant__ Batch<LaswpDesc> b) {
+    const LaswpDesc& d = batch_item(b, blockIdx.y);
     constexpr int ES = CPLX ? 2 : 1;
-    int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= c1) return;
-    double* col = a + (size_t)c * ld * ES;
-    for (int s = 0; s < k1 - k0; ++s) {
-        int k = reverse ? k1 - 1 - s : k0 + s;
-        int p = piv[k];
+    int c = d.c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.c1) return;
+    double* col = d.a + (size_t)c * d.ld * ES;
+    for (int s = 0; s < d.k1 - d.k0; ++s) {
+        int k = d.reverse ? d.k1 - 1 - s : d.k0 + s;
+        int p = d.piv[k];
         if (p != k) {
             for (int q = 0; q < ES; ++q) {
                 double tmp = col[(size_t)k * ES + q];
@@ -203,101 +223,69 @@ __global__ void laswp_kernel(double* a, int ld, int c0, int c1, const int* piv, 
     }
 }
 
-// B := L^-1 B for a w x w unit lower L (w <= 64) at `l`, B w x ncols at `b`.
-// One warp per column, x[i] += (-x[p]) * L[i, p] for p = 0..w-2 in order
-// (Triangular.SolveLowerUnit, Triangular.cs:26-57; complex BlockedLu.cs:312-327).
-template <bool CPLX>
-__global__ void trsm_lower_unit_kernel(const double* l, int ldl, double* b, int ldb, int w, int ncols) {
-    constexpr int ES = CPLX ? 2 : 1;
-    extern __shared__ double sL[];  // w x w, ld w
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-        int i = e % w, p = e / w;
-        for (int q = 0; q < ES; ++q) sL[(size_t)e * ES + q] = l[((size_t)p * ldl + i) * ES + q];
-    }
-    __syncthreads();
-    int lane = threadIdx.x & 31;
-    int warps = blockDim.x >> 5;
-    for (int c = blockIdx.x * warps + (threadIdx.x >> 5); c < ncols; c += gridDim.x * warps) {
-        double* x = b + (size_t)c * ldb * ES;
-        double xr[2], xi[2];
-        for (int h = 0; h < 2; ++h) {
-            int i = lane + 32 * h;
-            xr[h] = i < w ? x[(size_t)i * ES] : 0.0;
-            xi[h] = (CPLX && i < w) ? x[(size_t)i * ES + 1] : 0.0;
-        }
-        for (int p = 0; p < w - 1; ++p) {
-            double vr = __shfl_sync(0xffffffffu, xr[p >> 5], p & 31);
-            double vi = CPLX ? __shfl_sync(0xffffffffu, xi[p >> 5], p & 31) : 0.0;
-            if (vr == 0.0 && vi == 0.0) continue;
-            for (int h = 0; h < 2; ++h) {
-                int i = lane + 32 * h;
-                if (i > p && i < w) {
-                    if (!CPLX) {
-                        xr[h] = add_rn(xr[h], mul_rn(-vr, sL[(size_t)p * w + i]));
-                    } else {
-                        Z lv{sL[((size_t)p * w + i) * 2], sL[((size_t)p * w + i) * 2 + 1]};
-                        Z r = zadd(Z{xr[h], xi[h]}, zmul(Z{-vr, -vi}, lv));
-                        xr[h] = r.re;
-                        xi[h] = r.im;
-                    }
-                }
-            }
-        }
-        for (int h = 0; h < 2; ++h) {
-            int i = lane + 32 * h;
-            if (i < w) {
-                x[(size_t)i * ES] = xr[h];
-                if (CPLX) x[(size_t)i * ES + 1] = xi[h];
-            }
-        }
-    }
-}
+// Triangular block solves, one warp per right-hand side column, w <= 64.
+//  kind 0: B := L^-1 B for the unit lower L at t, with the reference's order
+//          (x[i] += (-x[p]) * L[i, p] for p = 0..w-2, columns with x[p] == 0
+//          skipped; Triangular.SolveLowerUnit, Triangular.cs:26-57, and the
+//          complex BlockedLu.cs:312-327).
+//  kind 1: X := T^-1 X for the diagonal block of the blocked solves: lower or
+//          upper, unit or not, optionally the conjugate transpose of the stored
+//          block.
+struct TrsmDesc {
+    const double* t;
+    int ldt;
+    double* b;
+    int ldb, w, ncols;
+    int lower, unit, conj;
+};
 
-// Diagonal-block substitution for the blocked solves: X := T^-1 X with T the
-// w x w block (w <= 64) at `t`: lower or upper, unit or not, optionally the
-// conjugate transpose of the stored block. One warp per right-hand side.
-template <bool CPLX>
-__global__ void trsm_block_kernel(const double* t, int ldt, double* b, int ldb, int w, int ncols, bool lower, bool unit,
-                                  bool conj_trans) {
+template <bool CPLX, int KIND>
+__global__ void trsm_kernel(const __grid_constant__ Batch<TrsmDesc> bt) {
+    const TrsmDesc& d = batch_item(bt, blockIdx.y);
     constexpr int ES = CPLX ? 2 : 1;
     extern __shared__ double sT[];  // effective operator, w x w, ld w: op(i, p)
+    const int w = d.w;
+    if (d.ncols <= 0 || (int)(blockIdx.x * (blockDim.x >> 5)) >= d.ncols) return;  // nothing for this block
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         int i = e % w, p = e / w;
-        // op(i, p) = stored(i, p), or conj(stored(p, i)) for the adjoint
-        int si = conj_trans ? p : i, sp = conj_trans ? i : p;
-        sT[(size_t)e * ES] = t[((size_t)sp * ldt + si) * ES];
-        if (CPLX) sT[(size_t)e * ES + 1] = conj_trans ? -t[((size_t)sp * ldt + si) * ES + 1] : t[((size_t)sp * ldt + si) * ES + 1];
+        int si = d.conj ? p : i, sp = d.conj ? i : p;
+        const double* src = d.t + ((size_t)sp * d.ldt + si) * ES;
+        sT[(size_t)e * ES] = src[0];
+        if (CPLX) sT[(size_t)e * ES + 1] = d.conj ? -src[1] : src[1];
     }
     __syncthreads();
-    int lane = threadIdx.x & 31;
-    int warps = blockDim.x >> 5;
-    for (int c = blockIdx.x * warps + (threadIdx.x >> 5); c < ncols; c += gridDim.x * warps) {
-        double* x = b + (size_t)c * ldb * ES;
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int c = blockIdx.x * warps + (threadIdx.x >> 5); c < d.ncols; c += gridDim.x * warps) {
+        double* x = d.b + (size_t)c * d.ldb * ES;
         Z v[2];
         for (int h = 0; h < 2; ++h) {
             int i = lane + 32 * h;
             v[h].re = i < w ? x[(size_t)i * ES] : 0.0;
             v[h].im = (CPLX && i < w) ? x[(size_t)i * ES + 1] : 0.0;
         }
-        for (int s = 0; s < w; ++s) {
+        const int steps = KIND == 0 ? w - 1 : w;
+        for (int s = 0; s < steps; ++s) {
+            const bool lower = KIND == 0 ? true : d.lower != 0;
             int p = lower ? s : w - 1 - s;
             int h = p >> 5, src = p & 31;
-            if (!unit) {
+            if (KIND == 1 && !d.unit) {
                 if (lane == src) {
                     if (!CPLX) {
                         v[h].re = __ddiv_rn(v[h].re, sT[(size_t)p * w + p]);
                     } else {
-                        Z d{sT[((size_t)p * w + p) * 2], sT[((size_t)p * w + p) * 2 + 1]};
-                        v[h] = zdiv(v[h], d);
+                        Z dg{sT[((size_t)p * w + p) * 2], sT[((size_t)p * w + p) * 2 + 1]};
+                        v[h] = zdiv(v[h], dg);
                     }
                 }
             }
             double vr = __shfl_sync(0xffffffffu, v[h].re, src);
             double vi = CPLX ? __shfl_sync(0xffffffffu, v[h].im, src) : 0.0;
+            if (KIND == 0 && vr == 0.0 && vi == 0.0) continue;
             for (int q = 0; q < 2; ++q) {
                 int i = lane + 32 * q;
-                bool below = lower ? (i > p) : (i < p);
-                if (below && i < w) {
+                bool beyond = lower ? (i > p) : (i < p);
+                if (beyond && i < w) {
                     if (!CPLX) {
                         v[q].re = add_rn(v[q].re, mul_rn(-vr, sT[(size_t)p * w + i]));
                     } else {
@@ -357,109 +345,119 @@ __global__ void pivot_range_kernel(const double* a, int ld, int limit, double* o
     }
 }
 
-__global__ void init_int_kernel(int* p, int v) { *p = v; }
-
-// The 64 x 64 complex block needs 64 KB of dynamic shared memory, above the
-// default 48 KB, so the triangular kernels opt in before each launch (the
-// attribute is per kernel; real and complex instances share a signature, so
-// no static flag can tell them apart).
-template <class K>
-void allow_64k_smem(Context&, K kernel) {
-    TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 16));
+__global__ void fill_int_kernel(int* p, int count, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] = v;
 }
 
-template <bool CPLX>
-void launch_trsm_lower_unit(Context& ctx, const double* l, int ldl, double* b, int ldb, int w, int ncols) {
-    if (ncols <= 0 || w <= 1) return;
-    allow_64k_smem(ctx, trsm_lower_unit_kernel<CPLX>);
-    int threads = 256;
-    int warps = threads / 32;
-    int grid = std::min((ncols + warps - 1) / warps, ctx.num_sms * 4);
-    size_t smem = (size_t)w * w * (CPLX ? 16 : 8);
-    trsm_lower_unit_kernel<CPLX><<<grid, threads, smem, ctx.stream>>>(l, ldl, b, ldb, w, ncols);
+// ---- launchers ---------------------------------------------------------------
+
+void launch_panels(Context& ctx, bool cplx, std::vector<PanelFactorDesc>& v) {
+    if (v.empty()) return;
+    Batch<PanelFactorDesc> b = make_batch(ctx, v);
+    if (cplx) panel_kernel<true><<<b.count, 512, 0, ctx.stream>>>(b);
+    else panel_kernel<false><<<b.count, 512, 0, ctx.stream>>>(b);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
 }
 
-template <bool CPLX>
-void launch_trsm_block(Context& ctx, const double* t, int ldt, double* b, int ldb, int w, int ncols, bool lower, bool unit,
-                       bool conj_trans) {
-    if (ncols <= 0 || w <= 0) return;
-    allow_64k_smem(ctx, trsm_block_kernel<CPLX>);
-    int threads = 256;
-    int warps = threads / 32;
-    int grid = std::min((ncols + warps - 1) / warps, ctx.num_sms * 4);
-    size_t smem = (size_t)w * w * (CPLX ? 16 : 8);
-    trsm_block_kernel<CPLX><<<grid, threads, smem, ctx.stream>>>(t, ldt, b, ldb, w, ncols, lower, unit, conj_trans);
+void launch_laswp(Context& ctx, bool cplx, std::vector<LaswpDesc>& v) {
+    int maxc = 0;
+    std::vector<LaswpDesc> live;
+    for (auto& d : v)
+        if (d.c1 > d.c0 && d.k1 > d.k0) {
+            live.push_back(d);
+            maxc = std::max(maxc, d.c1 - d.c0);
+        }
+    if (live.empty()) return;
+    Batch<LaswpDesc> b = make_batch(ctx, live);
+    dim3 grid((maxc + 127) / 128, b.count);
+    if (cplx) laswp_kernel<true><<<grid, 128, 0, ctx.stream>>>(b);
+    else laswp_kernel<false><<<grid, 128, 0, ctx.stream>>>(b);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
 }
 
-void launch_laswp(Context& ctx, bool cplx, double* a, int ld, int c0, int c1, const int* piv, int k0, int k1, bool reverse) {
-    if (c1 <= c0 || k1 <= k0) return;
-    int n = c1 - c0;
-    if (cplx)
-        laswp_kernel<true><<<(n + 127) / 128, 128, 0, ctx.stream>>>(a, ld, c0, c1, piv, k0, k1, reverse);
-    else
-        laswp_kernel<false><<<(n + 127) / 128, 128, 0, ctx.stream>>>(a, ld, c0, c1, piv, k0, k1, reverse);
+template <bool CPLX, int KIND>
+void launch_trsm_t(Context& ctx, std::vector<TrsmDesc>& live, int maxcols) {
+    // The 64 x 64 complex block needs 64 KB of dynamic shared memory, above
+    // the default 48 KB; the attribute is per kernel instance.
+    TNS_CUDA(cudaFuncSetAttribute(trsm_kernel<CPLX, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 16));
+    Batch<TrsmDesc> b = make_batch(ctx, live);
+    const int threads = 256, warps = threads / 32;
+    int per_item = std::max(1, std::min((maxcols + warps - 1) / warps, std::max(1, ctx.num_sms * 4 / (int)live.size())));
+    int wmax = 0;
+    for (auto& d : live) wmax = std::max(wmax, d.w);
+    size_t smem = (size_t)wmax * wmax * (CPLX ? 16 : 8);
+    trsm_kernel<CPLX, KIND><<<dim3(per_item, b.count), threads, smem, ctx.stream>>>(b);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
 }
 
-// Element offset (in doubles) of (i, j) in a padded matrix.
+void launch_trsm(Context& ctx, bool cplx, int kind, std::vector<TrsmDesc>& v) {
+    std::vector<TrsmDesc> live;
+    int maxcols = 0;
+    for (auto& d : v)
+        if (d.ncols > 0 && d.w > (kind == 0 ? 1 : 0)) {
+            live.push_back(d);
+            maxcols = std::max(maxcols, d.ncols);
+        }
+    if (live.empty()) return;
+    if (cplx) {
+        if (kind == 0) launch_trsm_t<true, 0>(ctx, live, maxcols);
+        else launch_trsm_t<true, 1>(ctx, live, maxcols);
+    } else {
+        if (kind == 0) launch_trsm_t<false, 0>(ctx, live, maxcols);
+        else launch_trsm_t<false, 1>(ctx, live, maxcols);
+    }
+}
+
 inline size_t off(const DMat& a, int i, int j) { return ((size_t)j * a.ld() + i) * (a.cplx ? 2 : 1); }
 
 }  // namespace
 
-LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
-    LuResult res;
-    int limit = std::min(m, n);
-    if (limit == 0) return res;
-    if (nb < 1) nb = std::min(m, n) < 1024 ? 32 : 64;
-    // The GEMM wants K % 16 == 0 and the panel's pivot row buffer holds 64.
-    nb = std::max(16, std::min(64, (nb + 15) / 16 * 16));
-    const bool cplx = a.cplx;
-    const int ld = a.ld();
-    DBuf flags(ctx, sizeof(int) + 2 * sizeof(double) + 8);
-    int* d_sing = flags.as<int>();
-    double* d_range = reinterpret_cast<double*>(flags.as<char>() + 8);
-    init_int_kernel<<<1, 1, 0, ctx.stream>>>(d_sing, INT_MAX);
-    ctx.kernel_launches++;
+// ---------------------------------------------------------------------------
 
-    auto panel = [&](int r0, int w) {
-        if (cplx)
-            panel_kernel<true><<<1, 512, 0, ctx.stream>>>(a.p, ld, m, r0, w, d_piv, d_sing);
-        else
-            panel_kernel<false><<<1, 512, 0, ctx.stream>>>(a.p, ld, m, r0, w, d_piv, d_sing);
-        TNS_CUDA(cudaGetLastError());
+int reference_block_size(int m, int n) { return std::min(m, n) < 1024 ? 32 : 64; }
+
+void getrf_batch(Context& ctx, std::vector<LuItem>& items) {
+    if (items.empty()) return;
+    const bool cplx = items[0].a->cplx;
+    int max_steps = 0;
+    for (auto& it : items) {
+        int limit = std::min(it.m, it.n);
+        if (it.nb < 1) it.nb = reference_block_size(it.m, it.n);
+        // The GEMM wants K % 16 == 0 and the panel's pivot-row buffer holds 64.
+        it.nb = std::max(16, std::min(64, (it.nb + 15) / 16 * 16));
+        fill_int_kernel<<<1, 1, 0, ctx.stream>>>(it.d_sing, 1, INT_MAX);
         ctx.kernel_launches++;
-    };
-
-    if (nb >= limit) {
-        // Whole-matrix panel (Lu.cs:244-249): factor n columns at once is only
-        // possible when n <= 64 (pivot-row buffer); wider unblocked shapes go
-        // through the blocked path, which gives the same pivots.
-        if (n <= 64) {
-            panel(0, n);
-        } else {
-            panel(0, limit);
-            launch_laswp(ctx, cplx, a.p, ld, limit, n, d_piv, 0, limit, false);
-            if (cplx)
-                launch_trsm_lower_unit<true>(ctx, a.p, ld, a.p + off(a, 0, limit), ld, limit, n - limit);
-            else
-                launch_trsm_lower_unit<false>(ctx, a.p, ld, a.p + off(a, 0, limit), ld, limit, n - limit);
-        }
-    } else {
-        for (int jb = 0; jb < limit; jb += nb) {
-            int w = std::min(nb, limit - jb);
-            panel(jb, w);
-            launch_laswp(ctx, cplx, a.p, ld, 0, jb, d_piv, jb, jb + w, false);
+        if (limit == 0) continue;
+        // A whole-matrix panel (Lu.cs:244-249) when it fits one panel launch.
+        int steps = (it.nb >= limit && it.n <= 64) ? 1 : (limit + it.nb - 1) / it.nb;
+        max_steps = std::max(max_steps, steps);
+    }
+    for (int k = 0; k < max_steps; ++k) {
+        std::vector<PanelFactorDesc> panels;
+        std::vector<LaswpDesc> swaps;
+        std::vector<TrsmDesc> trsms;
+        std::vector<GemmProblem> gemms;
+        for (auto& it : items) {
+            DMat& a = *it.a;
+            const int m = it.m, n = it.n, ld = a.ld();
+            const int limit = std::min(m, n);
+            if (limit == 0) continue;
+            if (it.nb >= limit && n <= 64) {
+                if (k == 0) panels.push_back(PanelFactorDesc{a.p, ld, m, 0, n, it.d_piv, it.d_sing});
+                continue;
+            }
+            const int jb = k * it.nb;
+            if (jb >= limit) continue;
+            const int w = std::min(it.nb, limit - jb);
+            panels.push_back(PanelFactorDesc{a.p, ld, m, jb, w, it.d_piv, it.d_sing});
+            swaps.push_back(LaswpDesc{a.p, ld, 0, jb, it.d_piv, jb, jb + w, 0});
             if (jb + w >= n) continue;
-            launch_laswp(ctx, cplx, a.p, ld, jb + w, n, d_piv, jb, jb + w, false);
-            if (cplx)
-                launch_trsm_lower_unit<true>(ctx, a.p + off(a, jb, jb), ld, a.p + off(a, jb, jb + w), ld, w, n - jb - w);
-            else
-                launch_trsm_lower_unit<false>(ctx, a.p + off(a, jb, jb), ld, a.p + off(a, jb, jb + w), ld, w, n - jb - w);
+            swaps.push_back(LaswpDesc{a.p, ld, jb + w, n, it.d_piv, jb, jb + w, 0});
+            trsms.push_back(TrsmDesc{a.p + off(a, jb, jb), ld, a.p + off(a, jb, jb + w), ld, w, n - jb - w, 1, 1, 0});
             if (jb + w >= m) continue;
             GemmProblem p{};
             p.A = a.p + off(a, jb + w, jb);
@@ -471,13 +469,126 @@ LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
             p.K = w;
             p.alpha_re = -1.0;
             p.beta_re = 1.0;
-            gemm(ctx, p, cplx);
+            p.work = (long long)(m - jb - w) * (n - jb - w) * w;
+            gemms.push_back(p);
+        }
+        launch_panels(ctx, cplx, panels);
+        launch_laswp(ctx, cplx, swaps);
+        launch_trsm(ctx, cplx, 0, trsms);
+        if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
+    }
+}
+
+void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
+    if (items.empty()) return;
+    const bool cplx = items[0].lu->cplx;
+    const int bs = 64;
+    const size_t es = cplx ? 2 : 1;
+    int max_blocks = 0;
+    std::vector<DMat> herm;  // conjugate transposes for the adjoint solves
+    for (auto& it : items) {
+        int n = it.lu->rows;
+        if (n == 0 || it.nrhs == 0) continue;
+        max_blocks = std::max(max_blocks, (n + bs - 1) / bs);
+    }
+    if (adjoint) {
+        herm.reserve(items.size());
+        for (auto& it : items) {
+            herm.emplace_back(ctx, it.lu->cols, it.lu->rows, cplx, "the conjugate transpose of the factors");
+            conj_transpose(ctx, herm.back(), *it.lu);
         }
     }
-    if (cplx)
-        pivot_range_kernel<true><<<1, 256, 0, ctx.stream>>>(a.p, ld, limit, d_range);
+    auto update = [&](std::vector<GemmProblem>& v, const double* A, int lda, const double* X, double* C, int ldb,
+                      int rows, int k, int nrhs) {
+        if (rows <= 0) return;
+        GemmProblem p{};
+        p.A = A;
+        p.B = X;
+        p.C = C;
+        p.lda = lda;
+        p.ldb = p.ldc = ldb;
+        p.M = round_up(rows, 2);
+        p.N = round_up(nrhs, 2);
+        p.K = round_up(k, 16);
+        p.alpha_re = -1.0;
+        p.beta_re = 1.0;
+        v.push_back(p);
+    };
+    if (!adjoint) {
+        std::vector<LaswpDesc> swaps;
+        for (auto& it : items) {
+            int n = it.lu->rows;
+            if (n == 0 || it.nrhs == 0) continue;
+            swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
+        }
+        launch_laswp(ctx, cplx, swaps);
+    }
+    // Pass 1: forward (L, unit; or U^H, non-unit, for the adjoint).
+    for (int kb = 0; kb < max_blocks; ++kb) {
+        std::vector<TrsmDesc> diag;
+        std::vector<GemmProblem> gemms;
+        for (size_t q = 0; q < items.size(); ++q) {
+            auto& it = items[q];
+            const DMat& F = *it.lu;
+            int n = F.rows, ld = F.ld(), ldb = it.b->ld();
+            int k0 = kb * bs;
+            if (n == 0 || it.nrhs == 0 || k0 >= n) continue;
+            int w = std::min(bs, n - k0);
+            double* B = it.b->p;
+            diag.push_back(TrsmDesc{F.p + ((size_t)k0 * ld + k0) * es, ld, B + (size_t)k0 * es, ldb, w, it.nrhs, 1,
+                                    adjoint ? 0 : 1, adjoint ? 1 : 0});
+            const double* A = adjoint ? herm[q].p + ((size_t)k0 * herm[q].ld() + k0 + w) * es
+                                      : F.p + ((size_t)k0 * ld + k0 + w) * es;
+            update(gemms, A, adjoint ? herm[q].ld() : ld, B + (size_t)k0 * es, B + (size_t)(k0 + w) * es, ldb,
+                   n - k0 - w, w, it.nrhs);
+        }
+        launch_trsm(ctx, cplx, 1, diag);
+        if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
+    }
+    // Pass 2: backward (U, non-unit; or L^H, unit, for the adjoint).
+    for (int kb = max_blocks - 1; kb >= 0; --kb) {
+        std::vector<TrsmDesc> diag;
+        std::vector<GemmProblem> gemms;
+        for (size_t q = 0; q < items.size(); ++q) {
+            auto& it = items[q];
+            const DMat& F = *it.lu;
+            int n = F.rows, ld = F.ld(), ldb = it.b->ld();
+            int k0 = kb * bs;
+            if (n == 0 || it.nrhs == 0 || k0 >= n) continue;
+            int w = std::min(bs, n - k0);
+            double* B = it.b->p;
+            diag.push_back(TrsmDesc{F.p + ((size_t)k0 * ld + k0) * es, ld, B + (size_t)k0 * es, ldb, w, it.nrhs, 0,
+                                    adjoint ? 1 : 0, adjoint ? 1 : 0});
+            const double* A = adjoint ? herm[q].p + ((size_t)k0 * herm[q].ld()) * es : F.p + ((size_t)k0 * ld) * es;
+            update(gemms, A, adjoint ? herm[q].ld() : ld, B + (size_t)k0 * es, B, ldb, k0, w, it.nrhs);
+        }
+        launch_trsm(ctx, cplx, 1, diag);
+        if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
+    }
+    if (adjoint) {
+        std::vector<LaswpDesc> swaps;
+        for (auto& it : items) {
+            int n = it.lu->rows;
+            if (n == 0 || it.nrhs == 0) continue;
+            swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 1});
+        }
+        launch_laswp(ctx, cplx, swaps);
+    }
+}
+
+LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
+    LuResult res;
+    int limit = std::min(m, n);
+    if (limit == 0) return res;
+    DBuf flags(ctx, sizeof(int) + 2 * sizeof(double) + 8);
+    int* d_sing = flags.as<int>();
+    double* d_range = reinterpret_cast<double*>(flags.as<char>() + 8);
+    std::vector<LuItem> items{LuItem{&a, m, n, nb, d_piv, d_sing}};
+    getrf_batch(ctx, items);
+    if (a.cplx)
+        pivot_range_kernel<true><<<1, 256, 0, ctx.stream>>>(a.p, a.ld(), limit, d_range);
     else
-        pivot_range_kernel<false><<<1, 256, 0, ctx.stream>>>(a.p, ld, limit, d_range);
+        pivot_range_kernel<false><<<1, 256, 0, ctx.stream>>>(a.p, a.ld(), limit, d_range);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
     int h_sing = INT_MAX;
@@ -492,70 +603,8 @@ LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
 }
 
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint) {
-    const int n = lu.rows;
-    if (n == 0 || nrhs == 0) return;
-    const bool cplx = lu.cplx;
-    const int ld = lu.ld();
-    const int ldb = b.ld();
-    const int bs = 64;
-    double* B = b.p;
-    const double* F = lu.p;
-    auto trsm = [&](const double* t, double* x, int w, bool lower, bool unit, bool ct) {
-        if (cplx) launch_trsm_block<true>(ctx, t, ld, x, ldb, w, nrhs, lower, unit, ct);
-        else launch_trsm_block<false>(ctx, t, ld, x, ldb, w, nrhs, lower, unit, ct);
-    };
-    auto update = [&](const double* A, int lda, const double* X, double* C, int rows, int k) {
-        if (rows <= 0) return;
-        GemmProblem p{};
-        p.A = A;
-        p.B = X;
-        p.C = C;
-        p.lda = lda;
-        p.ldb = p.ldc = ldb;
-        p.M = round_up(rows, 2);
-        p.N = round_up(nrhs, 2);
-        p.K = round_up(k, 16);
-        p.alpha_re = -1.0;
-        p.beta_re = 1.0;
-        gemm(ctx, p, cplx);
-    };
-    const size_t es = cplx ? 2 : 1;
-    if (!adjoint) {
-        launch_laswp(ctx, cplx, B, ldb, 0, nrhs, d_piv, 0, n, false);
-        // L (unit lower): forward, block by block.
-        for (int k0 = 0; k0 < n; k0 += bs) {
-            int w = std::min(bs, n - k0);
-            trsm(F + ((size_t)k0 * ld + k0) * es, B + (size_t)k0 * es, w, true, true, false);
-            update(F + ((size_t)k0 * ld + k0 + w) * es, ld, B + (size_t)k0 * es, B + (size_t)(k0 + w) * es, n - k0 - w, w);
-        }
-        // U: backward.
-        int last = ((n - 1) / bs) * bs;
-        for (int k0 = last; k0 >= 0; k0 -= bs) {
-            int w = std::min(bs, n - k0);
-            trsm(F + ((size_t)k0 * ld + k0) * es, B + (size_t)k0 * es, w, false, false, false);
-            update(F + ((size_t)k0 * ld) * es, ld, B + (size_t)k0 * es, B, k0, w);
-        }
-    } else {
-        // A^H = U^H L^H P^T: solve U^H (lower, non-unit), then L^H (upper,
-        // unit), then undo the interchanges in reverse. The off-diagonal
-        // blocks are the conjugate transposes of stored blocks, formed once.
-        DMat fh(ctx, lu.cols, lu.rows, cplx, "the conjugate transpose of the factors");
-        conj_transpose(ctx, fh, lu);
-        const double* H = fh.p;
-        const int ldh = fh.ld();
-        for (int k0 = 0; k0 < n; k0 += bs) {
-            int w = std::min(bs, n - k0);
-            trsm(F + ((size_t)k0 * ld + k0) * es, B + (size_t)k0 * es, w, true, false, true);
-            update(H + ((size_t)k0 * ldh + k0 + w) * es, ldh, B + (size_t)k0 * es, B + (size_t)(k0 + w) * es, n - k0 - w, w);
-        }
-        int last = ((n - 1) / bs) * bs;
-        for (int k0 = last; k0 >= 0; k0 -= bs) {
-            int w = std::min(bs, n - k0);
-            trsm(F + ((size_t)k0 * ld + k0) * es, B + (size_t)k0 * es, w, false, true, true);
-            update(H + ((size_t)k0 * ldh) * es, ldh, B + (size_t)k0 * es, B, k0, w);
-        }
-        launch_laswp(ctx, cplx, B, ldb, 0, nrhs, d_piv, 0, n, true);
-    }
+    std::vector<SolveItem> items{SolveItem{&lu, d_piv, &b, nrhs}};
+    getrs_batch(ctx, items, adjoint);
 }
 
 }  // namespace tns

@@ -72,8 +72,13 @@ struct Context {
     long long max_elements = 2147483591LL;
     std::string last_error;
     long long kernel_launches = 0;  // kernels launched through this context
-    GemmProblem* d_probs = nullptr;
-    size_t d_probs_cap = 0;
+    // Launch descriptors go to the device through a ring of pinned host memory
+    // mirrored in device memory, so that uploading them never blocks the host
+    // on the stream. Wrapping around synchronises the stream once.
+    char* h_ring = nullptr;
+    char* d_ring = nullptr;
+    size_t ring_cap = 0, ring_pos = 0;
+    const void* upload(const void* src, size_t bytes);
 
     // Optional per-launch timing of the GEMM kernel (CUDA events on this
     // context's stream), for the roofline report.
@@ -89,12 +94,11 @@ struct Context {
     // Batched work runs on worker contexts (one host thread and one stream
     // each), created on first use, so that independent matrices overlap on
     // the GPU. Their counters are summed into this context's statistics.
-    int max_workers = 16;
+    int max_workers = 4;
     std::vector<std::unique_ptr<Context>> workers;
 
     explicit Context(int dev);
     ~Context();
-    GemmProblem* upload_problems(const std::vector<GemmProblem>& probs);
     void sync();                       // stream sync + device error flag check
     void check_limit(long long elements, const char* purpose) const;
 };
@@ -152,6 +156,48 @@ void gemm(Context& ctx, const GemmProblem& p, bool cplx);
 GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, double alpha_im, double beta_re,
                       double beta_im);
 
+// ---- batched streaming kernels (blas1.cu) ----------------------------------
+// Descriptors of one item each; a batch of them runs in one launch.
+struct EwDesc {
+    int op;
+    double* dst;
+    double* dst2;
+    const double* s1;
+    const double* s2;
+    size_t count;  // doubles
+    double f;
+    int rows_p, n, cplx;
+};
+struct SumDesc {  // moduli sums of an m x n block (or a fold of n values into out[0])
+    const double* a;
+    int m, n, ld;
+    double* out;
+};
+struct ChainDesc {  // the ell test's abs-power chain of one matrix
+    const double* a;
+    int n, ld;
+    double* mags;
+    double* row;
+    double* next;
+};
+struct PanelDesc {  // Y := A X (or A^H X), X and Y n x t
+    const double* a;
+    int n, ld;
+    const double* x;
+    int ldx;
+    double* y;
+    int ldy, t;
+};
+void ew_batch(Context& ctx, std::vector<EwDesc>& v);
+EwDesc ew_scaled_copy(DMat& dst, const DMat& src, double f);
+EwDesc ew_add_scaled(DMat& t, const DMat& s, double f);
+EwDesc ew_identity(DMat& dst, double f);
+EwDesc ew_pade_split(DMat& den, DMat& num, const DMat& v, const DMat& u);
+std::vector<double> norm1_batch(Context& ctx, const std::vector<const DMat*>& mats);
+std::vector<double> norminf_batch(Context& ctx, const std::vector<const DMat*>& mats);
+std::vector<double> abs_power_batch(Context& ctx, const std::vector<const DMat*>& mats, int p);
+void panel_product_batch(Context& ctx, std::vector<PanelDesc>& v, bool cplx, bool adjoint);
+
 // ---- elementwise and reductions (blas1.cu) ---------------------------------
 void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, double beta_re, double beta_im);
 // dst := src * f (real factor, each part scaled on its own), whole padded extent.
@@ -185,6 +231,25 @@ struct LuResult {
 };
 // In-place LU of the valid m x n block of a (padded). d_piv: device int[min(m,n)].
 LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv);
+// The reference's default block size (Lu.DefaultBlockSizeFor, Lu.cs:221-222).
+int reference_block_size(int m, int n);
+// A batch of independent factorizations, advanced block step by block step in
+// lockstep (one launch per phase per step). d_sing receives the first
+// singular column, or INT_MAX.
+struct LuItem {
+    DMat* a;
+    int m, n, nb;
+    int* d_piv;
+    int* d_sing;
+};
+void getrf_batch(Context& ctx, std::vector<LuItem>& items);
+struct SolveItem {
+    const DMat* lu;
+    const int* d_piv;
+    DMat* b;
+    int nrhs;
+};
+void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint);
 // B := A^-1 B or A^-H B from factors (valid n x n), in place on the valid rows of b.
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
 
@@ -199,8 +264,11 @@ NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv,
 struct ExpmInfo {
     int degree = 0, squarings = 0;
 };
-// result := exp(a) for the valid n x n block.
+// result := exp(a) for the valid n x n block (n >= 2).
 void expm(Context& ctx, const DMat& a, DMat& result, ExpmInfo* info);
+// The same for a batch of matrices of any orders >= 2, one launch per phase.
+void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,
+                std::vector<ExpmInfo>& infos);
 
 struct ExpmvInfo {
     int degree = 0, scaling = 0, applications = 0, early_exits = 0;

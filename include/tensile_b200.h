@@ -163,8 +163,9 @@ int tns_zexpm_batched(tns_context* ctx, int count, const int* orders, const doub
                       const int* lda, double* const* out, const int* ldo, tns_expm_info* infos);
 int tns_zexpm_batched_device(tns_context* ctx, int count, const int* orders, const double* const* a,
                              const int* lda, double* const* out, const int* ldo, tns_expm_info* infos);
-/* How many matrices of a batch run concurrently (each on its own host thread
- * and CUDA stream, largest first). Default 16. */
+/* How many groups a batch is split into. Each group (cost-balanced, n^3 as the
+ * cost) runs the batched algorithm -- one launch per phase for all its
+ * matrices -- on its own host thread and CUDA stream. Default 4. */
 int tns_set_workers(tns_context* ctx, int workers);
 
 /* ---- action of the exponential ------------------------------------------ */
