@@ -74,6 +74,7 @@ SIGNATURES = {
     "tns_zexpm_batched_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "tns_dexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_zgemm_device_noalloc": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
     "tns_set_workers": (_I, [_P, _I]),
     "tns_get_stats": (_I, [_P, C.POINTER(Stats)]),
     "tns_reset_stats": (_I, [_P]),

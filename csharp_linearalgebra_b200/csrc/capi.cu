@@ -405,6 +405,8 @@ void reset_stats(Context& ctx) {
 
 }  // namespace
 
+void tns::set_detached_error(const std::string& msg) { g_error_no_ctx = msg; }
+
 extern "C" {
 
 int tns_create(int device, long long max_elements, tns_context** out) {

@@ -445,4 +445,43 @@ void gemm(Context& ctx, const GemmProblem& p, bool cplx) {
     gemm_grouped(ctx, v, cplx);
 }
 
+namespace {
+template <class Cfg>
+void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p) {
+    TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+    p.tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM;
+    p.tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
+    p.tile_begin = 0;
+    int total = p.tiles_m * p.tiles_n;
+    if (total == 0) return;
+    GemmLaunch L{};
+    L.inl[0] = p;
+    L.list = nullptr;
+    L.nprob = 1;
+    L.total_tiles = total;
+    L.err = d_err;
+    int ctas_per_sm = 1;
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
+    int grid = std::min(total, std::max(1, ctas_per_sm) * num_sms);
+    gemm_dmma_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(L);
+    TNS_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+// One complex product launched on a caller's stream without a context: the
+// problem's operands and its P + iQ workspace (W) are the caller's, nothing is
+// allocated and nothing is uploaded (the problem travels in the launch
+// parameters). Same kernel, tiles and KC rule as gemm().
+void gemm_detached_complex(cudaStream_t stream, int device, int* d_err, const GemmProblem& p0) {
+    GemmProblem p = p0;
+    if (p.kc <= 0) p.kc = reference_kc(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
+    check_problem(p, true);
+    if (p.M == 0 || p.N == 0 || p.K == 0) return;
+    int num_sms = 148;
+    TNS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    long long tiles = (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN);
+    if (tiles >= num_sms) launch_detached<CplxBig>(stream, num_sms, d_err, p);
+    else launch_detached<CplxSmall>(stream, num_sms, d_err, p);
+}
+
 }  // namespace tns

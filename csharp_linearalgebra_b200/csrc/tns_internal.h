@@ -155,6 +155,11 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx);
 void gemm(Context& ctx, const GemmProblem& p, bool cplx);
 GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, double alpha_im, double beta_re,
                       double beta_im);
+// One complex product on a caller's stream, with no context: allocates and
+// uploads nothing (the entry point for callers that cannot allocate).
+void gemm_detached_complex(cudaStream_t stream, int device, int* d_err, const GemmProblem& p);
+// The thread's message for errors raised outside any context (tns_last_error(NULL)).
+void set_detached_error(const std::string& msg);
 
 // ---- batched streaming kernels (blas1.cu) ----------------------------------
 // Descriptors of one item each; a batch of them runs in one launch.

@@ -187,6 +187,32 @@ int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, con
 int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
                double t, double* out, int ldo, tns_expmv_info* info);
 
+/* ---- complex product without allocation -------------------------------- */
+
+/* No counterpart in the reference: the reference's products run on the CPU
+ * with managed buffers and have no device memory to avoid.
+ *
+ * C := beta*C + alpha*A*B for complex device operands, the same 4M product and
+ * the same bits as tns_zgemm_device, for callers that may not allocate device
+ * memory when they need the product -- for instance a host application whose
+ * own allocator has reserved the GPU's memory up front, or a latency-critical
+ * loop that must not enter the driver's allocation path. It allocates nothing:
+ * its working storage is one fixed device array of 4,194,304 complex elements
+ * (64 MiB) inside the library, which every GPU that loads the library holds
+ * until the process exits. A product whose padded operands need more than that
+ * (roughly m*k + k*n + 2*m*n complex elements, with m rounded up to even and k
+ * to a multiple of 16) is refused with TNS_E_OUT_OF_RANGE; tns_last_error(NULL)
+ * says why. There is no context: stream is the caller's cudaStream_t (NULL for
+ * the default stream) on the current device, and the call returns when the
+ * product is in C.
+ *
+ * The first call on a device looks up the array's device address, with that
+ * device current; make that first call before any stream capture. All calls
+ * share the array, which keeps the previous call's contents; calls that
+ * overlap on the GPU (from several threads or streams) race on it. */
+int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const double* alpha, const double* a, int lda,
+                             const double* b, int ldb, const double* beta, double* c, int ldc);
+
 /* ---- diagnostics --------------------------------------------------------- */
 
 /* Counters of the work a context has issued, the device-side counterpart of
