@@ -85,3 +85,28 @@ def test_batched_matches_single(ws, orc):
         ref, info = orc.expm(a)
         assert (d.degree, d.squarings) == (info["degree"], info["squarings"])
         assert rel1(e, ref) <= TOL
+
+
+def test_frequency_sweep_matrices(ws, orc):
+    """Matrices of the benchmark's frequency sweep, A = -(G + i w C), at both
+    ends of the frequency range: degree and squarings equal the oracle's and
+    the batched result agrees to 1e-12."""
+    # orders below 200 so that the CPU oracle finishes quickly; the spectrum's
+    # scale (|A| ~ w) is the sweep's
+    rng = np.random.default_rng(9)
+    small = []
+    for k, w in enumerate(np.logspace(2.0, 6.0, 6)):
+        n = int(rng.integers(64, 200))
+        g = rng.standard_normal((n, n)) / math.sqrt(n)
+        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        d = np.exp(rng.uniform(math.log(1e-3), 0.0, n))
+        c = (q.T * d) @ q
+        c = 0.5 * (c + c.T)
+        small.append(np.asfortranarray(-(g + 1j * w * c)))
+    diags = []
+    outs = ws.expm_batched(small, diags)
+    for a, e, d in zip(small, outs, diags):
+        ref, info = orc.expm(a)
+        assert (d.degree, d.squarings) == (info["degree"], info["squarings"])
+        assert rel1(e, ref) <= TOL, rel1(e, ref)
+    assert max(d.squarings for d in diags) >= 15
