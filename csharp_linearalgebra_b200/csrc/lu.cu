@@ -305,6 +305,114 @@ __global__ void trsm_kernel(const __grid_constant__ Batch<TrsmDesc> bt) {
     }
 }
 
+// Triangular substitution in the reference's order, for any n: one CTA of
+// 512 threads per block of C right-hand sides; thread t owns rows t, t+512, ...
+// (RPT of them) of its C columns in registers. Step k publishes x[k] (after
+// the division, for a non-unit diagonal) through shared memory, double
+// buffered so one barrier per step suffices, and every row the step touches
+// applies its update -- so each x[i] receives exactly the reference's sequence
+// of operations:
+//   mode 0 (lower, unit):   x[i] += (-x[k]) * L[i,k], k = 0..n-2, i > k
+//                           (Triangular.SolveLowerUnit; BlockedLu.cs:312-327)
+//   mode 1 (upper):         x[k] /= U[k,k]; x[i] += (-x[k]) * U[i,k], i < k,
+//                           k = n-1..0 (Triangular.SolveUpper; BlockedLu.cs:329-352,
+//                           which skips a zero x[k] entirely)
+// Updates of a column whose x[k] is zero are skipped, as the reference skips
+// them (its real four-column kernels skip only when all four are zero, which
+// can change nothing but the sign of a zero). The adjoint solves accumulate
+// row by row in the reference (dot products), an order a right-looking sweep
+// cannot reproduce; they stay on the blocked path.
+struct SubstDesc {
+    const double* f;  // the factors (ld ldf)
+    int ldf;
+    double* x;  // right-hand sides, overwritten
+    int ldx, n, nrhs, mode;
+};
+
+template <bool CPLX, int RPT, int C>
+__global__ void __launch_bounds__(512) subst_kernel(const __grid_constant__ Batch<SubstDesc> b) {
+    const SubstDesc& d = batch_item(b, blockIdx.y);
+    constexpr int T = 512;
+    constexpr int ES = CPLX ? 2 : 1;
+    const int n = d.n, mode = d.mode;
+    const int c0 = blockIdx.x * C;
+    if (c0 >= d.nrhs || n == 0) return;  // whole block idle
+    __shared__ double s_x[2][C * 2];
+    const int tid = threadIdx.x;
+    Z v[RPT][C];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            int i = tid + r * T;
+            v[r][c] = Z{0.0, 0.0};
+            if (i < n && c0 + c < d.nrhs) {
+                const double* e = d.x + ((size_t)(c0 + c) * d.ldx + i) * ES;
+                v[r][c] = Z{e[0], CPLX ? e[1] : 0.0};
+            }
+        }
+    const bool forward = mode == 0;
+    const int steps = mode == 0 ? n - 1 : n;
+    for (int s = 0; s < steps; ++s) {
+        const int k = forward ? s : n - 1 - s;
+        const int owner = k % T, slot = k / T;
+        const int buf = s & 1;
+        if (tid == owner) {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                if (r != slot) continue;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    Z xk = v[r][c];
+                    if (mode == 1) {
+                        const double* dg = d.f + ((size_t)k * d.ldf + k) * ES;
+                        if (!CPLX) xk.re = __ddiv_rn(xk.re, dg[0]);
+                        else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, Z{dg[0], dg[1]});
+                        v[r][c] = xk;
+                    }
+                    s_x[buf][2 * c] = xk.re;
+                    s_x[buf][2 * c + 1] = xk.im;
+                }
+            }
+        }
+        __syncthreads();
+        Z xk[C];
+        bool live[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            xk[c] = Z{s_x[buf][2 * c], s_x[buf][2 * c + 1]};
+            live[c] = !(xk[c].re == 0.0 && xk[c].im == 0.0);
+        }
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + r * T;
+            if (i >= n) continue;
+            const bool touched = forward ? (i > k) : (i < k);
+            if (!touched) continue;
+            // the factor entry this row needs at this step: column k, row i
+            const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
+            const Z f{e[0], CPLX ? e[1] : 0.0};
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                if (!live[c]) continue;
+                if (!CPLX) v[r][c].re = add_rn(v[r][c].re, mul_rn(-xk[c].re, f.re));
+                else v[r][c] = zadd(v[r][c], zmul(Z{-xk[c].re, -xk[c].im}, f));  // x += (-xk) * f
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            int i = tid + r * T;
+            if (i < n && c0 + c < d.nrhs) {
+                double* e = d.x + ((size_t)(c0 + c) * d.ldx + i) * ES;
+                e[0] = v[r][c].re;
+                if (CPLX) e[1] = v[r][c].im;
+            }
+        }
+}
+
 // min / max |u_jj| over the diagonal (RecordPivotRange, Lu.cs:312-329). The
 // values are moduli (never -0), so Math.Min/Math.Max fold to the plain min and
 // max unless a NaN is present, which then wins; in that form the fold is
@@ -412,6 +520,42 @@ void launch_trsm(Context& ctx, bool cplx, int kind, std::vector<TrsmDesc>& v) {
     }
 }
 
+template <bool CPLX, int RPT>
+void launch_subst_t(Context& ctx, std::vector<SubstDesc>& v, int max_rhs) {
+    constexpr int C = RPT >= 16 ? 1 : 16 / RPT;
+    Batch<SubstDesc> b = make_batch(ctx, v);
+    dim3 grid((max_rhs + C - 1) / C, b.count);
+    subst_kernel<CPLX, RPT, C><<<grid, 512, 0, ctx.stream>>>(b);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
+
+void launch_subst(Context& ctx, bool cplx, std::vector<SubstDesc>& v) {
+    int max_n = 0, max_rhs = 0;
+    std::vector<SubstDesc> live;
+    for (auto& d : v)
+        if (d.n > 0 && d.nrhs > 0) {
+            live.push_back(d);
+            max_n = std::max(max_n, d.n);
+            max_rhs = std::max(max_rhs, d.nrhs);
+        }
+    if (live.empty()) return;
+    int rpt = (max_n + 511) / 512;
+    if (rpt > 16) fail(TNS_E_ARGUMENT, "triangular solve of order above 8192");
+#define TNS_SUBST(R)                                                        \
+    if (rpt <= R) {                                                         \
+        if (cplx) launch_subst_t<true, R>(ctx, live, max_rhs);              \
+        else launch_subst_t<false, R>(ctx, live, max_rhs);                  \
+        return;                                                             \
+    }
+    TNS_SUBST(1)
+    TNS_SUBST(2)
+    TNS_SUBST(4)
+    TNS_SUBST(8)
+    TNS_SUBST(16)
+#undef TNS_SUBST
+}
+
 inline size_t off(const DMat& a, int i, int j) { return ((size_t)j * a.ld() + i) * (a.cplx ? 2 : 1); }
 
 }  // namespace
@@ -515,15 +659,25 @@ void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
         v.push_back(p);
     };
     if (!adjoint) {
+        // P B, then L (unit lower) forward and U backward by substitution in
+        // the reference's order (Lu.Solve, Lu.cs:336-351; BlockedLu.Solve,
+        // BlockedLu.cs:105-118): the result matches the reference bit for bit.
         std::vector<LaswpDesc> swaps;
+        std::vector<SubstDesc> lower, upper;
         for (auto& it : items) {
             int n = it.lu->rows;
             if (n == 0 || it.nrhs == 0) continue;
             swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
+            lower.push_back(SubstDesc{it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs, 0});
+            upper.push_back(SubstDesc{it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs, 1});
         }
         launch_laswp(ctx, cplx, swaps);
+        launch_subst(ctx, cplx, lower);
+        launch_subst(ctx, cplx, upper);
+        return;
     }
-    // Pass 1: forward (L, unit; or U^H, non-unit, for the adjoint).
+    // The adjoint: blocked, 64-row diagonal blocks plus DMMA GEMM updates.
+    // Pass 1: forward (U^H, non-unit).
     for (int kb = 0; kb < max_blocks; ++kb) {
         std::vector<TrsmDesc> diag;
         std::vector<GemmProblem> gemms;
