@@ -15,9 +15,11 @@
 // the reference bit for bit. In a batch, step k of every matrix runs in one
 // launch per phase (a grouped GEMM for the trailing updates).
 //
-// Solves: 64-row diagonal-block substitution plus DMMA GEMM updates of the
-// rows below (a blocked, GEMM-based TRSM -- the reference's own planned next
-// step for its n-RHS solves).
+// Solves: forward and backward substitution in the reference's order (one CTA
+// per block of right-hand sides, rows in registers, one barrier per step), so
+// A^-1 B -- the Pade solve included -- matches the reference bit for bit. The
+// adjoint solves use 64-row diagonal blocks plus DMMA GEMM updates of the rows
+// beyond them (a blocked, GEMM-based TRSM).
 
 #include "batch.cuh"
 #include "device_util.cuh"
@@ -330,7 +332,7 @@ struct SubstDesc {
 };
 
 template <bool CPLX, int RPT, int C>
-__global__ void __launch_bounds__(512) subst_kernel(const __grid_constant__ Batch<SubstDesc> b) {
+__global__ void __launch_bounds__(512, 2) subst_kernel(const __grid_constant__ Batch<SubstDesc> b) {
     const SubstDesc& d = batch_item(b, blockIdx.y);
     constexpr int T = 512;
     constexpr int ES = CPLX ? 2 : 1;
@@ -353,7 +355,33 @@ __global__ void __launch_bounds__(512) subst_kernel(const __grid_constant__ Batc
         }
     const bool forward = mode == 0;
     const int steps = mode == 0 ? n - 1 : n;
-    for (int s = 0; s < steps; ++s) {
+    // The diagonal of the rows this thread owns (it divides them, mode 1).
+    Z dgv[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        int i = tid + r * T;
+        dgv[r] = Z{1.0, 0.0};
+        if (mode == 1 && i < n) {
+            const double* e = d.f + ((size_t)i * d.ldf + i) * ES;
+            dgv[r] = Z{e[0], CPLX ? e[1] : 0.0};
+        }
+    }
+    // Factor entries of one step (column k, this thread's rows), loaded one
+    // step ahead of their use so that the load overlaps a step of work.
+    auto load_f = [&](int s, Z (&f)[RPT]) {
+        const int k = forward ? s : n - 1 - s;
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + r * T;
+            const bool touched = s < steps && i < n && (forward ? (i > k) : (i < k));
+            f[r] = Z{0.0, 0.0};
+            if (touched) {
+                const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
+                f[r] = Z{e[0], CPLX ? e[1] : 0.0};
+            }
+        }
+    };
+    auto step = [&](int s, const Z (&f)[RPT]) {
         const int k = forward ? s : n - 1 - s;
         const int owner = k % T, slot = k / T;
         const int buf = s & 1;
@@ -365,9 +393,8 @@ __global__ void __launch_bounds__(512) subst_kernel(const __grid_constant__ Batc
                 for (int c = 0; c < C; ++c) {
                     Z xk = v[r][c];
                     if (mode == 1) {
-                        const double* dg = d.f + ((size_t)k * d.ldf + k) * ES;
-                        if (!CPLX) xk.re = __ddiv_rn(xk.re, dg[0]);
-                        else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, Z{dg[0], dg[1]});
+                        if (!CPLX) xk.re = __ddiv_rn(xk.re, dgv[r].re);
+                        else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, dgv[r]);
                         v[r][c] = xk;
                     }
                     s_x[buf][2 * c] = xk.re;
@@ -389,16 +416,21 @@ __global__ void __launch_bounds__(512) subst_kernel(const __grid_constant__ Batc
             if (i >= n) continue;
             const bool touched = forward ? (i > k) : (i < k);
             if (!touched) continue;
-            // the factor entry this row needs at this step: column k, row i
-            const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
-            const Z f{e[0], CPLX ? e[1] : 0.0};
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 if (!live[c]) continue;
-                if (!CPLX) v[r][c].re = add_rn(v[r][c].re, mul_rn(-xk[c].re, f.re));
-                else v[r][c] = zadd(v[r][c], zmul(Z{-xk[c].re, -xk[c].im}, f));  // x += (-xk) * f
+                if (!CPLX) v[r][c].re = add_rn(v[r][c].re, mul_rn(-xk[c].re, f[r].re));
+                else v[r][c] = zadd(v[r][c], zmul(Z{-xk[c].re, -xk[c].im}, f[r]));  // x += (-xk) * f
             }
         }
+    };
+    Z fa[RPT], fb[RPT];
+    load_f(0, fa);
+    for (int s = 0; s < steps; s += 2) {
+        load_f(s + 1, fb);
+        step(s, fa);
+        load_f(s + 2, fa);
+        if (s + 1 < steps) step(s + 1, fb);
     }
 #pragma unroll
     for (int r = 0; r < RPT; ++r)
@@ -522,7 +554,10 @@ void launch_trsm(Context& ctx, bool cplx, int kind, std::vector<TrsmDesc>& v) {
 
 template <bool CPLX, int RPT>
 void launch_subst_t(Context& ctx, std::vector<SubstDesc>& v, int max_rhs) {
-    constexpr int C = RPT >= 16 ? 1 : 16 / RPT;
+    // RPT * C values per thread (8 real, 4 complex) keep the kernel within 64
+    // registers, so that two 512-thread CTAs share an SM.
+    constexpr int W = CPLX ? 4 : 8;
+    constexpr int C = RPT >= W ? 1 : W / RPT;
     Batch<SubstDesc> b = make_batch(ctx, v);
     dim3 grid((max_rhs + C - 1) / C, b.count);
     subst_kernel<CPLX, RPT, C><<<grid, 512, 0, ctx.stream>>>(b);
