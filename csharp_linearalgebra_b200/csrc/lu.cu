@@ -445,6 +445,86 @@ __global__ void __launch_bounds__(512, 2) subst_kernel(const __grid_constant__ B
         }
 }
 
+// The same substitution for n <= 32 * RPT (up to 1024): one warp per
+// right-hand side, lane l holding rows l, l+32, ... in registers. Columns are
+// independent in the reference's order, so a warp needs no barrier: step k
+// broadcasts x[k] from its owner lane by shuffle and every lane updates its
+// rows beyond k. Eight warps of a CTA work on eight columns of one matrix and
+// share the diagonal (mode 1) through shared memory.
+template <bool CPLX, int RPT>
+__global__ void __launch_bounds__(256) subst_warp_kernel(const __grid_constant__ Batch<SubstDesc> b) {
+    const SubstDesc& d = batch_item(b, blockIdx.y);
+    constexpr int ES = CPLX ? 2 : 1;
+    __shared__ double s_diag[32 * RPT * 2];
+    const int n = d.n, mode = d.mode;
+    const int lane = threadIdx.x & 31;
+    const int col = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (blockIdx.x * 8 >= d.nrhs || n == 0) return;  // whole block idle
+    if (mode == 1) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double* e = d.f + ((size_t)i * d.ldf + i) * ES;
+            s_diag[2 * i] = e[0];
+            s_diag[2 * i + 1] = CPLX ? e[1] : 0.0;
+        }
+        __syncthreads();
+    }
+    if (col >= d.nrhs) return;
+    double* x = d.x + (size_t)col * d.ldx * ES;
+    Z v[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int i = lane + 32 * r;
+        v[r] = Z{0.0, 0.0};
+        if (i < n) v[r] = Z{x[(size_t)i * ES], CPLX ? x[(size_t)i * ES + 1] : 0.0};
+    }
+    auto update = [&](Z& t, int k, int i, Z xk) {
+        const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
+        if (!CPLX) t.re = add_rn(t.re, mul_rn(-xk.re, e[0]));
+        else t = zadd(t, zmul(Z{-xk.re, -xk.im}, Z{e[0], e[1]}));  // x += (-xk) * f
+    };
+    if (mode == 0) {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            for (int l = 0; l < 32; ++l) {
+                const int k = 32 * r + l;
+                if (k >= n - 1) break;
+                Z xk{__shfl_sync(0xffffffffu, v[r].re, l), CPLX ? __shfl_sync(0xffffffffu, v[r].im, l) : 0.0};
+                if (xk.re == 0.0 && xk.im == 0.0) continue;
+                if (lane > l && lane + 32 * r < n) update(v[r], k, lane + 32 * r, xk);
+#pragma unroll
+                for (int r2 = r + 1; r2 < RPT; ++r2)
+                    if (lane + 32 * r2 < n) update(v[r2], k, lane + 32 * r2, xk);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int r = RPT - 1; r >= 0; --r) {
+            for (int l = 31; l >= 0; --l) {
+                const int k = 32 * r + l;
+                if (k >= n) continue;
+                Z xk{__shfl_sync(0xffffffffu, v[r].re, l), CPLX ? __shfl_sync(0xffffffffu, v[r].im, l) : 0.0};
+                // Every lane divides the owner's value (the same operation), the owner keeps it.
+                const Z dg{s_diag[2 * k], s_diag[2 * k + 1]};
+                if (!CPLX) xk.re = __ddiv_rn(xk.re, dg.re);
+                else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, dg);
+                if (lane == l) v[r] = xk;
+                if (xk.re == 0.0 && xk.im == 0.0) continue;
+                if (lane < l) update(v[r], k, lane + 32 * r, xk);
+#pragma unroll
+                for (int r2 = 0; r2 < r; ++r2) update(v[r2], k, lane + 32 * r2, xk);
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n) {
+            x[(size_t)i * ES] = v[r].re;
+            if (CPLX) x[(size_t)i * ES + 1] = v[r].im;
+        }
+    }
+}
+
 // min / max |u_jj| over the diagonal (RecordPivotRange, Lu.cs:312-329). The
 // values are moduli (never -0), so Math.Min/Math.Max fold to the plain min and
 // max unless a NaN is present, which then wins; in that form the fold is
@@ -575,6 +655,39 @@ void launch_subst(Context& ctx, bool cplx, std::vector<SubstDesc>& v) {
             max_rhs = std::max(max_rhs, d.nrhs);
         }
     if (live.empty()) return;
+    // Orders up to 1024: one warp per right-hand side, one launch per size
+    // class (rows per lane 2, 4, ..., 32) so that small matrices do not carry
+    // the registers of large ones.
+    std::vector<SubstDesc> cls[5], rest;
+    for (auto& d : live) {
+        int need = (d.n + 31) / 32;
+        int c = need <= 2 ? 0 : need <= 4 ? 1 : need <= 8 ? 2 : need <= 16 ? 3 : need <= 32 ? 4 : -1;
+        if (c < 0) rest.push_back(d);
+        else cls[c].push_back(d);
+    }
+    auto warp_launch = [&](std::vector<SubstDesc>& v, auto kernel_real, auto kernel_cplx) {
+        if (v.empty()) return;
+        int mr = 0;
+        for (auto& d : v) mr = std::max(mr, d.nrhs);
+        Batch<SubstDesc> b = make_batch(ctx, v);
+        dim3 grid((mr + 7) / 8, b.count);
+        if (cplx) kernel_cplx<<<grid, 256, 0, ctx.stream>>>(b);
+        else kernel_real<<<grid, 256, 0, ctx.stream>>>(b);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    };
+    warp_launch(cls[0], subst_warp_kernel<false, 2>, subst_warp_kernel<true, 2>);
+    warp_launch(cls[1], subst_warp_kernel<false, 4>, subst_warp_kernel<true, 4>);
+    warp_launch(cls[2], subst_warp_kernel<false, 8>, subst_warp_kernel<true, 8>);
+    warp_launch(cls[3], subst_warp_kernel<false, 16>, subst_warp_kernel<true, 16>);
+    warp_launch(cls[4], subst_warp_kernel<false, 32>, subst_warp_kernel<true, 32>);
+    if (rest.empty()) return;
+    live = rest;
+    max_n = max_rhs = 0;
+    for (auto& d : live) {
+        max_n = std::max(max_n, d.n);
+        max_rhs = std::max(max_rhs, d.nrhs);
+    }
     int rpt = (max_n + 511) / 512;
     if (rpt > 16) fail(TNS_E_ARGUMENT, "triangular solve of order above 8192");
 #define TNS_SUBST(R)                                                        \
