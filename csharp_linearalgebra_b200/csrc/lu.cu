@@ -15,11 +15,12 @@
 // the reference bit for bit. In a batch, step k of every matrix runs in one
 // launch per phase (a grouped GEMM for the trailing updates).
 //
-// Solves: forward and backward substitution in the reference's order (one CTA
-// per block of right-hand sides, rows in registers, one barrier per step), so
-// A^-1 B -- the Pade solve included -- matches the reference bit for bit. The
-// adjoint solves use 64-row diagonal blocks plus DMMA GEMM updates of the rows
-// beyond them (a blocked, GEMM-based TRSM).
+// Solves: forward and backward substitution in the reference's order, blocked
+// into 32-row diagonal solves and register-tiled updates that continue each
+// element's chain of roundings in the reference's order, so A^-1 B -- the Pade
+// solve included -- matches the reference bit for bit. The adjoint solves use
+// 64-row diagonal blocks plus DMMA GEMM updates of the rows beyond them (a
+// blocked, GEMM-based TRSM).
 
 #include "batch.cuh"
 #include "device_util.cuh"
@@ -307,222 +308,209 @@ __global__ void trsm_kernel(const __grid_constant__ Batch<TrsmDesc> bt) {
     }
 }
 
-// Triangular substitution in the reference's order, for any n: one CTA of
-// 512 threads per block of C right-hand sides; thread t owns rows t, t+512, ...
-// (RPT of them) of its C columns in registers. Step k publishes x[k] (after
-// the division, for a non-unit diagonal) through shared memory, double
-// buffered so one barrier per step suffices, and every row the step touches
-// applies its update -- so each x[i] receives exactly the reference's sequence
-// of operations:
-//   mode 0 (lower, unit):   x[i] += (-x[k]) * L[i,k], k = 0..n-2, i > k
-//                           (Triangular.SolveLowerUnit; BlockedLu.cs:312-327)
-//   mode 1 (upper):         x[k] /= U[k,k]; x[i] += (-x[k]) * U[i,k], i < k,
-//                           k = n-1..0 (Triangular.SolveUpper; BlockedLu.cs:329-352,
-//                           which skips a zero x[k] entirely)
-// Updates of a column whose x[k] is zero are skipped, as the reference skips
-// them (its real four-column kernels skip only when all four are zero, which
-// can change nothing but the sign of a zero). The adjoint solves accumulate
-// row by row in the reference (dot products), an order a right-looking sweep
-// cannot reproduce; they stay on the blocked path.
-struct SubstDesc {
+// Triangular substitution in the reference's order. Per right-hand side
+// column the reference computes
+//   lower, unit:  x[i] += (-x[k]) * L[i,k],                  k = 0..n-2, i > k
+//                 (Triangular.SolveLowerUnit; BlockedLu.cs:312-327)
+//   upper:        x[k] /= U[k,k]; x[i] += (-x[k]) * U[i,k],  k = n-1..0, i < k
+//                 (Triangular.SolveUpper; BlockedLu.cs:329-352)
+// and skips every update of a column whose x[k] is zero (its real four-column
+// kernels skip only when all four x[k] are zero, which can change nothing but
+// the sign of a zero). So each x[i] receives one chain of roundings in the
+// order of k, and the chains of different (row, column) pairs are
+// independent. The rows are cut into blocks of 32; for each block, in the
+// order of k:
+//   1. subst_diag_kernel solves the block's own triangle, which completes
+//      x[k] for every k of the block;
+//   2. subst_update_kernel applies the block's steps to every row beyond it,
+//      continuing each row's chain from the value it holds, steps in order.
+// Blocking regroups whole chains and never reorders one, so every x[i] sees
+// the reference's operations in the reference's order and the solution
+// matches bit for bit; step 2, all but about 32/n of the work, runs as a
+// register-tiled product on every SM. The adjoint solves accumulate row by
+// row in the reference (dot products), an order a right-looking sweep cannot
+// reproduce; they stay on the blocked GEMM path.
+constexpr int kSubstBlock = 32;
+
+struct SubstDiagDesc {
     const double* f;  // the factors (ld ldf)
     int ldf;
-    double* x;  // right-hand sides, overwritten
-    int ldx, n, nrhs, mode;
+    double* x;  // right-hand sides (ld ldx), overwritten
+    int ldx, nrhs;
+    int k0, w;  // the block: rows and steps [k0, k0 + w)
 };
 
-template <bool CPLX, int RPT, int C>
-__global__ void __launch_bounds__(512, 2) subst_kernel(const __grid_constant__ Batch<SubstDesc> b) {
-    const SubstDesc& d = batch_item(b, blockIdx.y);
-    constexpr int T = 512;
-    constexpr int ES = CPLX ? 2 : 1;
-    const int n = d.n, mode = d.mode;
-    const int c0 = blockIdx.x * C;
-    if (c0 >= d.nrhs || n == 0) return;  // whole block idle
-    __shared__ double s_x[2][C * 2];
-    const int tid = threadIdx.x;
-    Z v[RPT][C];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r)
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            int i = tid + r * T;
-            v[r][c] = Z{0.0, 0.0};
-            if (i < n && c0 + c < d.nrhs) {
-                const double* e = d.x + ((size_t)(c0 + c) * d.ldx + i) * ES;
-                v[r][c] = Z{e[0], CPLX ? e[1] : 0.0};
-            }
-        }
-    const bool forward = mode == 0;
-    const int steps = mode == 0 ? n - 1 : n;
-    // The diagonal of the rows this thread owns (it divides them, mode 1).
-    Z dgv[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        int i = tid + r * T;
-        dgv[r] = Z{1.0, 0.0};
-        if (mode == 1 && i < n) {
-            const double* e = d.f + ((size_t)i * d.ldf + i) * ES;
-            dgv[r] = Z{e[0], CPLX ? e[1] : 0.0};
-        }
-    }
-    // Factor entries of one step (column k, this thread's rows), loaded one
-    // step ahead of their use so that the load overlaps a step of work.
-    auto load_f = [&](int s, Z (&f)[RPT]) {
-        const int k = forward ? s : n - 1 - s;
-#pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = tid + r * T;
-            const bool touched = s < steps && i < n && (forward ? (i > k) : (i < k));
-            f[r] = Z{0.0, 0.0};
-            if (touched) {
-                const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
-                f[r] = Z{e[0], CPLX ? e[1] : 0.0};
-            }
-        }
-    };
-    auto step = [&](int s, const Z (&f)[RPT]) {
-        const int k = forward ? s : n - 1 - s;
-        const int owner = k % T, slot = k / T;
-        const int buf = s & 1;
-        if (tid == owner) {
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                if (r != slot) continue;
-#pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    Z xk = v[r][c];
-                    if (mode == 1) {
-                        if (!CPLX) xk.re = __ddiv_rn(xk.re, dgv[r].re);
-                        else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, dgv[r]);
-                        v[r][c] = xk;
-                    }
-                    s_x[buf][2 * c] = xk.re;
-                    s_x[buf][2 * c + 1] = xk.im;
-                }
-            }
-        }
-        __syncthreads();
-        Z xk[C];
-        bool live[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            xk[c] = Z{s_x[buf][2 * c], s_x[buf][2 * c + 1]};
-            live[c] = !(xk[c].re == 0.0 && xk[c].im == 0.0);
-        }
-#pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = tid + r * T;
-            if (i >= n) continue;
-            const bool touched = forward ? (i > k) : (i < k);
-            if (!touched) continue;
-#pragma unroll
-            for (int c = 0; c < C; ++c) {
-                if (!live[c]) continue;
-                if (!CPLX) v[r][c].re = add_rn(v[r][c].re, mul_rn(-xk[c].re, f[r].re));
-                else v[r][c] = zadd(v[r][c], zmul(Z{-xk[c].re, -xk[c].im}, f[r]));  // x += (-xk) * f
-            }
-        }
-    };
-    Z fa[RPT], fb[RPT];
-    load_f(0, fa);
-    for (int s = 0; s < steps; s += 2) {
-        load_f(s + 1, fb);
-        step(s, fa);
-        load_f(s + 2, fa);
-        if (s + 1 < steps) step(s + 1, fb);
-    }
-#pragma unroll
-    for (int r = 0; r < RPT; ++r)
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            int i = tid + r * T;
-            if (i < n && c0 + c < d.nrhs) {
-                double* e = d.x + ((size_t)(c0 + c) * d.ldx + i) * ES;
-                e[0] = v[r][c].re;
-                if (CPLX) e[1] = v[r][c].im;
-            }
-        }
+struct SubstUpdateDesc {
+    const double* f;
+    int ldf;
+    double* x;
+    int ldx, nrhs;
+    int r0, r1;  // rows updated
+    int k0, k1;  // steps applied
+    int tiles_m, tile_begin;
+};
+
+// x + (-xk) * f with the reference's roundings: a product of two roundings
+// per part (no fused multiply-add), then the sum.
+template <bool CPLX>
+__device__ __forceinline__ Z subst_axpy(Z x, Z nxk, Z f) {
+    if (!CPLX) return Z{add_rn(x.re, mul_rn(nxk.re, f.re)), 0.0};
+    return zadd(x, zmul(nxk, f));
 }
 
-// The same substitution for n <= 32 * RPT (up to 1024): one warp per
-// right-hand side, lane l holding rows l, l+32, ... in registers. Columns are
-// independent in the reference's order, so a warp needs no barrier: step k
-// broadcasts x[k] from its owner lane by shuffle and every lane updates its
-// rows beyond k. Eight warps of a CTA work on eight columns of one matrix and
-// share the diagonal (mode 1) through shared memory.
-template <bool CPLX, int RPT>
-__global__ void __launch_bounds__(256) subst_warp_kernel(const __grid_constant__ Batch<SubstDesc> b) {
-    const SubstDesc& d = batch_item(b, blockIdx.y);
+// Step 1: the block's own triangle, one thread per right-hand side column,
+// the block's values in registers and its triangle in shared memory (every
+// thread reads the same entry at a time: a broadcast).
+template <bool CPLX, bool UPPER>
+__global__ void __launch_bounds__(128) subst_diag_kernel(const __grid_constant__ Batch<SubstDiagDesc> b) {
+    constexpr int B = kSubstBlock;
     constexpr int ES = CPLX ? 2 : 1;
-    __shared__ double s_diag[32 * RPT * 2];
-    const int n = d.n, mode = d.mode;
-    const int lane = threadIdx.x & 31;
-    const int col = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (blockIdx.x * 8 >= d.nrhs || n == 0) return;  // whole block idle
-    if (mode == 1) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const double* e = d.f + ((size_t)i * d.ldf + i) * ES;
-            s_diag[2 * i] = e[0];
-            s_diag[2 * i + 1] = CPLX ? e[1] : 0.0;
+    const SubstDiagDesc& d = batch_item(b, blockIdx.y);
+    if ((int)(blockIdx.x * blockDim.x) >= d.nrhs) return;  // whole block idle
+    const int w = d.w;
+    __shared__ Z t[B][B];  // t[k][i] = F[k0 + i, k0 + k]
+    for (int e = threadIdx.x; e < B * B; e += blockDim.x) {
+        const int k = e / B, i = e % B;
+        Z v{0.0, 0.0};
+        if (i < w && k < w) {
+            const double* p = d.f + ((size_t)(d.k0 + k) * d.ldf + d.k0 + i) * ES;
+            v = Z{p[0], CPLX ? p[1] : 0.0};
         }
-        __syncthreads();
+        t[k][i] = v;
     }
+    __syncthreads();
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.nrhs) return;
-    double* x = d.x + (size_t)col * d.ldx * ES;
-    Z v[RPT];
+    double* x = d.x + ((size_t)col * d.ldx + d.k0) * ES;
+    Z v[B];
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        const int i = lane + 32 * r;
-        v[r] = Z{0.0, 0.0};
-        if (i < n) v[r] = Z{x[(size_t)i * ES], CPLX ? x[(size_t)i * ES + 1] : 0.0};
+    for (int i = 0; i < B; ++i) {
+        v[i] = Z{0.0, 0.0};
+        if (i < w) v[i] = Z{x[(size_t)i * ES], CPLX ? x[(size_t)i * ES + 1] : 0.0};
     }
-    auto update = [&](Z& t, int k, int i, Z xk) {
-        const double* e = d.f + ((size_t)k * d.ldf + i) * ES;
-        if (!CPLX) t.re = add_rn(t.re, mul_rn(-xk.re, e[0]));
-        else t = zadd(t, zmul(Z{-xk.re, -xk.im}, Z{e[0], e[1]}));  // x += (-xk) * f
-    };
-    if (mode == 0) {
+    if (!UPPER) {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            for (int l = 0; l < 32; ++l) {
-                const int k = 32 * r + l;
-                if (k >= n - 1) break;
-                Z xk{__shfl_sync(0xffffffffu, v[r].re, l), CPLX ? __shfl_sync(0xffffffffu, v[r].im, l) : 0.0};
-                if (xk.re == 0.0 && xk.im == 0.0) continue;
-                if (lane > l && lane + 32 * r < n) update(v[r], k, lane + 32 * r, xk);
+        for (int k = 0; k < B - 1; ++k) {
+            const Z xk = v[k];
+            if (k >= w || (xk.re == 0.0 && xk.im == 0.0)) continue;
+            const Z nxk{-xk.re, -xk.im};
 #pragma unroll
-                for (int r2 = r + 1; r2 < RPT; ++r2)
-                    if (lane + 32 * r2 < n) update(v[r2], k, lane + 32 * r2, xk);
-            }
+            for (int i = k + 1; i < B; ++i)
+                if (i < w) v[i] = subst_axpy<CPLX>(v[i], nxk, t[k][i]);
         }
     } else {
 #pragma unroll
-        for (int r = RPT - 1; r >= 0; --r) {
-            for (int l = 31; l >= 0; --l) {
-                const int k = 32 * r + l;
-                if (k >= n) continue;
-                Z xk{__shfl_sync(0xffffffffu, v[r].re, l), CPLX ? __shfl_sync(0xffffffffu, v[r].im, l) : 0.0};
-                // Every lane divides the owner's value (the same operation), the owner keeps it.
-                const Z dg{s_diag[2 * k], s_diag[2 * k + 1]};
-                if (!CPLX) xk.re = __ddiv_rn(xk.re, dg.re);
-                else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, dg);
-                if (lane == l) v[r] = xk;
-                if (xk.re == 0.0 && xk.im == 0.0) continue;
-                if (lane < l) update(v[r], k, lane + 32 * r, xk);
+        for (int k = B - 1; k >= 0; --k) {
+            if (k >= w) continue;
+            Z xk = v[k];
+            const Z dg = t[k][k];
+            if (!CPLX) xk.re = __ddiv_rn(xk.re, dg.re);
+            else if (!(xk.re == 0.0 && xk.im == 0.0)) xk = zdiv(xk, dg);
+            v[k] = xk;
+            if (xk.re == 0.0 && xk.im == 0.0) continue;
+            const Z nxk{-xk.re, -xk.im};
 #pragma unroll
-                for (int r2 = 0; r2 < r; ++r2) update(v[r2], k, lane + 32 * r2, xk);
+            for (int i = 0; i < k; ++i) v[i] = subst_axpy<CPLX>(v[i], nxk, t[k][i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+        if (i < w) {
+            x[(size_t)i * ES] = v[i].re;
+            if (CPLX) x[(size_t)i * ES + 1] = v[i].im;
+        }
+}
+
+// Step 2: rows [r0, r1) of every column take the updates of steps [k0, k1)
+// (ascending for the lower factor, descending for the upper), 64 x 64 tiles
+// of (row, column) per CTA over a flat grid of every item's tiles. Thread
+// (tx, ty) keeps rows tx + 16 r and columns ty + 16 s (r, s < 4) in registers
+// from the value x already holds; each round stages 16 steps of the factor
+// column and of the solved x[k] in shared memory.
+template <bool CPLX, bool UPPER>
+__global__ void __launch_bounds__(256, 2) subst_update_kernel(const __grid_constant__ Batch<SubstUpdateDesc> b) {
+    constexpr int ES = CPLX ? 2 : 1;
+    constexpr int KC = 16;
+    int lo = 0, hi = b.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (batch_item(b, mid).tile_begin <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const SubstUpdateDesc& d = batch_item(b, lo);
+    const int tile = blockIdx.x - d.tile_begin;
+    const int i0 = d.r0 + (tile % d.tiles_m) * 64, c0 = (tile / d.tiles_m) * 64;
+    __shared__ Z sF[KC][64];
+    __shared__ Z sX[KC][64 + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    Z acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int i = i0 + tx + 16 * r, c = c0 + ty + 16 * s;
+            acc[r][s] = Z{0.0, 0.0};
+            if (i < d.r1 && c < d.nrhs) {
+                const double* p = d.x + ((size_t)c * d.ldx + i) * ES;
+                acc[r][s] = Z{p[0], CPLX ? p[1] : 0.0};
             }
         }
+    const int rounds = (d.k1 - d.k0 + KC - 1) / KC;
+    for (int q = 0; q < rounds; ++q) {
+        const int kq = UPPER ? d.k1 - (q + 1) * KC : d.k0 + q * KC;
+        for (int e = tid; e < KC * 64; e += 256) {
+            const int kk = e >> 6, r = e & 63;
+            const int k = kq + kk, i = i0 + r;
+            Z v{0.0, 0.0};
+            if (k >= d.k0 && k < d.k1 && i < d.r1) {
+                const double* p = d.f + ((size_t)k * d.ldf + i) * ES;
+                v = Z{p[0], CPLX ? p[1] : 0.0};
+            }
+            sF[kk][r] = v;
+        }
+        for (int e = tid; e < KC * 64; e += 256) {
+            const int kk = e % KC, c = e / KC;
+            const int k = kq + kk, col = c0 + c;
+            Z v{0.0, 0.0};  // steps outside [k0, k1) read as zero and are skipped
+            if (k >= d.k0 && k < d.k1 && col < d.nrhs) {
+                const double* p = d.x + ((size_t)col * d.ldx + k) * ES;
+                v = Z{p[0], CPLX ? p[1] : 0.0};
+            }
+            sX[kk][c] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < KC; ++j) {
+            const int kk = UPPER ? KC - 1 - j : j;
+            Z nxk[4];
+            bool live[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const Z xv = sX[kk][ty + 16 * s];
+                live[s] = !(xv.re == 0.0 && xv.im == 0.0);
+                nxk[s] = Z{-xv.re, -xv.im};
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const Z fv = sF[kk][tx + 16 * r];
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (live[s]) acc[r][s] = subst_axpy<CPLX>(acc[r][s], nxk[s], fv);
+            }
+        }
+        __syncthreads();
     }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        const int i = lane + 32 * r;
-        if (i < n) {
-            x[(size_t)i * ES] = v[r].re;
-            if (CPLX) x[(size_t)i * ES + 1] = v[r].im;
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int i = i0 + tx + 16 * r, c = c0 + ty + 16 * s;
+            if (i < d.r1 && c < d.nrhs) {
+                double* p = d.x + ((size_t)c * d.ldx + i) * ES;
+                p[0] = acc[r][s].re;
+                if (CPLX) p[1] = acc[r][s].im;
+            }
         }
-    }
 }
 
 // min / max |u_jj| over the diagonal (RecordPivotRange, Lu.cs:312-329). The
@@ -632,76 +620,41 @@ void launch_trsm(Context& ctx, bool cplx, int kind, std::vector<TrsmDesc>& v) {
     }
 }
 
-template <bool CPLX, int RPT>
-void launch_subst_t(Context& ctx, std::vector<SubstDesc>& v, int max_rhs) {
-    // RPT * C values per thread (8 real, 4 complex) keep the kernel within 64
-    // registers, so that two 512-thread CTAs share an SM.
-    constexpr int W = CPLX ? 4 : 8;
-    constexpr int C = RPT >= W ? 1 : W / RPT;
-    Batch<SubstDesc> b = make_batch(ctx, v);
-    dim3 grid((max_rhs + C - 1) / C, b.count);
-    subst_kernel<CPLX, RPT, C><<<grid, 512, 0, ctx.stream>>>(b);
-    TNS_CUDA(cudaGetLastError());
-    ctx.kernel_launches++;
-}
-
-void launch_subst(Context& ctx, bool cplx, std::vector<SubstDesc>& v) {
-    int max_n = 0, max_rhs = 0;
-    std::vector<SubstDesc> live;
-    for (auto& d : v)
-        if (d.n > 0 && d.nrhs > 0) {
-            live.push_back(d);
-            max_n = std::max(max_n, d.n);
-            max_rhs = std::max(max_rhs, d.nrhs);
-        }
-    if (live.empty()) return;
-    // Orders up to 1024: one warp per right-hand side, one launch per size
-    // class (rows per lane 2, 4, ..., 32) so that small matrices do not carry
-    // the registers of large ones.
-    std::vector<SubstDesc> cls[5], rest;
-    for (auto& d : live) {
-        int need = (d.n + 31) / 32;
-        int c = need <= 2 ? 0 : need <= 4 ? 1 : need <= 8 ? 2 : need <= 16 ? 3 : need <= 32 ? 4 : -1;
-        if (c < 0) rest.push_back(d);
-        else cls[c].push_back(d);
-    }
-    auto warp_launch = [&](std::vector<SubstDesc>& v, auto kernel_real, auto kernel_cplx) {
-        if (v.empty()) return;
+// One block step of the substitution for every item of a batch: the
+// diagonal blocks in one launch, then the updates of all items' tiles in one.
+template <bool CPLX, bool UPPER>
+void launch_subst_step_t(Context& ctx, std::vector<SubstDiagDesc>& diag, std::vector<SubstUpdateDesc>& upd) {
+    if (!diag.empty()) {
         int mr = 0;
-        for (auto& d : v) mr = std::max(mr, d.nrhs);
-        Batch<SubstDesc> b = make_batch(ctx, v);
-        dim3 grid((mr + 7) / 8, b.count);
-        if (cplx) kernel_cplx<<<grid, 256, 0, ctx.stream>>>(b);
-        else kernel_real<<<grid, 256, 0, ctx.stream>>>(b);
+        for (auto& d : diag) mr = std::max(mr, d.nrhs);
+        Batch<SubstDiagDesc> b = make_batch(ctx, diag);
+        subst_diag_kernel<CPLX, UPPER><<<dim3((mr + 127) / 128, b.count), 128, 0, ctx.stream>>>(b);
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches++;
-    };
-    warp_launch(cls[0], subst_warp_kernel<false, 2>, subst_warp_kernel<true, 2>);
-    warp_launch(cls[1], subst_warp_kernel<false, 4>, subst_warp_kernel<true, 4>);
-    warp_launch(cls[2], subst_warp_kernel<false, 8>, subst_warp_kernel<true, 8>);
-    warp_launch(cls[3], subst_warp_kernel<false, 16>, subst_warp_kernel<true, 16>);
-    warp_launch(cls[4], subst_warp_kernel<false, 32>, subst_warp_kernel<true, 32>);
-    if (rest.empty()) return;
-    live = rest;
-    max_n = max_rhs = 0;
-    for (auto& d : live) {
-        max_n = std::max(max_n, d.n);
-        max_rhs = std::max(max_rhs, d.nrhs);
     }
-    int rpt = (max_n + 511) / 512;
-    if (rpt > 16) fail(TNS_E_ARGUMENT, "triangular solve of order above 8192");
-#define TNS_SUBST(R)                                                        \
-    if (rpt <= R) {                                                         \
-        if (cplx) launch_subst_t<true, R>(ctx, live, max_rhs);              \
-        else launch_subst_t<false, R>(ctx, live, max_rhs);                  \
-        return;                                                             \
+    if (!upd.empty()) {
+        long long total = 0;
+        for (auto& u : upd) {
+            u.tile_begin = (int)total;
+            total += (long long)u.tiles_m * ((u.nrhs + 63) / 64);
+        }
+        if (total > INT_MAX) fail(TNS_E_ARGUMENT, "triangular solve too large for one launch");
+        Batch<SubstUpdateDesc> b = make_batch(ctx, upd);
+        subst_update_kernel<CPLX, UPPER><<<(unsigned)total, 256, 0, ctx.stream>>>(b);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
     }
-    TNS_SUBST(1)
-    TNS_SUBST(2)
-    TNS_SUBST(4)
-    TNS_SUBST(8)
-    TNS_SUBST(16)
-#undef TNS_SUBST
+}
+
+void launch_subst_step(Context& ctx, bool cplx, bool upper, std::vector<SubstDiagDesc>& diag,
+                       std::vector<SubstUpdateDesc>& upd) {
+    if (cplx) {
+        if (upper) launch_subst_step_t<true, true>(ctx, diag, upd);
+        else launch_subst_step_t<true, false>(ctx, diag, upd);
+    } else {
+        if (upper) launch_subst_step_t<false, true>(ctx, diag, upd);
+        else launch_subst_step_t<false, false>(ctx, diag, upd);
+    }
 }
 
 inline size_t off(const DMat& a, int i, int j) { return ((size_t)j * a.ld() + i) * (a.cplx ? 2 : 1); }
@@ -811,17 +764,35 @@ void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
         // the reference's order (Lu.Solve, Lu.cs:336-351; BlockedLu.Solve,
         // BlockedLu.cs:105-118): the result matches the reference bit for bit.
         std::vector<LaswpDesc> swaps;
-        std::vector<SubstDesc> lower, upper;
+        constexpr int B = kSubstBlock;
+        int steps = 0;
         for (auto& it : items) {
             int n = it.lu->rows;
             if (n == 0 || it.nrhs == 0) continue;
             swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
-            lower.push_back(SubstDesc{it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs, 0});
-            upper.push_back(SubstDesc{it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs, 1});
+            steps = std::max(steps, (n + B - 1) / B);
         }
         launch_laswp(ctx, cplx, swaps);
-        launch_subst(ctx, cplx, lower);
-        launch_subst(ctx, cplx, upper);
+        // Lower: blocks from the top; upper: each item's blocks from its last.
+        for (int upper = 0; upper < 2; ++upper)
+            for (int s = 0; s < steps; ++s) {
+                std::vector<SubstDiagDesc> diag;
+                std::vector<SubstUpdateDesc> upd;
+                for (auto& it : items) {
+                    const int n = it.lu->rows;
+                    if (n == 0 || it.nrhs == 0) continue;
+                    const int blocks = (n + B - 1) / B;
+                    if (s >= blocks) continue;
+                    const int k0 = (upper ? blocks - 1 - s : s) * B, w = std::min(B, n - k0);
+                    const int ldf = it.lu->ld(), ldx = it.b->ld();
+                    diag.push_back(SubstDiagDesc{it.lu->p, ldf, it.b->p, ldx, it.nrhs, k0, w});
+                    const int r0 = upper ? 0 : k0 + w, r1 = upper ? k0 : n;
+                    if (r1 > r0)
+                        upd.push_back(SubstUpdateDesc{it.lu->p, ldf, it.b->p, ldx, it.nrhs, r0, r1, k0, k0 + w,
+                                                      (r1 - r0 + 63) / 64, 0});
+                }
+                launch_subst_step(ctx, cplx, upper != 0, diag, upd);
+            }
         return;
     }
     // The adjoint: blocked, 64-row diagonal blocks plus DMMA GEMM updates.
