@@ -304,6 +304,8 @@ def ours(args, world, rank, local, dist):
                          "timing": "CUDA events around every GEMM launch of one extra sweep run as a single group",
                          "gemm_launches_per_sweep": int(st["gemm_launches"]),
                          "gemm_tflop_per_sweep": st["gemm_flops"] / 1e12,
+                         "algorithmic_bytes_per_launch":
+                             st["gemm_bytes"] / st["gemm_launches"] if st["gemm_launches"] else None,
                          "gemm_aggregate_tflops_in_timed_steps":
                              st_step["gemm_flops"] / (ms * args.steps * 1e-3) / 1e12 if ms > 0 else None},
             "cpu_baseline": cpu,

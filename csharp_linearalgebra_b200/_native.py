@@ -44,7 +44,7 @@ class ExpmvInfo(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
-                ("gemm_flops", C.c_double), ("gemm_ms", C.c_double)]
+                ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double)]
 
 
 # name -> (restype, argtypes)

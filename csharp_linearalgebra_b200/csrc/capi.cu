@@ -383,23 +383,25 @@ void collect_stats(Context& ctx, tns_stats* out) {
     out->gemm_launches = ctx.gemm_launches;
     out->gemm_flops = ctx.gemm_flops;
     out->gemm_ms = ctx.gemm_ms_done;
+    out->gemm_bytes = ctx.gemm_bytes;
     for (auto& w : ctx.workers) {
         w->drain_events();
         out->kernel_launches += w->kernel_launches;
         out->gemm_launches += w->gemm_launches;
         out->gemm_flops += w->gemm_flops;
         out->gemm_ms += w->gemm_ms_done;
+        out->gemm_bytes += w->gemm_bytes;
     }
 }
 
 void reset_stats(Context& ctx) {
     ctx.drain_events();
     ctx.kernel_launches = ctx.gemm_launches = 0;
-    ctx.gemm_flops = ctx.gemm_ms_done = 0.0;
+    ctx.gemm_flops = ctx.gemm_ms_done = ctx.gemm_bytes = 0.0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
-        w->gemm_flops = w->gemm_ms_done = 0.0;
+        w->gemm_flops = w->gemm_ms_done = w->gemm_bytes = 0.0;
     }
 }
 

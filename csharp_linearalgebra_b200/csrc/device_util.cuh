@@ -86,6 +86,18 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst_smem, const void* src_gm
         : "memory");
 }
 
+// Per-warpgroup register reallocation (all four warps of the warpgroup execute
+// it). An increase waits until registers released by a decrease are free, so
+// callers must keep the warpgroups' totals within the launch's allocation.
+template <int N>
+__device__ __forceinline__ void reg_alloc() {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(N));
+}
+template <int N>
+__device__ __forceinline__ void reg_dealloc() {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(N));
+}
+
 // ---------------------------------------------------------------------------
 // FP64 tensor-core MMA (DMMA): D(16x8) += A(16x4) * B(4x8), fp64 throughout.
 // Fragments (g = lane/4, t = lane%4): a0=(g,t) a1=(g+8,t); b0=(t,g);

@@ -38,6 +38,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <string>
+#include <type_traits>
 #include <vector>
 
 namespace tns {
@@ -60,7 +62,15 @@ struct GemmCfg {
     static constexpr int B_STAGE = BN * LDB_S;
     static constexpr int STAGE_BYTES = (A_STAGE + B_STAGE) * ESZ;
     static constexpr int CONSUMERS = WARPS_M * WARPS_N;
-    static constexpr int THREADS = (CONSUMERS + 1) * 32;
+    // Eight math warps plus one producer warp would put three warps on one SM
+    // sub-partition and cap every thread at 168 registers. Instead the
+    // producer is a whole warpgroup (one warp feeds, three leave) that hands
+    // registers to the math warpgroups: launched at 168 per thread,
+    // 128 x 40 + 256 x 232 = 384 x 168, the launch's whole allocation.
+    static constexpr bool kSplitRegs = CONSUMERS == 8;
+    static constexpr int kLaunchRegs = 168, kProducerRegs = 40, kMathRegs = 232;
+    static_assert(!kSplitRegs || 128 * kProducerRegs + 256 * kMathRegs == 384 * kLaunchRegs, "register split");
+    static constexpr int THREADS = (CONSUMERS + (kSplitRegs ? 4 : 1)) * 32;
     static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
     static_assert((LDA_S * ESZ) % 16 == 0 && (LDB_S * ESZ) % 16 == 0, "smem columns must stay 16B aligned");
     static_assert(SMEM <= 227 * 1024, "shared memory budget");
@@ -116,6 +126,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
     auto stage_b = [&](int s) {
         return reinterpret_cast<E*>(smem + s * Cfg::STAGE_BYTES + Cfg::A_STAGE * Cfg::ESZ);
     };
+
+    if constexpr (Cfg::kSplitRegs) {
+        if (warp >= Cfg::CONSUMERS) {
+            reg_dealloc<Cfg::kProducerRegs>();
+            if (warp != Cfg::CONSUMERS) return;  // only the warpgroup's first warp feeds
+        } else {
+            reg_alloc<Cfg::kMathRegs>();
+        }
+    }
 
     if (warp == Cfg::CONSUMERS) {
         // ------------------------------ producer ------------------------------
@@ -208,33 +227,47 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
             if (!mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
             const E* As = stage_a(s) + wm * Cfg::WM + g;
             const E* Bs = stage_b(s) + (wn * Cfg::WN + g) * Cfg::LDB_S + t;
+            // One k-step of DMMAs; PASS selects the half of A (complex) the
+            // pass multiplies, so each pass loads only that half.
+            auto mma_step = [&](auto pass_tag) {
+                constexpr int PASS = decltype(pass_tag)::value;
+                const double* Ad = reinterpret_cast<const double*>(As);
 #pragma unroll
-            for (int ks = 0; ks < Cfg::BK; ks += 4) {
-                E fa0[Cfg::NF], fa1[Cfg::NF], fb[Cfg::MF];
+                for (int ks = 0; ks < Cfg::BK; ks += 4) {
+                    E fa0[Cfg::NF], fa1[Cfg::NF];
+                    double fb[Cfg::MF];
 #pragma unroll
-                for (int i = 0; i < Cfg::NF; ++i) {
-                    fa0[i] = Bs[(i * 16) * Cfg::LDB_S + ks];
-                    fa1[i] = Bs[(i * 16 + 8) * Cfg::LDB_S + ks];
-                }
-#pragma unroll
-                for (int j = 0; j < Cfg::MF; ++j) fb[j] = As[(ks + t) * Cfg::LDA_S + j * 8];
-#pragma unroll
-                for (int i = 0; i < Cfg::NF; ++i)
+                    for (int i = 0; i < Cfg::NF; ++i) {
+                        fa0[i] = Bs[(i * 16) * Cfg::LDB_S + ks];
+                        fa1[i] = Bs[(i * 16 + 8) * Cfg::LDB_S + ks];
+                    }
 #pragma unroll
                     for (int j = 0; j < Cfg::MF; ++j) {
-                        if constexpr (Cfg::kComplex) {
-                            // (A*B)^T = B^T A^T. Pass 0: Ar*Br -> acc0, Ar*Bi -> acc1.
-                            // Pass 1: Ai*Bi -> acc0, Ai*Br -> acc1.
-                            double a_part = pass == 0 ? fb[j].x : fb[j].y;
-                            dmma_16x8x4(acc0[i][j], pass == 0 ? fa0[i].x : fa0[i].y,
-                                        pass == 0 ? fa1[i].x : fa1[i].y, a_part);
-                            dmma_16x8x4(acc1[i][j], pass == 0 ? fa0[i].y : fa0[i].x,
-                                        pass == 0 ? fa1[i].y : fa1[i].x, a_part);
-                        } else {
-                            dmma_16x8x4(acc0[i][j], fa0[i], fa1[i], fb[j]);
-                        }
+                        const int e = (ks + t) * Cfg::LDA_S + j * 8;
+                        fb[j] = Cfg::kComplex ? Ad[2 * e + PASS] : Ad[e];
                     }
-            }
+#pragma unroll
+                    for (int i = 0; i < Cfg::NF; ++i)
+#pragma unroll
+                        for (int j = 0; j < Cfg::MF; ++j) {
+                            if constexpr (Cfg::kComplex) {
+                                // (A*B)^T = B^T A^T. Pass 0: Ar*Br -> acc0, Ar*Bi -> acc1.
+                                // Pass 1: Ai*Bi -> acc0, Ai*Br -> acc1.
+                                if constexpr (PASS == 0) {
+                                    dmma_16x8x4(acc0[i][j], fa0[i].x, fa1[i].x, fb[j]);
+                                    dmma_16x8x4(acc1[i][j], fa0[i].y, fa1[i].y, fb[j]);
+                                } else {
+                                    dmma_16x8x4(acc0[i][j], fa0[i].y, fa1[i].y, fb[j]);
+                                    dmma_16x8x4(acc1[i][j], fa0[i].x, fa1[i].x, fb[j]);
+                                }
+                            } else {
+                                dmma_16x8x4(acc0[i][j], fa0[i], fa1[i], fb[j]);
+                            }
+                        }
+                }
+            };
+            if (pass == 0) mma_step(std::integral_constant<int, 0>{});
+            else mma_step(std::integral_constant<int, 1>{});
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
 
@@ -342,12 +375,28 @@ using RealSmall = GemmCfg<false, 2, 1, 4>;  // 64 x 64 tiles, 2 math warps
 using CplxBig = GemmCfg<true, 4, 2, 3>;     // 128 x 64 tiles, 8 math warps
 using CplxSmall = GemmCfg<true, 2, 2, 4>;   // 64 x 64 tiles, 4 math warps
 
+// The math warpgroups' register increase can only be met when the kernel is
+// launched with exactly the allocation the split assumes; with any other
+// allocation they would wait forever, so such a build is refused.
+template <class Cfg>
+void check_register_split() {
+    if constexpr (Cfg::kSplitRegs) {
+        cudaFuncAttributes fa{};
+        TNS_CUDA(cudaFuncGetAttributes(&fa, gemm_dmma_kernel<Cfg>));
+        if (fa.numRegs != Cfg::kLaunchRegs)
+            fail(TNS_E_DEVICE, "GEMM kernel built with " + std::to_string(fa.numRegs) +
+                                   " registers per thread; its register split needs " +
+                                   std::to_string(Cfg::kLaunchRegs));
+    }
+}
+
 template <class Cfg>
 void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     static std::atomic<bool> configured[64];
     int dev = ctx.device;
     if (!configured[dev].load(std::memory_order_acquire)) {
         TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+        check_register_split<Cfg>();
         configured[dev].store(true, std::memory_order_release);
     }
     int total = 0;
@@ -381,7 +430,12 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
     ctx.gemm_launches++;
-    for (auto& p : probs) ctx.gemm_flops += (Cfg::kComplex ? 8.0 : 2.0) * (double)(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
+    for (auto& p : probs) {
+        ctx.gemm_flops += (Cfg::kComplex ? 8.0 : 2.0) * (double)(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
+        const bool reads_c = p.beta_re != 0.0 || p.beta_im != 0.0;
+        ctx.gemm_bytes += (Cfg::kComplex ? 16.0 : 8.0) *
+                          ((double)p.M * p.K + (double)p.K * p.N + (double)p.M * p.N * (reads_c ? 2.0 : 1.0));
+    }
     if (ctx.timing) {
         TNS_CUDA(cudaEventRecord(e1, ctx.stream));
         ctx.gemm_events.emplace_back(e0, e1);
@@ -449,6 +503,7 @@ namespace {
 template <class Cfg>
 void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p) {
     TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+    check_register_split<Cfg>();
     p.tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM;
     p.tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
     p.tile_begin = 0;

@@ -85,6 +85,7 @@ struct Context {
     bool timing = false;
     long long gemm_launches = 0;
     double gemm_flops = 0.0;  // algorithmic: 2mnk real, 8mnk complex (4M), true sizes
+    double gemm_bytes = 0.0;  // least traffic: A, B read, C written (and read if beta != 0)
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_events;
     std::vector<cudaEvent_t> event_pool;
     double gemm_ms_done = 0.0;  // elapsed time of events already drained

@@ -220,12 +220,16 @@ int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const double* al
  * (src/Tensile.Kernels/Lu.cs:92-164, src/Tensile/MatrixExponential.cs:575-582).
  * gemm_ms is the summed CUDA-event duration of the GEMM kernel launches made
  * while timing was enabled; gemm_flops counts 2mnk (real) or 8mnk (complex 4M)
- * at the products' true sizes. */
+ * at the products' true sizes; gemm_bytes is the least memory traffic of
+ * those launches (A and B read once, C written once and read once when beta
+ * is non-zero) at the launched sizes (m, n rounded up to even, k to a multiple
+ * of 16). */
 typedef struct {
     long long kernel_launches; /* every kernel this context launched */
     long long gemm_launches;
     double gemm_flops;
     double gemm_ms;
+    double gemm_bytes;
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
