@@ -67,8 +67,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
             sys.stderr.write(f"--- {src}\n{text}\n")
         raise RuntimeError("nvcc failed for " + ", ".join(s for s, _ in failed))
     if _stale(LIB, objs):
-        cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
-               "-lcuda"]
+        cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -86,6 +86,24 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst_smem, const void* src_gm
         : "memory");
 }
 
+// One tiled TMA load of a 2-D box (coordinates innermost first, in elements)
+// into shared memory, completing on `bar` with the box's byte count. No
+// multicast. The innermost coordinate times the element size must be a
+// multiple of 16 bytes; the destination is 128-byte aligned.
+__device__ __forceinline__ void tma_load_2d(void* dst_smem, const void* tmap, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_addr(dst_smem)),
+        "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Orders the host's (generic proxy) writes of a tensor map in global memory
+// before this thread's TMA reads of it (the tensor-map proxy).
+__device__ __forceinline__ void tensormap_acquire(const void* tmap) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+}
+
 // Per-warpgroup register reallocation (all four warps of the warpgroup execute
 // it). An increase waits until registers released by a decrease are free, so
 // callers must keep the warpgroups' totals within the launch's allocation.

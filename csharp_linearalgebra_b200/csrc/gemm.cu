@@ -16,11 +16,14 @@
 //    Q += Ai*Br, then P + iQ is combined into C with the reference's alpha and
 //    beta special cases (ComplexKernels.Combine). Both passes stream the same
 //    interleaved tiles; no split copies of A or B are made.
-//  - Operand tiles are staged in shared memory by the TMA engine's bulk copies
-//    (cp.async.bulk, one per tile column) completing on mbarriers; a producer
-//    warp runs STAGES tiles ahead of the math warps. Smem columns are padded so
-//    the DMMA fragment loads are bank-conflict free (real: A stride = 4 mod 16
-//    doubles, B stride 20; complex: A stride = 2 mod 8 complex, B stride 20).
+//  - Operand tiles are staged in shared memory by tiled TMA loads
+//    (cp.async.bulk.tensor.2d; one box of B and one or two of A per k-step)
+//    completing on mbarriers; a producer warp runs STAGES k-steps ahead of the
+//    math warps. Each box is loaded wider than its tile so that its columns
+//    land padded and the DMMA fragment loads are bank-conflict free (real: A
+//    stride = 4 mod 16 doubles, B stride 20; complex: A stride = 2 mod 8
+//    complex, B stride 20). The extra rows are real data or the TMA unit's
+//    zero fill beyond the operand, and are never multiplied.
 //  - The MMA computes C^T = B^T A^T, so a thread's accumulator pair covers two
 //    consecutive rows of column-major C and the epilogue moves 16-byte pairs.
 //  - Persistent CTAs walk a list of problems (grouped GEMM): the same kernel
@@ -35,6 +38,9 @@
 
 #include "device_util.cuh"
 #include "tns_internal.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -56,10 +62,17 @@ struct GemmCfg {
     static constexpr int BN = WARPS_N * WN;
     static constexpr int BK = 16;
     static constexpr int STAGES = STAGES_;
-    static constexpr int LDA_S = BM + (CPLX ? 2 : 4);  // smem A column stride, elements
-    static constexpr int LDB_S = BK + 4;               // smem B column stride, elements
-    static constexpr int A_STAGE = BK * LDA_S;         // elements
+    // A stage holds A_BOXES TMA boxes of A_BOX_ROWS rows (complex boxes stop
+    // at 64 rows: a box row may hold at most 256 doubles). Each box is loaded
+    // wider than its rows, so its columns land padded in shared memory.
+    static constexpr int A_BOX_ROWS = CPLX ? 64 : BM;
+    static constexpr int A_BOXES = BM / A_BOX_ROWS;
+    static constexpr int LDA_S = A_BOX_ROWS + (CPLX ? 2 : 4);  // smem A column stride, elements
+    static constexpr int LDB_S = BK + 4;                       // smem B column stride, elements
+    static constexpr int A_BOX = BK * LDA_S;                   // elements
+    static constexpr int A_STAGE = A_BOXES * A_BOX;
     static constexpr int B_STAGE = BN * LDB_S;
+    static constexpr int DPE = CPLX ? 2 : 1;  // doubles per element (TMA maps count doubles)
     static constexpr int STAGE_BYTES = (A_STAGE + B_STAGE) * ESZ;
     static constexpr int CONSUMERS = WARPS_M * WARPS_N;
     // Eight math warps plus one producer warp would put three warps on one SM
@@ -73,6 +86,9 @@ struct GemmCfg {
     static constexpr int THREADS = (CONSUMERS + (kSplitRegs ? 4 : 1)) * 32;
     static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
     static_assert((LDA_S * ESZ) % 16 == 0 && (LDB_S * ESZ) % 16 == 0, "smem columns must stay 16B aligned");
+    static_assert((A_BOX * ESZ) % 128 == 0 && (B_STAGE * ESZ) % 128 == 0, "TMA boxes land 128B aligned");
+    static_assert(LDA_S * DPE <= 256 && LDB_S * DPE <= 256 && BN <= 256, "TMA box extents");
+    static_assert(WM <= A_BOX_ROWS && A_BOX_ROWS % WM == 0, "a warp's rows stay inside one A box");
     static_assert(SMEM <= 227 * 1024, "shared memory budget");
 };
 
@@ -86,11 +102,20 @@ __device__ __forceinline__ int find_problem(const GemmProblem* probs, int nprob,
     return lo;
 }
 
-// Problems of one launch: up to four travel in the parameter block, a longer
-// list lives in device memory.
+// The TMA descriptors of one problem's operands, viewed as 2-D arrays of
+// doubles (complex: two doubles per element): A is (DPE*M) x K, B is
+// (DPE*K) x N, column-major with the problem's leading dimensions.
+struct GemmMaps {
+    CUtensorMap a, b;
+};
+
+// Problems of one launch: up to four travel in the parameter block with their
+// descriptors, a longer list (and its descriptors) lives in device memory.
 struct GemmLaunch {
     GemmProblem inl[4];
+    GemmMaps inl_maps[4];
     const GemmProblem* list;
+    const GemmMaps* maps_list;
     int nprob;
     int total_tiles;
     int* err;
@@ -138,18 +163,24 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
 
     if (warp == Cfg::CONSUMERS) {
         // ------------------------------ producer ------------------------------
+        // One lane issues each stage as A_BOXES + 1 tiled TMA loads. Boxes
+        // reaching past the operand's extent are zero-filled by the TMA unit,
+        // so every stage carries exactly STAGE_BYTES.
+        const GemmMaps* maps = L.maps_list ? L.maps_list : L.inl_maps;
         uint32_t it = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-            const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
+            const int pi = find_problem(probs, nprob, tile);
+            const GemmProblem& P = probs[pi];
+            const CUtensorMap* ma = &maps[pi].a;
+            const CUtensorMap* mb = &maps[pi].b;
+            if (L.maps_list && lane == 0) {
+                tensormap_acquire(ma);
+                tensormap_acquire(mb);
+            }
             int local = tile - P.tile_begin;
             int m0 = (local % P.tiles_m) * Cfg::BM;
             int n0 = (local / P.tiles_m) * Cfg::BN;
-            int rows = min(Cfg::BM, P.M - m0);
-            int cols = min(Cfg::BN, P.N - n0);
-            uint32_t bytes = (uint32_t)(Cfg::BK * rows + cols * Cfg::BK) * Cfg::ESZ;
-            const E* A = reinterpret_cast<const E*>(P.A);
-            const E* B = reinterpret_cast<const E*>(P.B);
             const int nk = P.K / Cfg::BK;
             for (int q = 0; q < nk * PASSES; ++q, ++it) {
                 const int k0 = (q % nk) * Cfg::BK;
@@ -159,20 +190,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
                     ok = false;
                     break;
                 }
-                if (lane == 0) mbar_arrive_expect_tx(&full[s], bytes);
-                __syncwarp();
-                E* As = stage_a(s);
-                E* Bs = stage_b(s);
-                for (int c = lane; c < Cfg::BK + cols; c += 32) {
-                    if (c < Cfg::BK) {
-                        bulk_copy_g2s(As + c * Cfg::LDA_S, A + (size_t)(k0 + c) * P.lda + m0,
-                                      (uint32_t)rows * Cfg::ESZ, &full[s]);
-                    } else {
-                        int nn = c - Cfg::BK;
-                        bulk_copy_g2s(Bs + nn * Cfg::LDB_S, B + (size_t)(n0 + nn) * P.ldb + k0,
-                                      (uint32_t)Cfg::BK * Cfg::ESZ, &full[s]);
-                    }
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&full[s], (uint32_t)Cfg::STAGE_BYTES);
+                    E* As = stage_a(s);
+#pragma unroll
+                    for (int h = 0; h < Cfg::A_BOXES; ++h)
+                        tma_load_2d(As + h * Cfg::A_BOX, ma, Cfg::DPE * (m0 + h * Cfg::A_BOX_ROWS), k0, &full[s]);
+                    tma_load_2d(stage_b(s), mb, Cfg::DPE * k0, n0, &full[s]);
                 }
+                __syncwarp();
             }
         }
         // Drain: do not leave while copies into this CTA's shared memory are in
@@ -225,7 +251,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
             const int kt = q % nk;
             int s = it % Cfg::STAGES;
             if (!mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
-            const E* As = stage_a(s) + wm * Cfg::WM + g;
+            const E* As = stage_a(s) + (wm * Cfg::WM / Cfg::A_BOX_ROWS) * Cfg::A_BOX +
+                          (wm * Cfg::WM) % Cfg::A_BOX_ROWS + g;
             const E* Bs = stage_b(s) + (wn * Cfg::WN + g) * Cfg::LDB_S + t;
             // One k-step of DMMAs; PASS selects the half of A (complex) the
             // pass multiplies, so each pass loads only that half.
@@ -390,6 +417,42 @@ void check_register_split() {
     }
 }
 
+// A 2-D double-precision TMA descriptor: `rows` x `cols` doubles, column
+// stride `ld_bytes`, boxes of box_rows x box_cols, zero fill outside.
+void encode_map(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols, uint64_t ld_bytes,
+                uint32_t box_rows, uint32_t box_cols) {
+    cuuint64_t dims[2] = {rows, cols};
+    cuuint64_t strides[1] = {ld_bytes};
+    cuuint32_t box[2] = {box_rows, box_cols};
+    cuuint32_t elem[2] = {1, 1};
+    // The driver's encoder, looked up through the runtime so that the library
+    // loads (and its host-only entry points work) where no driver is present.
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) fail(TNS_E_DEVICE, "the CUDA driver does not provide cuTensorMapEncodeTiled");
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dims, strides, box, elem,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(TNS_E_DEVICE, "TMA descriptor encoding failed (CUresult " + std::to_string((int)r) + ")");
+}
+
+// Descriptors of one problem's operands for configuration Cfg.
+template <class Cfg>
+GemmMaps encode_maps(const GemmProblem& p) {
+    GemmMaps m;
+    encode_map(&m.a, p.A, (uint64_t)Cfg::DPE * p.M, (uint64_t)p.K, (uint64_t)p.lda * Cfg::ESZ,
+               Cfg::DPE * Cfg::LDA_S, Cfg::BK);
+    encode_map(&m.b, p.B, (uint64_t)Cfg::DPE * p.K, (uint64_t)p.N, (uint64_t)p.ldb * Cfg::ESZ,
+               Cfg::DPE * Cfg::LDB_S, Cfg::BN);
+    return m;
+}
+
 template <class Cfg>
 void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     static std::atomic<bool> configured[64];
@@ -412,10 +475,17 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     L.total_tiles = total;
     L.err = ctx.d_err;
     if (probs.size() <= 4) {
-        for (size_t i = 0; i < probs.size(); ++i) L.inl[i] = probs[i];
+        for (size_t i = 0; i < probs.size(); ++i) {
+            L.inl[i] = probs[i];
+            L.inl_maps[i] = encode_maps<Cfg>(probs[i]);
+        }
         L.list = nullptr;
+        L.maps_list = nullptr;
     } else {
+        std::vector<GemmMaps> maps(probs.size());
+        for (size_t i = 0; i < probs.size(); ++i) maps[i] = encode_maps<Cfg>(probs[i]);
         L.list = static_cast<const GemmProblem*>(ctx.upload(probs.data(), sizeof(GemmProblem) * probs.size()));
+        L.maps_list = static_cast<const GemmMaps*>(ctx.upload(maps.data(), sizeof(GemmMaps) * maps.size()));
     }
     int ctas_per_sm = 1;
     TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
@@ -511,7 +581,9 @@ void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p
     if (total == 0) return;
     GemmLaunch L{};
     L.inl[0] = p;
+    L.inl_maps[0] = encode_maps<Cfg>(p);
     L.list = nullptr;
+    L.maps_list = nullptr;
     L.nprob = 1;
     L.total_tiles = total;
     L.err = d_err;
