@@ -28,6 +28,7 @@ Context::Context(int dev) : device(dev) {
     TNS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     TNS_CUDA(cudaMalloc(&d_err, sizeof(int)));
     TNS_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    TNS_CUDA(cudaMalloc(&d_tiles, sizeof(unsigned long long)));
     // Keep freed blocks in the stream-ordered pool instead of handing them back
     // to the driver at every synchronisation: the algorithms allocate and free
     // work matrices between host-side decisions.
@@ -73,6 +74,7 @@ Context::~Context() {
     if (h_ring) cudaFreeHost(h_ring);
     if (d_ring) cudaFree(d_ring);
     if (d_err) cudaFree(d_err);
+    if (d_tiles) cudaFree(d_tiles);
     if (stream) cudaStreamDestroy(stream);
 }
 

@@ -84,7 +84,8 @@ struct GemmCfg {
     static constexpr int kLaunchRegs = 168, kProducerRegs = 40, kMathRegs = 232;
     static_assert(!kSplitRegs || 128 * kProducerRegs + 256 * kMathRegs == 384 * kLaunchRegs, "register split");
     static constexpr int THREADS = (CONSUMERS + (kSplitRegs ? 4 : 1)) * 32;
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 128;
+    // stages, full and empty barriers, the tile announced with each stage, alignment slack
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + STAGES * 4 + 128;
     static_assert((LDA_S * ESZ) % 16 == 0 && (LDB_S * ESZ) % 16 == 0, "smem columns must stay 16B aligned");
     static_assert((A_BOX * ESZ) % 128 == 0 && (B_STAGE * ESZ) % 128 == 0, "TMA boxes land 128B aligned");
     static_assert(LDA_S * DPE <= 256 && LDB_S * DPE <= 256 && BN <= 256, "TMA box extents");
@@ -116,6 +117,7 @@ struct GemmLaunch {
     GemmMaps inl_maps[4];
     const GemmProblem* list;
     const GemmMaps* maps_list;
+    unsigned long long* tiles;  // zeroed tile counter (dynamic order), or null (static round robin)
     int nprob;
     int total_tiles;
     int* err;
@@ -134,6 +136,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
     uint64_t* empty = full + Cfg::STAGES;
+    // The producer writes the tile a stage starts (or -1: no more tiles)
+    // before the stage's arrival, which releases it to the math warps.
+    int* tile_slot = reinterpret_cast<int*>(empty + Cfg::STAGES);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -169,7 +174,36 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
         const GemmMaps* maps = L.maps_list ? L.maps_list : L.inl_maps;
         uint32_t it = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+        // Tiles in the order of the launch's list: taken from the shared
+        // counter as the CTA frees up (the host lists the heaviest problems
+        // first), or round robin without one.
+        long long taken = 0;
+        auto next_tile = [&]() -> int {
+            int t = -1;
+            if (lane == 0) {
+                const unsigned long long v = L.tiles ? atomicAdd(L.tiles, 1ull)
+                                                     : (unsigned long long)blockIdx.x + taken * gridDim.x;
+                t = v < (unsigned long long)total_tiles ? (int)v : -1;
+            }
+            ++taken;
+            return __shfl_sync(0xffffffffu, t, 0);
+        };
+        while (ok) {
+            const int tile = next_tile();
+            if (tile < 0) {
+                // End marker: a stage without copies announcing no tile.
+                const int s = it % Cfg::STAGES;
+                if (!mbar_wait_bounded(&empty[s], ((it / Cfg::STAGES) & 1) ^ 1, err, kDevTimeoutEmpty)) {
+                    ok = false;
+                    break;
+                }
+                if (lane == 0) {
+                    tile_slot[s] = -1;
+                    mbar_arrive(&full[s]);
+                }
+                __syncwarp();
+                break;
+            }
             const int pi = find_problem(probs, nprob, tile);
             const GemmProblem& P = probs[pi];
             const CUtensorMap* ma = &maps[pi].a;
@@ -191,6 +225,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
                     break;
                 }
                 if (lane == 0) {
+                    if (q == 0) tile_slot[s] = tile;
                     mbar_arrive_expect_tx(&full[s], (uint32_t)Cfg::STAGE_BYTES);
                     E* As = stage_a(s);
 #pragma unroll
@@ -221,7 +256,11 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
     const int t = lane & 3;
     uint32_t it = 0;
 
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    for (;;) {
+        // The first stage of each tile announces it (or the end).
+        if (!mbar_wait_bounded(&full[it % Cfg::STAGES], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
+        const int tile = tile_slot[it % Cfg::STAGES];
+        if (tile < 0) break;
         const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
         int local = tile - P.tile_begin;
         const int m0 = (local % P.tiles_m) * Cfg::BM;
@@ -250,7 +289,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
             const int pass = q / nk;
             const int kt = q % nk;
             int s = it % Cfg::STAGES;
-            if (!mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
+            if (q > 0 && !mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
             const E* As = stage_a(s) + (wm * Cfg::WM / Cfg::A_BOX_ROWS) * Cfg::A_BOX +
                           (wm * Cfg::WM) % Cfg::A_BOX_ROWS + g;
             const E* Bs = stage_b(s) + (wn * Cfg::WN + g) * Cfg::LDB_S + t;
@@ -474,6 +513,8 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
     L.nprob = (int)probs.size();
     L.total_tiles = total;
     L.err = ctx.d_err;
+    L.tiles = ctx.d_tiles;
+    TNS_CUDA(cudaMemsetAsync(ctx.d_tiles, 0, sizeof(unsigned long long), ctx.stream));
     if (probs.size() <= 4) {
         for (size_t i = 0; i < probs.size(); ++i) {
             L.inl[i] = probs[i];
@@ -548,6 +589,9 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
         work.push_back(p);
     }
     if (work.empty()) return;
+    // Heaviest tiles (deepest K) first: CTAs take tiles in list order as they
+    // free up, so the launch ends on light tiles.
+    std::stable_sort(work.begin(), work.end(), [](const GemmProblem& x, const GemmProblem& y) { return x.K > y.K; });
     // Big tiles only when they fill the machine.
     if (cplx) {
         long long tiles = 0;
@@ -587,6 +631,7 @@ void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p
     L.nprob = 1;
     L.total_tiles = total;
     L.err = d_err;
+    L.tiles = nullptr;  // no counter without a context: static round robin
     int ctas_per_sm = 1;
     TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
     int grid = std::min(total, std::max(1, ctas_per_sm) * num_sms);

@@ -69,6 +69,7 @@ struct Context {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     int* d_err = nullptr;           // device-side error flag (bounded waits)
+    unsigned long long* d_tiles = nullptr;  // grouped GEMM's tile counter, zeroed before each launch
     long long max_elements = 2147483591LL;
     std::string last_error;
     long long kernel_launches = 0;  // kernels launched through this context
