@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "batched complex expm/s: split-prec vs plain FP64 GPU at ≤1e-12 rel err; vs CPU"
+# DRAM bytes of the GEMM launches per algorithmic byte, from one ncu capture of every GEMM launch of
+# the 16-matrix sweep (profiles/gemm_dmma_complex_sweep16.md): 109.1 MB measured / 153.4 MB.
+GEMM_TRAFFIC_RATIO = 109.1 / 153.35
 WORKLOAD = ("frequency sweep of 256 complex128 matrices A_k = -(G + i w_k C), n_k ~ U{64..1024}, "
             "G ~ N(0,1)/sqrt(n), C = Q^T D Q (D log-uniform [1e-3,1]), w_k log-spaced 1e2..1e6; Expm of each")
 
@@ -300,7 +303,12 @@ def ours(args, world, rank, local, dist):
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if (achieved and peak) else None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (MEASURED_PEAKS.json has no FP64 figure)",
-                         "traffic": None,
+                         "traffic": (GEMM_TRAFFIC_RATIO * st["gemm_bytes"] / st["gemm_launches"])
+                                    if st["gemm_launches"] else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every GEMM launch of "
+                                           "the 16-matrix sweep = 0.711 x its algorithmic bytes "
+                                           "(profiles/gemm_dmma_complex_sweep16.md), scaled to this sweep's "
+                                           "algorithmic bytes per launch",
                          "timing": "CUDA events around every GEMM launch of one extra sweep run as a single group",
                          "gemm_launches_per_sweep": int(st["gemm_launches"]),
                          "gemm_tflop_per_sweep": st["gemm_flops"] / 1e12,

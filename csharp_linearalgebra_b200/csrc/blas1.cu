@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 namespace tns {
@@ -181,7 +182,21 @@ __global__ void abs_power_step_kernel(const __grid_constant__ Batch<ChainDesc> b
     double* out = parity ? d.row : d.next;
     const double* col = d.mags + (size_t)j * d.ld;
     double sum = 0.0;
-    for (int i = 0; i < d.n; ++i) sum = add_rn(sum, mul_rn(row[i], col[i]));
+    // The sum stays sequential in i; the column is loaded 16 entries ahead
+    // (16-byte loads: ld and the block starts are even).
+    constexpr int U = 16;
+    int i0 = 0;
+    for (; i0 + U <= d.n; i0 += U) {
+        double2 cv[U / 2];
+#pragma unroll
+        for (int u = 0; u < U / 2; ++u) cv[u] = reinterpret_cast<const double2*>(col + i0)[u];
+#pragma unroll
+        for (int u = 0; u < U / 2; ++u) {
+            sum = add_rn(sum, mul_rn(row[i0 + 2 * u], cv[u].x));
+            sum = add_rn(sum, mul_rn(row[i0 + 2 * u + 1], cv[u].y));
+        }
+    }
+    for (int i = i0; i < d.n; ++i) sum = add_rn(sum, mul_rn(row[i], col[i]));
     out[j] = sum;
 }
 
@@ -219,29 +234,41 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant_
         }
         __syncthreads();
         if (!row_ok) continue;
-        for (int jj = 0; jj < len; ++jj) {
-            const size_t idx = (size_t)(j0 + jj) * d.ld + i;
-            if (!CPLX) {
-                const double aij = d.a[idx];
+        // The sums stay sequential in j; the loads of A run U columns ahead
+        // of them, so each thread keeps U loads in flight.
+        constexpr int U = 16;
+        using AE = typename std::conditional<CPLX, double2, double>::type;
+        const AE* arow = reinterpret_cast<const AE*>(d.a) + (size_t)j0 * d.ld + i;
+        for (int jb = 0; jb < len; jb += U) {
+            AE av[U];
 #pragma unroll
-                for (int c = 0; c < TMAX; ++c) {
-                    if (c < t) {
-                        double s = sx[c * CH + jj];
-                        double term = s != 0.0 ? mul_rn(s, aij) : 0.0;
-                        acc[c][0] = add_rn(acc[c][0], term);
+            for (int u = 0; u < U; ++u)
+                if (jb + u < len) av[u] = arow[(size_t)(jb + u) * d.ld];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (jb + u >= len) break;
+                const int jj = jb + u;
+                if constexpr (!CPLX) {
+#pragma unroll
+                    for (int c = 0; c < TMAX; ++c) {
+                        if (c < t) {
+                            double s = sx[c * CH + jj];
+                            double term = s != 0.0 ? mul_rn(s, av[u]) : 0.0;
+                            acc[c][0] = add_rn(acc[c][0], term);
+                        }
                     }
-                }
-            } else {
-                const double2 aij = reinterpret_cast<const double2*>(d.a)[idx];
+                } else {
+                    const double2 aij = av[u];
 #pragma unroll
-                for (int c = 0; c < TMAX; ++c) {
-                    if (c < t) {
-                        double sr = sx[(c * CH + jj) * 2], si = sx[(c * CH + jj) * 2 + 1];
-                        bool nr = sr != 0.0, ni = si != 0.0;
-                        acc[c][0] = add_rn(acc[c][0], nr ? mul_rn(sr, aij.x) : 0.0);  // pr
-                        acc[c][2] = add_rn(acc[c][2], nr ? mul_rn(sr, aij.y) : 0.0);  // qr
-                        acc[c][1] = add_rn(acc[c][1], ni ? mul_rn(si, aij.x) : 0.0);  // pi
-                        acc[c][3] = add_rn(acc[c][3], ni ? mul_rn(si, aij.y) : 0.0);  // qi
+                    for (int c = 0; c < TMAX; ++c) {
+                        if (c < t) {
+                            double sr = sx[(c * CH + jj) * 2], si = sx[(c * CH + jj) * 2 + 1];
+                            bool nr = sr != 0.0, ni = si != 0.0;
+                            acc[c][0] = add_rn(acc[c][0], nr ? mul_rn(sr, aij.x) : 0.0);  // pr
+                            acc[c][2] = add_rn(acc[c][2], nr ? mul_rn(sr, aij.y) : 0.0);  // qr
+                            acc[c][1] = add_rn(acc[c][1], ni ? mul_rn(si, aij.x) : 0.0);  // pi
+                            acc[c][3] = add_rn(acc[c][3], ni ? mul_rn(si, aij.y) : 0.0);  // qi
+                        }
                     }
                 }
             }
