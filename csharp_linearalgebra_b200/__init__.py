@@ -222,6 +222,28 @@ class Workspace:
                        _p(c), _ld(c))
         return c
 
+    def multiply_split(self, a, b, slices: int = 8):
+        """A*B in the split-precision form (8-bit slices on the tensor cores,
+        FP64 recombination); within about K * 2^(-7 slices) of the row and
+        column scales of the FP64 product. Returns a new matrix."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+        a, b = _fortran(a, cplx), _fortran(b, cplx)
+        if a.ndim != 2 or b.ndim != 2:
+            raise ValueError("operands must be matrices")
+        m, k = a.shape
+        k2, n = b.shape
+        if k != k2:
+            raise ValueError(f"Inner dimensions disagree: A is {m}x{k}, B is {k2}x{n}.")
+        c = np.zeros((m, n), dtype=a.dtype, order="F")
+        name = "tns_zgemm_split" if cplx else "tns_dgemm_split"
+        self._call(name, m, n, k, _p(a), _ld(a), _p(b), _ld(b), _p(c), _ld(c), int(slices))
+        return c
+
+    def set_split_slices(self, slices: int):
+        """0: Expm entirely in plain FP64 (the reference's rounding); 4..8: its
+        Pade-evaluation and squaring products in the split-precision form."""
+        self._call("tns_set_split_slices", int(slices))
+
     # -- norms --------------------------------------------------------------
     def _norm(self, a, kind: bytes) -> float:
         cplx = np.iscomplexobj(a)

@@ -44,7 +44,9 @@ class ExpmvInfo(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
-                ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double)]
+                ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double),
+                ("split_launches", C.c_longlong), ("split_flops", C.c_double), ("split_int8_ops", C.c_double),
+                ("split_ms", C.c_double)]
 
 
 # name -> (restype, argtypes)
@@ -58,6 +60,9 @@ SIGNATURES = {
     "tns_dgemm_device": (_I, [_P, _I, _I, _I, _D, _P, _I, _P, _I, _D, _P, _I]),
     "tns_zgemm": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
     "tns_zgemm_device": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
+    "tns_dgemm_split": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
+    "tns_zgemm_split": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
+    "tns_set_split_slices": (_I, [_P, _I]),
     "tns_dnorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
     "tns_znorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
     "tns_dgetrf": (_I, [_P, _I, _I, _P, _I, _I, _P, C.POINTER(LuInfo)]),

@@ -109,6 +109,24 @@ int gemm_entry(tns_context* c, bool cplx, bool dev, int m, int n, int k, const d
     });
 }
 
+int gemm_split_entry(tns_context* c, bool cplx, int m, int n, int k, const double* a, int lda, const double* b,
+                     int ldb, double* cm, int ldc, int slices) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, m, k, lda, "A");
+        check_operand(b, k, n, ldb, "B");
+        check_operand(cm, m, n, ldc, "C");
+        require(slices >= 4 && slices <= 8, TNS_E_ARGUMENT, "split-precision products take 4 to 8 slices");
+        if (m == 0 || n == 0) return;
+        DMat A = upload(ctx, a, m, k, lda, cplx, false, "the A operand");
+        DMat B = upload(ctx, b, k, n, ldb, cplx, false, "the B operand");
+        DMat C(ctx, m, n, cplx, "the C operand");
+        std::vector<tns::SplitProduct> v{tns::SplitProduct{&A, &B, &C, 0.0}};
+        tns::gemm_split_batch(ctx, v, slices);
+        tns::copy_out(ctx, C, cm, ldc, false);
+        ctx.sync();
+    });
+}
+
 int norm_entry(tns_context* c, bool cplx, char kind, int m, int n, const double* a, int lda, double* out) {
     return guarded(c, [&](Context& ctx) {
         check_operand(a, m, n, lda, "A");
@@ -340,6 +358,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             Context& wc = *ctx.workers[w];
             wc.max_elements = ctx.max_elements;
             wc.timing = ctx.timing;
+            wc.split_slices = ctx.split_slices;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
                 run_group(wc, groups[w]);
@@ -384,6 +403,10 @@ void collect_stats(Context& ctx, tns_stats* out) {
     out->gemm_flops = ctx.gemm_flops;
     out->gemm_ms = ctx.gemm_ms_done;
     out->gemm_bytes = ctx.gemm_bytes;
+    out->split_launches = ctx.split_launches;
+    out->split_flops = ctx.split_flops;
+    out->split_int8_ops = ctx.split_int8_ops;
+    out->split_ms = ctx.split_ms_done;
     for (auto& w : ctx.workers) {
         w->drain_events();
         out->kernel_launches += w->kernel_launches;
@@ -391,6 +414,10 @@ void collect_stats(Context& ctx, tns_stats* out) {
         out->gemm_flops += w->gemm_flops;
         out->gemm_ms += w->gemm_ms_done;
         out->gemm_bytes += w->gemm_bytes;
+        out->split_launches += w->split_launches;
+        out->split_flops += w->split_flops;
+        out->split_int8_ops += w->split_int8_ops;
+        out->split_ms += w->split_ms_done;
     }
 }
 
@@ -398,10 +425,14 @@ void reset_stats(Context& ctx) {
     ctx.drain_events();
     ctx.kernel_launches = ctx.gemm_launches = 0;
     ctx.gemm_flops = ctx.gemm_ms_done = ctx.gemm_bytes = 0.0;
+    ctx.split_launches = 0;
+    ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = 0.0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
         w->gemm_flops = w->gemm_ms_done = w->gemm_bytes = 0.0;
+        w->split_launches = 0;
+        w->split_flops = w->split_int8_ops = w->split_ms_done = 0.0;
     }
 }
 
@@ -466,6 +497,23 @@ int tns_zgemm(tns_context* c, int m, int n, int k, const double* alpha, const do
 int tns_zgemm_device(tns_context* c, int m, int n, int k, const double* alpha, const double* a, int lda,
                      const double* b, int ldb, const double* beta, double* cm, int ldc) {
     return gemm_entry(c, true, true, m, n, k, alpha, a, lda, b, ldb, beta, cm, ldc);
+}
+
+int tns_dgemm_split(tns_context* c, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                    double* cm, int ldc, int slices) {
+    return gemm_split_entry(c, false, m, n, k, a, lda, b, ldb, cm, ldc, slices);
+}
+int tns_zgemm_split(tns_context* c, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                    double* cm, int ldc, int slices) {
+    return gemm_split_entry(c, true, m, n, k, a, lda, b, ldb, cm, ldc, slices);
+}
+int tns_set_split_slices(tns_context* c, int slices) {
+    return guarded(c, [&](Context& ctx) {
+        require(slices == 0 || (slices >= 4 && slices <= 8), TNS_E_ARGUMENT,
+                "split slices must be 0 (plain FP64) or 4 to 8");
+        ctx.split_slices = slices;
+        for (auto& w : ctx.workers) w->split_slices = slices;
+    });
 }
 
 int tns_dnorm(tns_context* c, char kind, int m, int n, const double* a, int lda, double* out) {

@@ -50,16 +50,20 @@ cudaEvent_t Context::take_event() {
 }
 
 void Context::drain_events() {
-    if (gemm_events.empty()) return;
+    if (gemm_events.empty() && split_events.empty()) return;
     TNS_CUDA(cudaStreamSynchronize(stream));
-    for (auto& pr : gemm_events) {
-        float ms = 0.f;
-        TNS_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
-        gemm_ms_done += ms;
-        event_pool.push_back(pr.first);
-        event_pool.push_back(pr.second);
-    }
-    gemm_events.clear();
+    auto drain = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& evs, double& total) {
+        for (auto& pr : evs) {
+            float ms = 0.f;
+            TNS_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            total += ms;
+            event_pool.push_back(pr.first);
+            event_pool.push_back(pr.second);
+        }
+        evs.clear();
+    };
+    drain(gemm_events, gemm_ms_done);
+    drain(split_events, split_ms_done);
 }
 
 Context::~Context() {

@@ -90,8 +90,14 @@ struct Context {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_events;
     std::vector<cudaEvent_t> event_pool;
     double gemm_ms_done = 0.0;  // elapsed time of events already drained
+    // The split-precision product's launches (counted and timed apart from the
+    // FP64 GEMM's): FP64-equivalent algorithmic flops and 8-bit operations.
+    int split_slices = 0;       // 0: Pade and squaring products in plain FP64
+    long long split_launches = 0;
+    double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;
     cudaEvent_t take_event();
-    void drain_events();        // sums finished event pairs into gemm_ms_done
+    void drain_events();        // sums finished event pairs into gemm_ms_done / split_ms_done
 
     // Batched work runs on worker contexts (one host thread and one stream
     // each), created on first use, so that independent matrices overlap on
@@ -160,6 +166,15 @@ GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, do
 // One complex product on a caller's stream, with no context: allocates and
 // uploads nothing (the entry point for callers that cannot allocate).
 void gemm_detached_complex(cudaStream_t stream, int device, int* d_err, const GemmProblem& p);
+// Split-precision products C := A B (beta 0) or C += A B (beta 1) from
+// `slices` 8-bit slices per operand on the tcgen05 tensor cores (ozaki.cu).
+struct SplitProduct {
+    const DMat* a;
+    const DMat* b;
+    DMat* c;
+    double beta;
+};
+void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int slices);
 // The thread's message for errors raised outside any context (tns_last_error(NULL)).
 void set_detached_error(const std::string& msg);
 

@@ -75,6 +75,28 @@ int tns_zgemm(tns_context* ctx, int m, int n, int k, const double* alpha, const 
 int tns_zgemm_device(tns_context* ctx, int m, int n, int k, const double* alpha, const double* a,
                      int lda, const double* b, int ldb, const double* beta, double* c, int ldc);
 
+/* ---- split-precision form ------------------------------------------------ */
+
+/* C := A*B in the split-precision form: each operand is cut into `slices`
+ * (4..8) signed 8-bit slices under power-of-two row (A) and column (B) scales,
+ * the slice products run on the 8-bit tensor cores with exact 32-bit
+ * accumulation and are recombined in FP64. With 8 slices the result agrees
+ * with the FP64 product to about K * 2^-56 of the row and column scales; it
+ * does not reproduce the reference's rounding. Complex operands keep four real
+ * multiplications per complex multiply-add (never 3M). No counterpart in the
+ * reference: this is the split-precision form of ComplexKernels.Multiply
+ * (src/Tensile/ComplexKernels.cs:49-108) and Gemm (src/Tensile.Kernels/Gemm.cs:117-203). */
+int tns_dgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                    double* c, int ldc, int slices);
+int tns_zgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
+                    double* c, int ldc, int slices);
+/* 0 (the default): every product of Expm in plain FP64, the reference's
+ * rounding. 4..8: Expm's Pade-evaluation and squaring products in the
+ * split-precision form with that many slices; A^2, A^4, A^6 and every norm
+ * estimate that selects the degree and s stay in plain FP64, so the degree
+ * and s remain the reference's. */
+int tns_set_split_slices(tns_context* ctx, int slices);
+
 /* ---- exact norms -------------------------------------------------------- */
 
 /* kind: '1' (largest column sum), 'I' (largest row sum), 'F' (Frobenius,
@@ -230,6 +252,12 @@ typedef struct {
     double gemm_flops;
     double gemm_ms;
     double gemm_bytes;
+    /* the split-precision product's launches: FP64-equivalent flops (8mnk /
+     * 2mnk), 8-bit tensor operations actually issued, and their event time */
+    long long split_launches;
+    double split_flops;
+    double split_int8_ops;
+    double split_ms;
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
