@@ -188,19 +188,48 @@ def measured_fp64_peak(torch):
     return best
 
 
+def measured_int8_peak(torch):
+    """cuBLASLt 8-bit GEMM TOPS (burst, torch._int_mm 8192^3) on this GPU: the
+    denominator of the split-precision kernel's roofline."""
+    n = 8192
+    try:
+        a = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-127, 127, (n, n), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        del a, b
+        torch.cuda.empty_cache()
+        return best, "torch._int_mm (cuBLASLt int8) 8192^3 measured in this process"
+    except Exception as exc:  # report the nominal figure, saying so
+        return 4500.0, f"nominal dense INT8 4.5 POPS (measurement failed: {type(exc).__name__})"
+
+
+def rel1_device(x, y):
+    """||x - y||_1 / ||y||_1 for matrices stored transposed (row j = column j)."""
+    return float((x - y).abs().sum(dim=1).max() / y.abs().sum(dim=1).max())
+
+
 def ours(args, world, rank, local, dist):
     import torch
     torch.cuda.set_device(local)
     from csharp_linearalgebra_b200 import Workspace
 
-    peak = None if args.no_peak else measured_fp64_peak(torch)
+    peak64 = None if args.no_peak else measured_fp64_peak(torch)
+    peak8, peak8_src = (None, None) if args.no_peak else measured_int8_peak(torch)
     orders, mats = make_sweep(args.count, args.seed + 1000 * rank)
     count = len(mats)
-    # device-resident inputs and outputs
+    # device-resident inputs and one set of outputs per form
     dev_in = [torch.from_numpy(m.T.copy()).to("cuda") for m in mats]  # row-major of A^T == column-major A
-    dev_out = [torch.empty_like(t) for t in dev_in]
     a_ptrs = [t.data_ptr() for t in dev_in]
-    o_ptrs = [t.data_ptr() for t in dev_out]
     in_bytes = sum(n * n * 16 for n in orders)
     # pinned host buffers for the end-to-end path
     host_in = [torch.from_numpy(m.T.copy()).pin_memory() for m in mats]
@@ -216,61 +245,83 @@ def ours(args, world, rank, local, dist):
         if dist is not None:
             dist.barrier()
 
-    def step_device():
-        return ws.expm_batched_device(count, orders, a_ptrs, orders, o_ptrs, orders)
-
-    for _ in range(args.warmup):
-        diags = step_device()
-    torch.cuda.synchronize()
-
-    # timed region, inputs resident in HBM
-    ws.reset_stats()
-    with ClockSampler(local) as clocks:
-        barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            diags = step_device()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    st_step = ws.stats()
-    ms = e0.elapsed_time(e1) / args.steps
-
-    # The dominant kernel (the grouped DMMA GEMM) timed launch by launch with
-    # CUDA events on the library's stream: one more sweep with a single group,
-    # so that no other stream shares the GPU with a timed launch.
-    ws.set_workers(1)
-    ws.reset_stats()
-    ws.set_timing(True)
-    step_device()
-    ws.set_timing(False)
-    st = ws.stats()
-    ws.set_workers(args.groups)
-    if dist is not None:
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * count / (ms * 1e-3)
+        return float(t.item())
 
-    # end to end through the host-buffer entry point
-    e2e_value = None
-    if not args.no_e2e:
-        barrier()
+    def run_form(moduli, inputs):
+        """Warm-up, K timed steps (inputs in HBM), one single-group sweep timed
+        launch by launch, and K end-to-end steps, all in one form."""
+        ws.set_split_moduli(moduli)
+        outs = [torch.empty_like(t) for t in inputs]
+        ip = [t.data_ptr() for t in inputs]
+        op = [t.data_ptr() for t in outs]
+
+        def step():
+            return ws.expm_batched_device(count, orders, ip, orders, op, orders)
+
+        for _ in range(args.warmup):
+            diags = step()
         torch.cuda.synchronize()
-        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        for _ in range(args.steps):
-            ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
-        e3.record(stream)
-        torch.cuda.synchronize()
-        ms_e2e = e2.elapsed_time(e3) / args.steps
-        if dist is not None:
-            t = torch.tensor([ms_e2e], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
-        e2e_value = world * count / (ms_e2e * 1e-3)
+        ws.reset_stats()
+        with ClockSampler(local) as clocks:
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                diags = step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+        st_step = ws.stats()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        # The dominant kernels timed launch by launch with CUDA events on the
+        # library's stream: one more sweep with a single group, so that no
+        # other stream shares the GPU with a timed launch.
+        ws.set_workers(1)
+        ws.reset_stats()
+        ws.set_timing(True)
+        step()
+        ws.set_timing(False)
+        st = ws.stats()
+        ws.set_workers(args.groups)
+        e2e_ms = None
+        if not args.no_e2e:
+            barrier()
+            torch.cuda.synchronize()
+            e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e2.record(stream)
+            for _ in range(args.steps):
+                ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
+            e3.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = max_over_ranks(e2.elapsed_time(e3) / args.steps)
+        return {"ms": ms, "st_step": st_step, "st": st, "clocks": clocks.summary(), "diags": diags,
+                "e2e_ms": e2e_ms, "outs": outs}
+
+    plain = run_form(0, dev_in)
+    split = run_form(args.moduli, dev_in)
+    assert [(d.degree, d.squarings) for d in plain["diags"]] == [(d.degree, d.squarings) for d in split["diags"]]
+
+    # Accuracy of the split form against the plain FP64 form (bit-identical to
+    # the reference's result), next to each matrix's FP64 floor: how far the
+    # plain result moves when the input moves by about one ulp.
+    gen = torch.Generator(device="cuda").manual_seed(12345)
+    pert = [t * (1.0 + 2.0 ** -52 * torch.randn(t.shape, dtype=torch.float64, device="cuda", generator=gen))
+            for t in dev_in]
+    ws.set_split_moduli(0)
+    pert_out = [torch.empty_like(t) for t in pert]
+    ws.expm_batched_device(count, orders, [t.data_ptr() for t in pert], orders, [t.data_ptr() for t in pert_out],
+                           orders)
+    torch.cuda.synchronize()
+    errs = [rel1_device(s, p) for s, p in zip(split["outs"], plain["outs"])]
+    floors = [rel1_device(q, p) for q, p in zip(pert_out, plain["outs"])]
+    ratios = [e / f if f > 0 else (0.0 if e == 0 else float("inf")) for e, f in zip(errs, floors)]
+    del pert, pert_out
 
     # CPU baseline (rank 0, N = 1 only): the oracle on a bounded sample
     cpu = None
@@ -286,39 +337,74 @@ def ours(args, world, rank, local, dist):
                "sample": f"first {len(sample)} matrices of this sweep (orders {[orders[i] for i in sample]}), "
                          f"{dt:.1f} s, C++ restatement of the reference, all host threads"}
 
-    achieved = st["gemm_flops"] / (st["gemm_ms"] * 1e-3) / 1e12 if st["gemm_ms"] > 0 else None
-    degrees = sorted(set((d.degree, d.squarings) for d in diags))
+    def dmma_roofline(r):
+        st = r["st"]
+        achieved = st["gemm_flops"] / (st["gemm_ms"] * 1e-3) / 1e12 if st["gemm_ms"] > 0 else None
+        return {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA, complex 4M)",
+                "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": (achieved / peak64) if (achieved and peak64) else None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": (GEMM_TRAFFIC_RATIO * st["gemm_bytes"] / st["gemm_launches"])
+                           if st["gemm_launches"] else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every GEMM launch of "
+                                  "the 16-matrix sweep = 0.711 x its algorithmic bytes "
+                                  "(profiles/gemm_dmma_complex_sweep16.md), scaled to this sweep's "
+                                  "algorithmic bytes per launch",
+                "timing": "CUDA events around every GEMM launch of one extra sweep run as a single group",
+                "gemm_launches_per_sweep": int(st["gemm_launches"]),
+                "gemm_tflop_per_sweep": st["gemm_flops"] / 1e12,
+                "algorithmic_bytes_per_launch": st["gemm_bytes"] / st["gemm_launches"] if st["gemm_launches"] else None}
+
+    def rate(ms):
+        return world * count / (ms * 1e-3) if ms else None
+
+    sst = split["st"]
+    int8_tops = sst["split_int8_ops"] / (sst["split_ms"] * 1e-3) / 1e12 if sst["split_ms"] > 0 else None
+    degrees = sorted(set((d.degree, d.squarings) for d in split["diags"]))
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 (complex128, FP64 DMMA)", "data": "synthetic, seeded",
-            "config": {"workload": WORKLOAD, "count": count, "seed": args.seed, "form": "plain FP64 (DMMA)",
+            "metric": METRIC, "value": rate(split["ms"]), "unit": "expm/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": split["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": f"f64 results; Pade/squaring products from int8 residues modulo {args.moduli} moduli "
+                     "(exact int32 sums, CRT reconstruction in f64); decisions, LU and solve in f64",
+            "data": "synthetic, seeded",
+            "config": {"workload": WORKLOAD, "count": count, "seed": args.seed,
+                       "form": f"split precision, {args.moduli} moduli (tcgen05 kind::i8, Chinese remainder "
+                               "reconstruction) for the Pade-evaluation and squaring products; A^2, A^4, A^6, norms, "
+                               "normest1, LU and the Pade solve in plain FP64",
                        "l2": f"inputs larger than L2: {in_bytes / 1e9:.2f} GB of matrices per step per GPU",
                        "parallelism": f"independent matrices; {world} rank(s), each its own sweep",
                        "squarings_range": [min(s for _, s in degrees), max(s for _, s in degrees)]},
-            "e2e": {"value": e2e_value, "unit": "expm/s", "h2d_bytes_per_step": in_bytes,
+            "e2e": {"value": rate(split["e2e_ms"]), "unit": "expm/s", "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": in_bytes},
-            "roofline": {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA, complex 4M)",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (MEASURED_PEAKS.json has no FP64 figure)",
-                         "traffic": (GEMM_TRAFFIC_RATIO * st["gemm_bytes"] / st["gemm_launches"])
-                                    if st["gemm_launches"] else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every GEMM launch of "
-                                           "the 16-matrix sweep = 0.711 x its algorithmic bytes "
-                                           "(profiles/gemm_dmma_complex_sweep16.md), scaled to this sweep's "
-                                           "algorithmic bytes per launch",
-                         "timing": "CUDA events around every GEMM launch of one extra sweep run as a single group",
-                         "gemm_launches_per_sweep": int(st["gemm_launches"]),
-                         "gemm_tflop_per_sweep": st["gemm_flops"] / 1e12,
-                         "algorithmic_bytes_per_launch":
-                             st["gemm_bytes"] / st["gemm_launches"] if st["gemm_launches"] else None,
-                         "gemm_aggregate_tflops_in_timed_steps":
-                             st_step["gemm_flops"] / (ms * args.steps * 1e-3) / 1e12 if ms > 0 else None},
+            "roofline": {"bound": "tensor", "kernel": "modular_gemm_kernel (tcgen05.mma kind::i8, TMEM accumulators)",
+                         "achieved": int8_tops, "peak": peak8, "unit": "TOPS (int8)",
+                         "frac": (int8_tops / peak8) if (int8_tops and peak8) else None,
+                         "peak_source": peak8_src,
+                         "fp64_equivalent_tflops": sst["split_flops"] / (sst["split_ms"] * 1e-3) / 1e12
+                         if sst["split_ms"] > 0 else None,
+                         "traffic": None,
+                         "timing": "CUDA events around every split-product launch of one extra sweep run as a "
+                                   "single group; int8 operations counted on the padded residue extents",
+                         "split_launches_per_sweep": int(sst["split_launches"]),
+                         "split_int8_pops_per_sweep": sst["split_int8_ops"] / 1e15},
+            "split_accuracy": {
+                "vs": "plain FP64 GPU form (bit-identical to the reference's CPU result)",
+                "rel_err_1norm_max": max(errs), "rel_err_1norm_median": statistics.median(errs),
+                "frac_within_1e-12": sum(e <= 1e-12 for e in errs) / len(errs),
+                "max_ratio_to_fp64_floor": max(ratios), "median_ratio_to_fp64_floor": statistics.median(ratios),
+                "fp64_floor": "per matrix, ||expm(A(1+2^-52 z)) - expm(A)||_1 / ||expm(A)||_1 in the plain form, "
+                              "z ~ N(0,1) entrywise: the distance any arithmetic that is not the reference's bit "
+                              "for bit can be expected to have",
+                "fp64_floor_max": max(floors)},
+            "plain_fp64": {"value": rate(plain["ms"]), "ms_per_step": plain["ms"],
+                           "e2e": rate(plain["e2e_ms"]), "gpu_launches": int(plain["st_step"]["kernel_launches"]),
+                           "bit_identical_to_reference": True, "roofline": dmma_roofline(plain),
+                           "clocks": plain["clocks"]},
             "cpu_baseline": cpu,
-            "clocks": clocks.summary(),
-            "gpu_launches": int(st_step["kernel_launches"]),
+            "clocks": split["clocks"],
+            "gpu_launches": int(split["st_step"]["kernel_launches"]),
         }
         print(json.dumps(line), flush=True)
     ws.dispose()
@@ -337,7 +423,8 @@ def main():
     p.add_argument("--ref-budget", type=float, default=2e9, help="sum of n^3 per reference-arm step")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
-    p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS DGEMM peak (profiling runs)")
+    p.add_argument("--no-peak", action="store_true", help="skip the measured FP64/INT8 peaks (profiling runs)")
+    p.add_argument("--moduli", type=int, default=20, help="moduli of the split-precision form (8..22)")
     args = p.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:

@@ -222,10 +222,11 @@ class Workspace:
                        _p(c), _ld(c))
         return c
 
-    def multiply_split(self, a, b, slices: int = 8):
-        """A*B in the split-precision form (8-bit slices on the tensor cores,
-        FP64 recombination); within about K * 2^(-7 slices) of the row and
-        column scales of the FP64 product. Returns a new matrix."""
+    def multiply_split(self, a, b, moduli: int = 20):
+        """A*B in the split-precision form: t-bit integer images of the
+        operands (power-of-two row and column scales), their residues modulo
+        `moduli` coprime moduli multiplied on the 8-bit tensor cores, the
+        product rebuilt by the Chinese remainder theorem. Returns a new matrix."""
         cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
         a, b = _fortran(a, cplx), _fortran(b, cplx)
         if a.ndim != 2 or b.ndim != 2:
@@ -236,13 +237,13 @@ class Workspace:
             raise ValueError(f"Inner dimensions disagree: A is {m}x{k}, B is {k2}x{n}.")
         c = np.zeros((m, n), dtype=a.dtype, order="F")
         name = "tns_zgemm_split" if cplx else "tns_dgemm_split"
-        self._call(name, m, n, k, _p(a), _ld(a), _p(b), _ld(b), _p(c), _ld(c), int(slices))
+        self._call(name, m, n, k, _p(a), _ld(a), _p(b), _ld(b), _p(c), _ld(c), int(moduli))
         return c
 
-    def set_split_slices(self, slices: int):
-        """0: Expm entirely in plain FP64 (the reference's rounding); 4..8: its
+    def set_split_moduli(self, moduli: int):
+        """0: Expm entirely in plain FP64 (the reference's rounding); 8..22: its
         Pade-evaluation and squaring products in the split-precision form."""
-        self._call("tns_set_split_slices", int(slices))
+        self._call("tns_set_split_moduli", int(moduli))
 
     # -- norms --------------------------------------------------------------
     def _norm(self, a, kind: bytes) -> float:

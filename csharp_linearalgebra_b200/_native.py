@@ -62,7 +62,7 @@ SIGNATURES = {
     "tns_zgemm_device": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
     "tns_dgemm_split": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
     "tns_zgemm_split": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
-    "tns_set_split_slices": (_I, [_P, _I]),
+    "tns_set_split_moduli": (_I, [_P, _I]),
     "tns_dnorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
     "tns_znorm": (_I, [_P, _CH, _I, _I, _P, _I, C.POINTER(_D)]),
     "tns_dgetrf": (_I, [_P, _I, _I, _P, _I, _I, _P, C.POINTER(LuInfo)]),

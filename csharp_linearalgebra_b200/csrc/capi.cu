@@ -110,18 +110,18 @@ int gemm_entry(tns_context* c, bool cplx, bool dev, int m, int n, int k, const d
 }
 
 int gemm_split_entry(tns_context* c, bool cplx, int m, int n, int k, const double* a, int lda, const double* b,
-                     int ldb, double* cm, int ldc, int slices) {
+                     int ldb, double* cm, int ldc, int moduli) {
     return guarded(c, [&](Context& ctx) {
         check_operand(a, m, k, lda, "A");
         check_operand(b, k, n, ldb, "B");
         check_operand(cm, m, n, ldc, "C");
-        require(slices >= 4 && slices <= 8, TNS_E_ARGUMENT, "split-precision products take 4 to 8 slices");
+        require(moduli >= 8 && moduli <= 22, TNS_E_ARGUMENT, "split-precision products take 8 to 22 moduli");
         if (m == 0 || n == 0) return;
         DMat A = upload(ctx, a, m, k, lda, cplx, false, "the A operand");
         DMat B = upload(ctx, b, k, n, ldb, cplx, false, "the B operand");
         DMat C(ctx, m, n, cplx, "the C operand");
         std::vector<tns::SplitProduct> v{tns::SplitProduct{&A, &B, &C, 0.0}};
-        tns::gemm_split_batch(ctx, v, slices);
+        tns::gemm_split_batch(ctx, v, moduli);
         tns::copy_out(ctx, C, cm, ldc, false);
         ctx.sync();
     });
@@ -358,7 +358,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             Context& wc = *ctx.workers[w];
             wc.max_elements = ctx.max_elements;
             wc.timing = ctx.timing;
-            wc.split_slices = ctx.split_slices;
+            wc.split_moduli = ctx.split_moduli;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
                 run_group(wc, groups[w]);
@@ -500,19 +500,19 @@ int tns_zgemm_device(tns_context* c, int m, int n, int k, const double* alpha, c
 }
 
 int tns_dgemm_split(tns_context* c, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
-                    double* cm, int ldc, int slices) {
-    return gemm_split_entry(c, false, m, n, k, a, lda, b, ldb, cm, ldc, slices);
+                    double* cm, int ldc, int moduli) {
+    return gemm_split_entry(c, false, m, n, k, a, lda, b, ldb, cm, ldc, moduli);
 }
 int tns_zgemm_split(tns_context* c, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
-                    double* cm, int ldc, int slices) {
-    return gemm_split_entry(c, true, m, n, k, a, lda, b, ldb, cm, ldc, slices);
+                    double* cm, int ldc, int moduli) {
+    return gemm_split_entry(c, true, m, n, k, a, lda, b, ldb, cm, ldc, moduli);
 }
-int tns_set_split_slices(tns_context* c, int slices) {
+int tns_set_split_moduli(tns_context* c, int moduli) {
     return guarded(c, [&](Context& ctx) {
-        require(slices == 0 || (slices >= 4 && slices <= 8), TNS_E_ARGUMENT,
-                "split slices must be 0 (plain FP64) or 4 to 8");
-        ctx.split_slices = slices;
-        for (auto& w : ctx.workers) w->split_slices = slices;
+        require(moduli == 0 || (moduli >= 8 && moduli <= 22), TNS_E_ARGUMENT,
+                "split moduli must be 0 (plain FP64) or 8 to 22");
+        ctx.split_moduli = moduli;
+        for (auto& w : ctx.workers) w->split_moduli = moduli;
     });
 }
 

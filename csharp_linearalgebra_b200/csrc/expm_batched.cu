@@ -149,9 +149,20 @@ std::vector<double> power_norms(Context& ctx, const std::vector<const DMat*>& ma
     return mats[0]->cplx ? power_estimates<CplxE>(ctx, mats, power) : power_estimates<RealE>(ctx, mats, power);
 }
 
+// Whether a product may take the split-precision form when the context asks
+// for it: the powers that feed the degree and s decisions (A^2, A^4, A^6)
+// never do; the Pade evaluation and the squarings may.
+enum class Form { kExact, kSplittable };
+
 void product_batch(Context& ctx, std::vector<std::pair<const DMat*, const DMat*>> ab, std::vector<DMat*> c,
-                   double beta) {
+                   double beta, Form form = Form::kExact) {
     if (ab.empty()) return;
+    if (form == Form::kSplittable && ctx.split_moduli > 0) {
+        std::vector<SplitProduct> v;
+        for (size_t k = 0; k < ab.size(); ++k) v.push_back(SplitProduct{ab[k].first, ab[k].second, c[k], beta});
+        gemm_split_batch(ctx, v, ctx.split_moduli);
+        return;
+    }
     std::vector<GemmProblem> probs;
     for (size_t k = 0; k < ab.size(); ++k) probs.push_back(make_gemm(*ab[k].first, *ab[k].second, *c[k], 1.0, 0.0, beta, 0.0));
     gemm_grouped(ctx, probs, ab[0].first->cplx);
@@ -307,7 +318,7 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
                 ab.push_back({&j.a4, &j.a4});
                 c.push_back(&j.a8);
             }
-        product_batch(ctx, ab, c, 0.0);
+        product_batch(ctx, ab, c, 0.0, Form::kSplittable);
         // The powers of degree-13 jobs are no longer needed.
         for (auto& j : jobs)
             if (j.degree == 13) {
@@ -383,7 +394,7 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
                 ab.push_back({&ev[k].b6, &ev[k].inner_even});
                 c.push_back(&ev[k].v);
             }
-        product_batch(ctx, ab, c, 1.0);
+        product_batch(ctx, ab, c, 1.0, Form::kSplittable);
         // u = A w (B w for degree 13).
         ab.clear();
         c.clear();
@@ -392,7 +403,7 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
             ab.push_back({jobs[k].degree == 13 ? &ev[k].b : jobs[k].a, &ev[k].w});
             c.push_back(&ev[k].u);
         }
-        product_batch(ctx, ab, c, 0.0);
+        product_batch(ctx, ab, c, 0.0, Form::kSplittable);
     }
     // SolvePade (:372-405): den = v - u, num = v + u, LU of den, solve.
     std::vector<DMat> den(cnt), num(cnt);
@@ -451,7 +462,7 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
                     ab.push_back({&num[k], &num[k]});
                     c.push_back(&sq[k]);
                 }
-            product_batch(ctx, ab, c, 0.0);
+            product_batch(ctx, ab, c, 0.0, Form::kSplittable);
             for (size_t k = 0; k < cnt; ++k)
                 if (jobs[k].s > r) std::swap(num[k], sq[k]);
         }

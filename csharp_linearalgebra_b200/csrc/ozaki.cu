@@ -1,38 +1,47 @@
 // Split-precision products: FP64 (real or complex) C := A B (+ C) computed
-// from 8-bit integer slices on the tcgen05 tensor cores, with exact 32-bit
-// integer accumulation and FP64 recombination (the Ozaki scheme).
+// from 8-bit integer residues on the tcgen05 tensor cores, with exact 32-bit
+// integer accumulation and a Chinese-remainder reconstruction in FP64
+// (the modular form of the Ozaki scheme).
 //
-// Slicing. Every row i of A is scaled by 2^-e_i, every column j of B by
-// 2^-f_j, where 2^e bounds the row's (column's) largest magnitude from above
-// (complex: the larger of |Re| and |Im|, shared by both parts), so every
-// scaled entry x lies in (-1, 1). Then S signed 8-bit slices are peeled off
-// exactly: x <- 128 x, a_s = trunc(x), x <- x - a_s, so that
-//     A[i,k] = 2^e_i * sum_s a_s[i,k] 2^(-7 s)   (to 7 S bits of the row's scale).
-// Product. The slice products with equal weight 2^(-7 d), d = s + t, are summed
-// in one 32-bit integer accumulator (exact: |a_s|,|b_t| <= 127, at most S
-// pairs, K' <= the limit checked on the host); pairs with d > S + 1 are left
-// out, below the precision of the scheme. The FP64 result is
-//     C[i,j] = 2^(e_i + f_j) * sum_{d = S+1 .. 2} 2^(-7 d) P_d[i,j],
-// summed from the smallest weight to the largest.
+// Integers. Every row i of A is scaled by 2^(t - e_i), every column j of B by
+// 2^(t - f_j), where 2^e bounds the row's (column's) largest magnitude from
+// above (complex: the larger of |Re| and |Im|, shared by both parts), and
+// rounded to the nearest integer: A' = rint(A 2^(t-e)), |A'| <= 2^t. Both steps
+// are exact in FP64 (a power-of-two scaling, then rint), so the only error of
+// the scheme is this rounding, 1/2 in the last of t bits of the row's scale.
+// Residues. For each of N pairwise coprime moduli p <= 256 (256, 255, 253,
+// 251, 247, 241, ... -- their prime factors are disjoint), A' mod p and
+// B' mod p are taken exactly (as symmetric residues, |r| <= 128, in 8 bits).
+// Products. For each modulus, R = (A' mod p)(B' mod p) is one 8-bit GEMM with
+// exact 32-bit accumulation (|r|^2 K' < 2^31); R mod p = (A'B') mod p. t is
+// the largest value with 2 K' 2^(2t) < P = prod(p), so A'B' is the unique
+// residue class representative in (-P/2, P/2).
+// Reconstruction. With u_q = (R_q y_q) mod p_q, y_q = (P/p_q)^-1 mod p_q,
+// A'B' / P = frac(sum_q u_q / p_q) (the representative in [-1/2, 1/2]); the
+// sum runs in double-double (1/p_q as a double-double, products by FMA, the
+// integer part dropped after every term), and A'B' = frac * P, then
+// C = A'B' 2^(e_i + f_j - 2t). The reconstruction's own error, below 2^-100 of
+// P, is far under the rounding of A' and B'.
 // Complex. With the real and imaginary parts sharing their exponents, the
 // complex product is the single real product
 //     [Ar Ai] * [[Br, Bi], [-Bi, Br]]   (columns of the right factor interleaved,
 // so that output columns 2j, 2j+1 are Re, Im of C[:, j]) -- four real
 // multiplications per complex multiply-add, as the 4M method (never 3M).
 //
-// Kernel. One CTA per 128 x 128 output tile: a TMA producer warp streams
-// 128 x 128-byte slice tiles (128-byte swizzle) through a 4-stage mbarrier
-// ring; one thread issues tcgen05.mma kind::i8 (M = N = 128, K = 32) into one of
-// two TMEM accumulators (columns 0..255); four epilogue warps read each
-// finished accumulator (tcgen05.ld), add its weighted FP64 value into a
-// running FP64 sum kept in TMEM (columns 256..511, two per double) and, after
-// the last weight, scale and store C. The epilogue of one weight overlaps
-// the MMAs of the next. Every wait is bounded; TMEM is released on every path.
+// Kernels. Residues: one thread per 16 bytes of a residue row, all moduli.
+// Product: one CTA per 128 x 128 output tile and all moduli: a TMA producer
+// warp streams 128 x 128-byte residue tiles (128-byte swizzle) through a
+// 4-stage mbarrier ring; one thread issues tcgen05.mma kind::i8 (M = N = 128,
+// K = 32) into one of two TMEM accumulators; four epilogue warps reduce each
+// finished accumulator to u_q (tcgen05.ld) and store it as a byte plane while
+// the next modulus' MMAs run. Every wait is bounded; TMEM is released on
+// every path. Reconstruction: one CTA per 32 x 32 output tile, all planes
+// staged in shared memory, one column of 32 rows per warp store.
 //
-// Accuracy: the result differs from an FP64 product by at most about
-// K 2^(-7 S) (row scale)(column scale) per entry; with S = 8 that is at the
-// level of FP64 rounding for the orders used here. It does not reproduce the
-// reference's rounding order; it is the split-precision form of the product.
+// Accuracy: each entry differs from the exact product by at most about
+// K 2^-t of its row scale times its column scale (A' and B' rounded), the
+// split-precision form's only error; with 20 moduli and K' <= 2048, t = 71.
+// It does not reproduce the reference's rounding.
 
 #include "batch.cuh"
 #include "device_util.cuh"
@@ -44,6 +53,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -51,15 +61,33 @@ namespace tns {
 
 namespace {
 
-constexpr int kTile = 128;       // output tile rows and columns; slice tile rows
+constexpr int kMaxModuli = 22;
+// Pairwise coprime, largest first: 2^8, 3*5*17, 11*23, 251, 13*19, then primes
+// and 7*31.
+constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223,
+                                     217, 211, 199, 197, 193, 191, 181, 179, 173, 167, 163};
+
+constexpr int kTile = 128;       // output tile rows and columns; residue tile rows
 constexpr int kKb = 128;         // bytes (8-bit elements) of K per stage
 constexpr int kStages = 4;
 constexpr uint32_t kStageBytes = 2u * kTile * kKb;  // A and B tiles, 16 KB each
 constexpr int kSplitThreads = 192;                  // producer, MMA, 4 epilogue warps
-constexpr uint32_t kTmemCols = 512;                 // 2 x 128 accumulators + 128 doubles
+constexpr uint32_t kTmemCols = 256;                 // two 128-column accumulators
 constexpr int kSplitSmem = kStages * (int)kStageBytes + 1024 + 256;
 
 enum : int { kErrSplitFull = 11, kErrSplitEmpty = 12, kErrSplitAcc = 13, kErrSplitDrain = 14 };
+
+// The moduli of one product form and the constants of its reconstruction.
+struct CrtParams {
+    int nm;                       // moduli used
+    int t;                        // integer bits of the scaled operands
+    int p[kMaxModuli];            // moduli
+    int y[kMaxModuli];            // (P / p)^-1 mod p
+    int pow36[kMaxModuli];        // 2^36 mod p
+    double inv_hi[kMaxModuli];    // 1/p as a double-double
+    double inv_lo[kMaxModuli];
+    double P_hi, P_lo;            // P = prod p as a double-double
+};
 
 // ---- exponents ---------------------------------------------------------------
 
@@ -110,37 +138,44 @@ __global__ void col_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
     if (lane == 0) d.out[j] = bound_exponent(m);
 }
 
-// ---- slicing ---------------------------------------------------------------------
+// ---- residues ----------------------------------------------------------------------
 
-// Peels S signed 8-bit slices off x in (-1, 1); exact.
-template <int S>
-__device__ __forceinline__ void peel(double x, int8_t (&a)[S]) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) {
-        x *= 128.0;
-        const double t = trunc(x);
-        x -= t;
-        a[s] = (int8_t)(int)t;
-    }
+// x = rint(v 2^shift), an integer-valued double with |x| <= 2^t (t <= 96); its
+// split x = h 2^36 + l into 64-bit integers (same sign, |l| < 2^36).
+__device__ __forceinline__ void to_integer(double v, int shift, long long& h, long long& l) {
+    const double x = rint(scalbn(v, shift));
+    const double hd = trunc(scalbn(x, -36));
+    h = (long long)hd;
+    l = (long long)(x - scalbn(hd, 36));
 }
 
-struct SliceDesc {
+// The symmetric residue of h 2^36 + l modulo p: in [-p/2, p - 1 - p/2].
+__device__ __forceinline__ int residue(long long h, long long l, int p, int pow36) {
+    int r = (int)(((h % p) * pow36 + l % p) % p);
+    const int half = p >> 1;
+    if (r > p - 1 - half) r -= p;
+    if (r < -half) r += p;
+    return r;
+}
+
+struct ResDesc {
     const double* src;  // A (rows x k) or B (k x cols), column-major, ld elements
     int ld, m, k;       // logical rows (A) or columns (B); depth
-    int rows_p, kp;     // padded slice extents: rows of the slice array, bytes per row
+    int rows_p, kp;     // padded residue extents: rows of a plane, bytes per row
     const int* e;       // exponents of the rows (A) or columns (B)
-    int8_t* dst;        // S x rows_p x kp
+    int8_t* dst;        // nm x rows_p x kp
 };
 
-// A': row i holds [Re A(i,:), Im A(i,:)] (real: A(i,:)), 16 bytes per thread.
-template <bool CPLX, int S>
-__global__ void slice_a_kernel(const __grid_constant__ Batch<SliceDesc> b) {
-    const SliceDesc& d = batch_item(b, blockIdx.z);
+// A' planes: row i holds [Re A(i,:), Im A(i,:)] (real: A(i,:)); 16 bytes of
+// one row per thread, every modulus.
+template <bool CPLX>
+__global__ void residue_a_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
+    const ResDesc& d = batch_item(b, blockIdx.z);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int c0 = blockIdx.y * 16;
     if (i >= d.rows_p || c0 >= d.kp) return;
-    const int e = i < d.m ? d.e[i] : 0;
-    alignas(16) int8_t out[S][16];
+    const int shift = cp.t - (i < d.m ? d.e[i] : 0);
+    long long h[16], l[16];
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const int kk = c0 + u;
@@ -153,29 +188,30 @@ __global__ void slice_a_kernel(const __grid_constant__ Batch<SliceDesc> b) {
                 v = d.src[(size_t)kk * d.ld + i];
             }
         }
-        int8_t a[S];
-        peel<S>(scalbn(v, -e), a);
-#pragma unroll
-        for (int s = 0; s < S; ++s) out[s][u] = a[s];
+        to_integer(v, shift, h[u], l[u]);
     }
+    for (int q = 0; q < cp.nm; ++q) {
+        alignas(16) int8_t out[16];
 #pragma unroll
-    for (int s = 0; s < S; ++s)
-        *reinterpret_cast<int4*>(d.dst + ((size_t)s * d.rows_p + i) * d.kp + c0) = *reinterpret_cast<int4*>(out[s]);
+        for (int u = 0; u < 16; ++u) out[u] = (int8_t)residue(h[u], l[u], cp.p[q], cp.pow36[q]);
+        *reinterpret_cast<int4*>(d.dst + ((size_t)q * d.rows_p + i) * d.kp + c0) = *reinterpret_cast<int4*>(out);
+    }
 }
 
-// B': row n of the right factor, K-major. Complex: row 2j = [Re B(:,j); -Im B(:,j)],
-// row 2j+1 = [Im B(:,j); Re B(:,j)]; real: row j = B(:,j). 16 bytes per thread.
-template <bool CPLX, int S>
-__global__ void slice_b_kernel(const __grid_constant__ Batch<SliceDesc> b) {
-    const SliceDesc& d = batch_item(b, blockIdx.y);
+// B' planes: row n of the right factor, K-major. Complex: row 2j =
+// [Re B(:,j); -Im B(:,j)], row 2j+1 = [Im B(:,j); Re B(:,j)]; real: row j =
+// B(:,j). 16 bytes of one row per thread, every modulus.
+template <bool CPLX>
+__global__ void residue_b_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
+    const ResDesc& d = batch_item(b, blockIdx.y);
     const int chunks = d.kp / 16;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)chunks * d.rows_p) return;
     const int n = (int)(idx / chunks), c0 = (int)(idx % chunks) * 16;
     const int j = CPLX ? n / 2 : n;
     const bool live = j < d.m;
-    const int e = live ? d.e[j] : 0;
-    alignas(16) int8_t out[S][16];
+    const int shift = cp.t - (live ? d.e[j] : 0);
+    long long h[16], l[16];
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const int kk = c0 + u;
@@ -193,35 +229,32 @@ __global__ void slice_b_kernel(const __grid_constant__ Batch<SliceDesc> b) {
                 v = d.src[(size_t)j * d.ld + kk];
             }
         }
-        int8_t a[S];
-        peel<S>(scalbn(v, -e), a);
-#pragma unroll
-        for (int s = 0; s < S; ++s) out[s][u] = a[s];
+        to_integer(v, shift, h[u], l[u]);
     }
+    for (int q = 0; q < cp.nm; ++q) {
+        alignas(16) int8_t out[16];
 #pragma unroll
-    for (int s = 0; s < S; ++s)
-        *reinterpret_cast<int4*>(d.dst + ((size_t)s * d.rows_p + n) * d.kp + c0) = *reinterpret_cast<int4*>(out[s]);
+        for (int u = 0; u < 16; ++u) out[u] = (int8_t)residue(h[u], l[u], cp.p[q], cp.pow36[q]);
+        *reinterpret_cast<int4*>(d.dst + ((size_t)q * d.rows_p + n) * d.kp + c0) = *reinterpret_cast<int4*>(out);
+    }
 }
 
-// ---- the product --------------------------------------------------------------------
+// ---- the products, one per modulus ---------------------------------------------------
 
-struct SplitDesc {
-    int m, n;                // output rows and (complex or real) columns
-    int kp;                  // bytes per slice row (multiple of 128)
+struct ModDesc {
+    int kp;                  // bytes per residue row (multiple of 128)
+    int np;                  // columns of an output plane (multiple of 128)
+    int mp;                  // rows of an output plane (multiple of 128)
     int tiles_m, tile_begin;
-    const int* ea;           // row exponents of A
-    const int* eb;           // column exponents of B
-    double* c;               // column-major output (complex interleaved), ld elements
-    int ldc;
-    int accumulate;          // 0: C = AB, 1: C += AB
+    uint8_t* u;              // nm planes of mp x np bytes, row-major: u_q of each product entry
 };
-struct SplitMaps {
-    CUtensorMap a, b;  // slices as (kp bytes) x (rows) x S, boxes of 128 x 128 x 1, 128-byte swizzle
+struct ModMaps {
+    CUtensorMap a, b;  // residues as (kp bytes) x (rows) x nm, boxes of 128 x 128 x 1, 128-byte swizzle
 };
 
-template <bool CPLX, int S>
 __global__ void __launch_bounds__(kSplitThreads, 1)
-    split_gemm_kernel(const SplitDesc* __restrict__ descs, const SplitMaps* __restrict__ maps, int nprob, int* err) {
+    modular_gemm_kernel(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps, int nprob,
+                        const __grid_constant__ CrtParams cp, int* err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -240,11 +273,12 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         if (descs[mid].tile_begin <= (int)blockIdx.x) lo = mid;
         else hi = mid - 1;
     }
-    const SplitDesc& D = descs[lo];
-    const SplitMaps& MP = maps[lo];
+    const ModDesc& D = descs[lo];
+    const ModMaps& MP = maps[lo];
     const int local = blockIdx.x - D.tile_begin;
     const int m0 = (local % D.tiles_m) * kTile, n0 = (local / D.tiles_m) * kTile;
     const int nkb = D.kp / kKb;
+    const int nm = cp.nm;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -277,21 +311,17 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             tensormap_acquire(&MP.a);
             tensormap_acquire(&MP.b);
             bool ok = true;
-            for (int q = 0; q < S && ok; ++q) {
-                const int dsum = S + 1 - q;
-                for (int s = max(1, dsum - S); s <= min(S, dsum - 1) && ok; ++s) {
-                    const int t = dsum - s;
-                    for (int kb = 0; kb < nkb; ++kb) {
-                        const int st = issued % kStages;
-                        if (!mbar_wait_bounded(&empty[st], ((issued / kStages) & 1) ^ 1, err, kErrSplitEmpty)) {
-                            ok = false;
-                            break;
-                        }
-                        mbar_arrive_expect_tx(&full[st], kStageBytes);
-                        tma_load_3d(stage_a(st), &MP.a, kb * kKb, m0, s - 1, &full[st]);
-                        tma_load_3d(stage_b(st), &MP.b, kb * kKb, n0, t - 1, &full[st]);
-                        ++issued;
+            for (int q = 0; q < nm && ok; ++q) {
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int st = issued % kStages;
+                    if (!mbar_wait_bounded(&empty[st], ((issued / kStages) & 1) ^ 1, err, kErrSplitEmpty)) {
+                        ok = false;
+                        break;
                     }
+                    mbar_arrive_expect_tx(&full[st], kStageBytes);
+                    tma_load_3d(stage_a(st), &MP.a, kb * kKb, m0, q, &full[st]);
+                    tma_load_3d(stage_b(st), &MP.b, kb * kKb, n0, q, &full[st]);
+                    ++issued;
                 }
             }
         }
@@ -300,29 +330,25 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             constexpr uint32_t idesc = i8_instr_desc(kTile, kTile);
             uint32_t it = 0;
             bool ok = true;
-            for (int q = 0; q < S && ok; ++q) {
-                const int dsum = S + 1 - q, buf = q & 1;
+            for (int q = 0; q < nm && ok; ++q) {
+                const int buf = q & 1;
                 if (!mbar_wait_bounded(&acce[buf], ((q >> 1) & 1) ^ 1, err, kErrSplitAcc)) break;
                 tc_fence_after_sync();
                 const uint32_t dacc = tmem + buf * kTile;
-                bool first = true;
-                for (int s = max(1, dsum - S); s <= min(S, dsum - 1) && ok; ++s) {
-                    for (int kb = 0; kb < nkb; ++kb) {
-                        const int st = it % kStages;
-                        if (!mbar_wait_bounded(&full[st], (it / kStages) & 1, err, kErrSplitFull)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after_sync();
-#pragma unroll
-                        for (int kk = 0; kk < kKb / 32; ++kk) {
-                            mma_i8(dacc, sw128_kmajor_desc(stage_a(st), kk * 32), sw128_kmajor_desc(stage_b(st), kk * 32),
-                                   idesc, !(first && kk == 0));
-                        }
-                        first = false;
-                        mma_commit(&empty[st]);
-                        ++it;
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int st = it % kStages;
+                    if (!mbar_wait_bounded(&full[st], (it / kStages) & 1, err, kErrSplitFull)) {
+                        ok = false;
+                        break;
                     }
+                    tc_fence_after_sync();
+#pragma unroll
+                    for (int kk = 0; kk < kKb / 32; ++kk) {
+                        mma_i8(dacc, sw128_kmajor_desc(stage_a(st), kk * 32), sw128_kmajor_desc(stage_b(st), kk * 32),
+                               idesc, !(kb == 0 && kk == 0));
+                    }
+                    mma_commit(&empty[st]);
+                    ++it;
                 }
                 if (ok) mma_commit(&accf[buf]);
             }
@@ -330,79 +356,33 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             mma_commit(done);
         }
     } else {
-        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (the rows of the tile).
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (the rows of the
+        // tile) and stores u_q = (R mod p) y mod p as one byte per entry.
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
-        const int i = m0 + row;
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-        const int ei = i < D.m ? D.ea[i] : 0;
-        for (int q = 0; q < S; ++q) {
-            const int dsum = S + 1 - q, buf = q & 1;
+        for (int q = 0; q < nm; ++q) {
+            const int buf = q & 1;
             // The TMEM moves below are warp-collective: the warp goes on only
             // if every lane saw the accumulator complete.
             const bool got = mbar_wait_bounded(&accf[buf], (q >> 1) & 1, err, kErrSplitAcc);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after_sync();
-            const double w = scalbn(1.0, -7 * dsum);
+            const int p = cp.p[q], y = cp.y[q];
+            uint8_t* plane = D.u + ((size_t)q * D.mp + m0 + row) * D.np + n0;
             for (int c0 = 0; c0 < kTile; c0 += 16) {
-                uint32_t v[16], f0[16], f1[16];
+                uint32_t v[16];
                 tmem_ld16(tmem + lane_addr + buf * kTile + c0, v);
-                if (q > 0) {
-                    tmem_ld16(tmem + lane_addr + 2 * kTile + 2 * c0, f0);
-                    tmem_ld16(tmem + lane_addr + 2 * kTile + 2 * c0 + 16, f1);
-                }
                 tmem_wait_ld();
-                double acc[16];
+                alignas(16) uint8_t out[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
-                    const double x = (double)(int)v[e] * w;
-                    if (q > 0) {
-                        const uint32_t* f = e < 8 ? f0 : f1;
-                        const int o = (e & 7) * 2;
-                        acc[e] = __hiloint2double((int)f[o + 1], (int)f[o]) + x;
-                    } else {
-                        acc[e] = x;
-                    }
+                    int r = ((int)v[e] % p) * y % p;
+                    if (r < 0) r += p;
+                    out[e] = (uint8_t)r;
                 }
-                if (q < S - 1) {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        uint32_t* f = e < 8 ? f0 : f1;
-                        const int o = (e & 7) * 2;
-                        f[o] = (uint32_t)__double2loint(acc[e]);
-                        f[o + 1] = (uint32_t)__double2hiint(acc[e]);
-                    }
-                    tmem_st16(tmem + lane_addr + 2 * kTile + 2 * c0, f0);
-                    tmem_st16(tmem + lane_addr + 2 * kTile + 2 * c0 + 16, f1);
-                } else if (i < D.m) {
-                    if (CPLX) {
-#pragma unroll
-                        for (int e = 0; e < 16; e += 2) {
-                            const int j = (n0 + c0 + e) >> 1;
-                            if (j >= D.n) continue;
-                            const int sc = ei + D.eb[j];
-                            double2 r = make_double2(scalbn(acc[e], sc), scalbn(acc[e + 1], sc));
-                            double2* p = reinterpret_cast<double2*>(D.c) + (size_t)j * D.ldc + i;
-                            if (D.accumulate) {
-                                const double2 o = *p;
-                                r = make_double2(o.x + r.x, o.y + r.y);
-                            }
-                            *p = r;
-                        }
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < 16; ++e) {
-                            const int j = n0 + c0 + e;
-                            if (j >= D.n) continue;
-                            double r = scalbn(acc[e], ei + D.eb[j]);
-                            double* p = D.c + (size_t)j * D.ldc + i;
-                            if (D.accumulate) r += *p;
-                            *p = r;
-                        }
-                    }
-                }
+                *reinterpret_cast<int4*>(plane + c0) = *reinterpret_cast<int4*>(out);
             }
-            if (q < S - 1) tmem_wait_st();
             tc_fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[buf]);
@@ -425,6 +405,87 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     }
 }
 
+// ---- reconstruction ----------------------------------------------------------------------
+
+struct CrtDesc {
+    const uint8_t* u;   // nm planes, mp x np row-major
+    int mp, np;
+    int m, n;           // output rows and (complex or real) columns
+    const int* ea;      // row exponents of A
+    const int* eb;      // column exponents of B
+    double* c;          // column-major output (complex interleaved), ld elements
+    int ldc;
+    int accumulate;     // 0: C = AB, 1: C += AB
+};
+
+// A'B' / P = frac(sum_q u_q / p_q) in double-double, then A'B' = frac * P.
+__device__ __forceinline__ double reconstruct(const uint8_t* us, int stride, const CrtParams& cp) {
+    double fh = 0.0, fl = 0.0;
+    for (int q = 0; q < cp.nm; ++q) {
+        const double u = (double)us[q * stride];
+        const double ph = u * cp.inv_hi[q];
+        const double pl = fma(u, cp.inv_hi[q], -ph) + u * cp.inv_lo[q];
+        // (fh, fl) += (ph, pl), then drop the integer part
+        const double s = fh + ph;
+        const double bb = s - fh;
+        const double e = (fh - (s - bb)) + (ph - bb) + fl + pl;
+        fh = s + e;
+        fl = e - (fh - s);
+        const double k = rint(fh);
+        fh -= k;
+        const double s2 = fh + fl;
+        fl = fl - (s2 - fh);
+        fh = s2;
+    }
+    const double r = fh * cp.P_hi;
+    return r + (fma(fh, cp.P_hi, -r) + fh * cp.P_lo + fl * cp.P_hi);
+}
+
+// One CTA per 32 x 32 output tile: the tile's residue bytes of every modulus
+// in shared memory (rows of the planes read contiguously), then warp w
+// computes output columns w, w + 8, ..., one row per lane (column-major stores
+// of 32 consecutive rows).
+template <bool CPLX>
+__global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<CrtDesc> b,
+                                                  const __grid_constant__ CrtParams cp) {
+    const CrtDesc& d = batch_item(b, blockIdx.z);
+    constexpr int DPE = CPLX ? 2 : 1;
+    constexpr int TW = 32 * DPE;  // plane columns per tile
+    __shared__ uint8_t su[kMaxModuli][32][TW];
+    const int r0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    if (r0 >= d.m || j0 >= d.n) return;
+    const int nm = cp.nm;
+    for (int e = threadIdx.x; e < nm * 32 * TW; e += blockDim.x) {
+        const int q = e / (32 * TW), rr = (e / TW) % 32, cc = e % TW;
+        const int row = r0 + rr, col = j0 * DPE + cc;
+        su[q][rr][cc] = (row < d.mp && col < d.np) ? d.u[((size_t)q * d.mp + row) * d.np + col] : 0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = r0 + lane;
+    if (i >= d.m) return;
+    const int ei = d.ea[i];
+    for (int jj = warp; jj < 32; jj += 8) {
+        const int j = j0 + jj;
+        if (j >= d.n) break;
+        const int sc = ei + d.eb[j] - 2 * cp.t;
+        const double re = scalbn(reconstruct(&su[0][lane][jj * DPE], 32 * TW, cp), sc);
+        if (CPLX) {
+            const double im = scalbn(reconstruct(&su[0][lane][jj * DPE + 1], 32 * TW, cp), sc);
+            double2* p = reinterpret_cast<double2*>(d.c) + (size_t)j * d.ldc + i;
+            double2 r = make_double2(re, im);
+            if (d.accumulate) {
+                const double2 o = *p;
+                r = make_double2(o.x + r.x, o.y + r.y);
+            }
+            *p = r;
+        } else {
+            double* p = d.c + (size_t)j * d.ldc + i;
+            *p = d.accumulate ? *p + re : re;
+        }
+    }
+}
+
 // ---- host ------------------------------------------------------------------------------
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -440,10 +501,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// The slices of one operand as a 3-D byte array (kp x rows_p x S), boxes of
+// The residues of one operand as a 3-D byte array (kp x rows_p x nm), boxes of
 // 128 x 128 x 1 with 128-byte swizzle.
-void encode_slices(CUtensorMap* map, const int8_t* base, int kp, int rows_p, int S) {
-    cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows_p, (cuuint64_t)S};
+void encode_residues(CUtensorMap* map, const int8_t* base, int kp, int rows_p, int nm) {
+    cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows_p, (cuuint64_t)nm};
     cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)kp * rows_p};
     cuuint32_t box[3] = {(cuuint32_t)kKb, (cuuint32_t)kTile, 1};
     cuuint32_t elem[3] = {1, 1, 1};
@@ -454,12 +515,62 @@ void encode_slices(CUtensorMap* map, const int8_t* base, int kp, int rows_p, int
         fail(TNS_E_DEVICE, "TMA descriptor encoding for the split product failed (CUresult " + std::to_string((int)r) + ")");
 }
 
-template <bool CPLX, int S>
-void split_launch(Context& ctx, std::vector<SplitProduct>& v) {
+int inverse_mod(int a, int p) {  // a^-1 mod p, a and p coprime
+    int t = 0, nt = 1, r = p, nr = a % p;
+    while (nr != 0) {
+        const int qq = r / nr;
+        int tmp = t - qq * nt;
+        t = nt;
+        nt = tmp;
+        tmp = r - qq * nr;
+        r = nr;
+        nr = tmp;
+    }
+    return t < 0 ? t + p : t;
+}
+
+// Moduli and reconstruction constants for nm moduli and products of depth
+// kmax (the deepest K' of the batch).
+CrtParams crt_params(int nm, int kmax) {
+    CrtParams cp{};
+    cp.nm = nm;
+    double ph = 1.0, pl = 0.0;  // P as a double-double
+    for (int q = 0; q < nm; ++q) {
+        const int p = kModuli[q];
+        cp.p[q] = p;
+        int mq = 1;  // (P / p) mod p
+        for (int r = 0; r < nm; ++r)
+            if (r != q) mq = (int)((long long)mq * (kModuli[r] % p) % p);
+        cp.y[q] = inverse_mod(mq, p);
+        long long pw = 1;
+        for (int s = 0; s < 36; ++s) pw = pw * 2 % p;
+        cp.pow36[q] = (int)pw;
+        cp.inv_hi[q] = 1.0 / p;
+        cp.inv_lo[q] = std::fma(-cp.inv_hi[q], (double)p, 1.0) / p;
+        const double h = ph * p;
+        const double l = std::fma(ph, (double)p, -h) + pl * p;
+        ph = h + l;
+        pl = l - (ph - h);
+    }
+    cp.P_hi = ph;
+    cp.P_lo = pl;
+    // 2 K' 2^(2t) < P: with P >= 2^L and K' <= 2^c, 1 + c + 2t < L.
+    int L = 0;
+    std::frexp(ph, &L);
+    L -= 1;
+    int c = 0;
+    while ((1LL << c) < (long long)std::max(1, kmax)) ++c;
+    cp.t = std::min(96, (L - 2 - c) / 2);
+    if (cp.t < 8) fail(TNS_E_ARGUMENT, "too few moduli for a split-precision product of this depth");
+    return cp;
+}
+
+template <bool CPLX>
+void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
     constexpr int DPE = CPLX ? 2 : 1;
     struct Sizes {
         int m, n, k, mp, np, kp;
-        size_t a_off, b_off, ea_off, eb_off;
+        size_t a_off, b_off, u_off, ea_off, eb_off;
     };
     std::vector<Sizes> z;
     size_t total = 0;
@@ -468,6 +579,7 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v) {
         total += (bytes + 255) & ~size_t(255);
         return off;
     };
+    int kmax = 1;
     for (auto& p : v) {
         Sizes s{};
         s.m = p.a->rows;
@@ -476,23 +588,27 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v) {
         s.mp = round_up(s.m, kTile);
         s.np = round_up(DPE * s.n, kTile);
         s.kp = round_up(DPE * s.k, kKb);
-        // Exactness of the 32-bit sums: at most S pairs of K' products of |127|^2.
-        if ((double)S * s.kp * 127.0 * 127.0 >= 2147483647.0)
+        // Exact 32-bit sums of residue products (|r| <= 128).
+        if ((double)s.kp * 128.0 * 128.0 >= 2147483647.0)
             fail(TNS_E_ARGUMENT, "split-precision product too deep for exact 32-bit accumulation");
-        s.a_off = take((size_t)S * s.mp * s.kp);
-        s.b_off = take((size_t)S * s.np * s.kp);
+        kmax = std::max(kmax, DPE * s.k);
+        s.a_off = take((size_t)nm * s.mp * s.kp);
+        s.b_off = take((size_t)nm * s.np * s.kp);
+        s.u_off = take((size_t)nm * s.mp * s.np);
         s.ea_off = take(sizeof(int) * s.mp);
         s.eb_off = take(sizeof(int) * std::max(1, s.n));
         z.push_back(s);
     }
+    const CrtParams cp = crt_params(nm, kmax);
     DBuf scratch(ctx, total);
     auto at = [&](size_t off) { return static_cast<char*>(scratch.p) + off; };
 
     std::vector<ExpDesc> rows, cols;
-    std::vector<SliceDesc> sa, sb;
-    std::vector<SplitDesc> gd;
-    std::vector<SplitMaps> maps(v.size());
-    int max_m = 0, max_cols = 0, max_rows_a = 0, max_chunks = 0;
+    std::vector<ResDesc> ra, rb;
+    std::vector<ModDesc> md;
+    std::vector<CrtDesc> cd;
+    std::vector<ModMaps> maps(v.size());
+    int max_m = 0, max_cols = 0, max_rows_a = 0, max_chunks = 0, max_out_rows = 0, max_out_cols = 0;
     long long max_b_threads = 0;
     int tiles = 0;
     for (size_t q = 0; q < v.size(); ++q) {
@@ -502,30 +618,23 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v) {
         int* eb = reinterpret_cast<int*>(at(s.eb_off));
         int8_t* a8 = reinterpret_cast<int8_t*>(at(s.a_off));
         int8_t* b8 = reinterpret_cast<int8_t*>(at(s.b_off));
+        uint8_t* u8 = reinterpret_cast<uint8_t*>(at(s.u_off));
         rows.push_back(ExpDesc{p.a->p, p.a->ld(), s.m, s.k, ea});
         cols.push_back(ExpDesc{p.b->p, p.b->ld(), s.k, s.n, eb});
-        sa.push_back(SliceDesc{p.a->p, p.a->ld(), s.m, s.k, s.mp, s.kp, ea, a8});
-        sb.push_back(SliceDesc{p.b->p, p.b->ld(), s.n, s.k, s.np, s.kp, eb, b8});
-        SplitDesc g{};
-        g.m = s.m;
-        g.n = s.n;
-        g.kp = s.kp;
-        g.tiles_m = s.mp / kTile;
-        g.tile_begin = tiles;
-        g.ea = ea;
-        g.eb = eb;
-        g.c = p.c->p;
-        g.ldc = p.c->ld();
-        g.accumulate = p.beta != 0.0 ? 1 : 0;
-        gd.push_back(g);
+        ra.push_back(ResDesc{p.a->p, p.a->ld(), s.m, s.k, s.mp, s.kp, ea, a8});
+        rb.push_back(ResDesc{p.b->p, p.b->ld(), s.n, s.k, s.np, s.kp, eb, b8});
+        md.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles, u8});
+        cd.push_back(CrtDesc{u8, s.mp, s.np, s.m, s.n, ea, eb, p.c->p, p.c->ld(), p.beta != 0.0 ? 1 : 0});
         tiles += (s.mp / kTile) * (s.np / kTile);
-        encode_slices(&maps[q].a, a8, s.kp, s.mp, S);
-        encode_slices(&maps[q].b, b8, s.kp, s.np, S);
+        encode_residues(&maps[q].a, a8, s.kp, s.mp, nm);
+        encode_residues(&maps[q].b, b8, s.kp, s.np, nm);
         max_m = std::max(max_m, s.m);
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
         max_chunks = std::max(max_chunks, s.kp / 16);
         max_b_threads = std::max(max_b_threads, (long long)(s.kp / 16) * s.np);
+        max_out_rows = std::max(max_out_rows, s.m);
+        max_out_cols = std::max(max_out_cols, s.n);
     }
     if (tiles == 0) return;
     {
@@ -535,48 +644,53 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v) {
         Batch<ExpDesc> bc = make_batch(ctx, cols);
         col_exponent_kernel<CPLX><<<dim3((max_cols + 7) / 8, bc.count), 256, 0, ctx.stream>>>(bc);
         TNS_CUDA(cudaGetLastError());
-        Batch<SliceDesc> bsa = make_batch(ctx, sa);
-        slice_a_kernel<CPLX, S><<<dim3((max_rows_a + 127) / 128, max_chunks, bsa.count), 128, 0, ctx.stream>>>(bsa);
+        Batch<ResDesc> bra = make_batch(ctx, ra);
+        residue_a_kernel<CPLX><<<dim3((max_rows_a + 127) / 128, max_chunks, bra.count), 128, 0, ctx.stream>>>(bra, cp);
         TNS_CUDA(cudaGetLastError());
-        Batch<SliceDesc> bsb = make_batch(ctx, sb);
-        slice_b_kernel<CPLX, S><<<dim3((unsigned)((max_b_threads + 127) / 128), bsb.count), 128, 0, ctx.stream>>>(bsb);
+        Batch<ResDesc> brb = make_batch(ctx, rb);
+        residue_b_kernel<CPLX><<<dim3((unsigned)((max_b_threads + 127) / 128), brb.count), 128, 0, ctx.stream>>>(brb,
+                                                                                                                 cp);
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches += 4;
     }
     static bool configured[64] = {};
     if (!configured[ctx.device]) {
-        TNS_CUDA(cudaFuncSetAttribute(split_gemm_kernel<CPLX, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      kSplitSmem));
+        TNS_CUDA(cudaFuncSetAttribute(modular_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSplitSmem));
         configured[ctx.device] = true;
     }
-    const SplitDesc* d_desc = static_cast<const SplitDesc*>(ctx.upload(gd.data(), sizeof(SplitDesc) * gd.size()));
-    const SplitMaps* d_maps = static_cast<const SplitMaps*>(ctx.upload(maps.data(), sizeof(SplitMaps) * maps.size()));
+    const ModDesc* d_desc = static_cast<const ModDesc*>(ctx.upload(md.data(), sizeof(ModDesc) * md.size()));
+    const ModMaps* d_maps = static_cast<const ModMaps*>(ctx.upload(maps.data(), sizeof(ModMaps) * maps.size()));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ctx.timing) {
         e0 = ctx.take_event();
         e1 = ctx.take_event();
         TNS_CUDA(cudaEventRecord(e0, ctx.stream));
     }
-    split_gemm_kernel<CPLX, S><<<tiles, kSplitThreads, kSplitSmem, ctx.stream>>>(d_desc, d_maps, (int)gd.size(),
-                                                                                 ctx.d_err);
+    modular_gemm_kernel<<<tiles, kSplitThreads, kSplitSmem, ctx.stream>>>(d_desc, d_maps, (int)md.size(), cp,
+                                                                           ctx.d_err);
     TNS_CUDA(cudaGetLastError());
     if (ctx.timing) {
         TNS_CUDA(cudaEventRecord(e1, ctx.stream));
         ctx.split_events.emplace_back(e0, e1);
     }
-    ctx.kernel_launches++;
+    {
+        Batch<CrtDesc> b = make_batch(ctx, cd);
+        crt_kernel<CPLX><<<dim3((max_out_cols + 31) / 32, (max_out_rows + 31) / 32, b.count), 256, 0, ctx.stream>>>(
+            b, cp);
+        TNS_CUDA(cudaGetLastError());
+    }
+    ctx.kernel_launches += 2;
     ctx.split_launches++;
     for (size_t q = 0; q < v.size(); ++q) {
         const auto& s = z[q];
-        const int pairs = S * (S + 1) / 2;
-        ctx.split_int8_ops += 2.0 * s.mp * (double)s.np * s.kp * pairs;
+        ctx.split_int8_ops += 2.0 * s.mp * (double)s.np * s.kp * nm;
         ctx.split_flops += (CPLX ? 8.0 : 2.0) * (double)s.m * s.n * s.k;
     }
 }
 
 }  // namespace
 
-void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int slices) {
+void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int moduli) {
     std::vector<SplitProduct> live;
     for (auto& p : v) {
         if (p.a->cols != p.b->rows || p.c->rows != p.a->rows || p.c->cols != p.b->cols || p.a->cplx != p.b->cplx ||
@@ -585,21 +699,10 @@ void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int slices) {
         if (p.a->rows > 0 && p.b->cols > 0) live.push_back(p);
     }
     if (live.empty()) return;
-    const bool cplx = live[0].a->cplx;
-#define TNS_SPLIT(SV)                                              \
-    case SV:                                                       \
-        if (cplx) split_launch<true, SV>(ctx, live);               \
-        else split_launch<false, SV>(ctx, live);                   \
-        return;
-    switch (slices) {
-        TNS_SPLIT(4)
-        TNS_SPLIT(5)
-        TNS_SPLIT(6)
-        TNS_SPLIT(7)
-        TNS_SPLIT(8)
-        default: fail(TNS_E_ARGUMENT, "split-precision products take 4 to 8 slices");
-    }
-#undef TNS_SPLIT
+    if (moduli < 8 || moduli > kMaxModuli)
+        fail(TNS_E_ARGUMENT, "split-precision products take 8 to " + std::to_string(kMaxModuli) + " moduli");
+    if (live[0].a->cplx) split_launch<true>(ctx, live, moduli);
+    else split_launch<false>(ctx, live, moduli);
 }
 
 }  // namespace tns

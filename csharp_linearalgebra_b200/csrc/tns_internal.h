@@ -92,7 +92,7 @@ struct Context {
     double gemm_ms_done = 0.0;  // elapsed time of events already drained
     // The split-precision product's launches (counted and timed apart from the
     // FP64 GEMM's): FP64-equivalent algorithmic flops and 8-bit operations.
-    int split_slices = 0;       // 0: Pade and squaring products in plain FP64
+    int split_moduli = 0;       // 0: Pade and squaring products in plain FP64
     long long split_launches = 0;
     double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;
@@ -167,14 +167,15 @@ GemmProblem make_gemm(const DMat& a, const DMat& b, DMat& c, double alpha_re, do
 // uploads nothing (the entry point for callers that cannot allocate).
 void gemm_detached_complex(cudaStream_t stream, int device, int* d_err, const GemmProblem& p);
 // Split-precision products C := A B (beta 0) or C += A B (beta 1) from
-// `slices` 8-bit slices per operand on the tcgen05 tensor cores (ozaki.cu).
+// 8-bit residues modulo `moduli` coprime moduli on the tcgen05 tensor cores,
+// reconstructed by the Chinese remainder theorem (ozaki.cu).
 struct SplitProduct {
     const DMat* a;
     const DMat* b;
     DMat* c;
     double beta;
 };
-void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int slices);
+void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int moduli);
 // The thread's message for errors raised outside any context (tns_last_error(NULL)).
 void set_detached_error(const std::string& msg);
 

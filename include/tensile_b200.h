@@ -77,25 +77,29 @@ int tns_zgemm_device(tns_context* ctx, int m, int n, int k, const double* alpha,
 
 /* ---- split-precision form ------------------------------------------------ */
 
-/* C := A*B in the split-precision form: each operand is cut into `slices`
- * (4..8) signed 8-bit slices under power-of-two row (A) and column (B) scales,
- * the slice products run on the 8-bit tensor cores with exact 32-bit
- * accumulation and are recombined in FP64. With 8 slices the result agrees
- * with the FP64 product to about K * 2^-56 of the row and column scales; it
- * does not reproduce the reference's rounding. Complex operands keep four real
- * multiplications per complex multiply-add (never 3M). No counterpart in the
- * reference: this is the split-precision form of ComplexKernels.Multiply
+/* C := A*B in the split-precision form: the rows of A and the columns of B
+ * are scaled by powers of two and rounded to t-bit integers, their residues
+ * modulo `moduli` (8..22) pairwise coprime moduli <= 256 are multiplied on the
+ * 8-bit tensor cores with exact 32-bit accumulation, and the integer product
+ * is rebuilt by the Chinese remainder theorem in FP64 (t is the largest with
+ * 2 K 2^(2t) below the product of the moduli: 71 for 20 moduli and K <= 2048,
+ * complex K counted twice). Each entry agrees with the exact product to about
+ * K 2^-t of its row and column scales; it does not reproduce the reference's
+ * rounding. Complex operands keep four real multiplications per complex
+ * multiply-add (never 3M). No counterpart in the reference: this is the
+ * split-precision form of ComplexKernels.Multiply
  * (src/Tensile/ComplexKernels.cs:49-108) and Gemm (src/Tensile.Kernels/Gemm.cs:117-203). */
 int tns_dgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
-                    double* c, int ldc, int slices);
+                    double* c, int ldc, int moduli);
 int tns_zgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
-                    double* c, int ldc, int slices);
+                    double* c, int ldc, int moduli);
 /* 0 (the default): every product of Expm in plain FP64, the reference's
- * rounding. 4..8: Expm's Pade-evaluation and squaring products in the
- * split-precision form with that many slices; A^2, A^4, A^6 and every norm
+ * rounding. 8..22: Expm's Pade-evaluation and squaring products in the
+ * split-precision form with that many moduli; A^2, A^4, A^6 and every norm
  * estimate that selects the degree and s stay in plain FP64, so the degree
- * and s remain the reference's. */
-int tns_set_split_slices(tns_context* ctx, int slices);
+ * and s remain the reference's, as do the LU and the solve of the Pade
+ * denominator. */
+int tns_set_split_moduli(tns_context* ctx, int moduli);
 
 /* ---- exact norms -------------------------------------------------------- */
 
