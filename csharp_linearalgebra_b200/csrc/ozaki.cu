@@ -17,11 +17,12 @@
 // the largest value with 2 K' 2^(2t) < P = prod(p), so A'B' is the unique
 // residue class representative in (-P/2, P/2).
 // Reconstruction. With u_q = (R_q y_q) mod p_q, y_q = (P/p_q)^-1 mod p_q,
-// A'B' / P = frac(sum_q u_q / p_q) (the representative in [-1/2, 1/2]); the
-// sum runs in double-double (1/p_q as a double-double, products by FMA, the
-// integer part dropped after every term), and A'B' = frac * P, then
-// C = A'B' 2^(e_i + f_j - 2t). The reconstruction's own error, below 2^-100 of
-// P, is far under the rounding of A' and B'.
+// A'B' / P = frac(sum_q u_q / p_q) (the representative in [-1/2, 1/2]). All
+// 1/p_q share one binary exponent, so with 1/p_q written as three aligned
+// 39-bit digits the sum is three exact FP64 integer sums; the fraction of the
+// leading one is exact, the trailing ones join in double-double, and
+// A'B' = frac * P, then C = A'B' 2^(e_i + f_j - 2t). The reconstruction's own
+// error, below 2^-110 of P, is far under the rounding of A' and B'.
 // Complex. With the real and imaginary parts sharing their exponents, the
 // complex product is the single real product
 //     [Ar Ai] * [[Br, Bi], [-Bi, Br]]   (columns of the right factor interleaved,
@@ -83,9 +84,12 @@ struct CrtParams {
     int t;                        // integer bits of the scaled operands
     int p[kMaxModuli];            // moduli
     int y[kMaxModuli];            // (P / p)^-1 mod p
-    int pow36[kMaxModuli];        // 2^36 mod p
-    double inv_hi[kMaxModuli];    // 1/p as a double-double
-    double inv_lo[kMaxModuli];
+    double pow48[kMaxModuli];     // 2^48 mod p
+    double inv[kMaxModuli];       // 1/p rounded (the residues' quotients)
+    // 1/p = d1 2^-47 + d2 2^-86 + d3 2^-125 (+ under 2^-125), each digit an
+    // integer below 2^40: every 1/p lies in [2^-8, 2^-7), so the digits of all
+    // moduli are aligned and sum_q u_q d_q stays an exact FP64 integer.
+    double d1[kMaxModuli], d2[kMaxModuli], d3[kMaxModuli];
     double P_hi, P_lo;            // P = prod p as a double-double
 };
 
@@ -107,7 +111,24 @@ __global__ void row_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.rows) return;
     double m = 0.0;
-    for (int k = 0; k < d.cols; ++k) {
+    // Eight columns' loads in flight per step; the maximum is order-free.
+    int k = 0;
+    for (; k + 8 <= d.cols; k += 8) {
+        if (CPLX) {
+            double2 z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = reinterpret_cast<const double2*>(d.a)[(size_t)(k + u) * d.ld + i];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) m = fmax(m, fmax(fabs(z[u].x), fabs(z[u].y)));
+        } else {
+            double z[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) z[u] = d.a[(size_t)(k + u) * d.ld + i];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) m = fmax(m, fabs(z[u]));
+        }
+    }
+    for (; k < d.cols; ++k) {
         if (CPLX) {
             const double2 z = reinterpret_cast<const double2*>(d.a)[(size_t)k * d.ld + i];
             m = fmax(m, fmax(fabs(z.x), fabs(z.y)));
@@ -140,34 +161,41 @@ __global__ void col_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
 
 // ---- residues ----------------------------------------------------------------------
 
-// x = rint(v 2^shift), an integer-valued double with |x| <= 2^t (t <= 96); its
-// split x = h 2^36 + l into 64-bit integers (same sign, |l| < 2^36).
-__device__ __forceinline__ void to_integer(double v, int shift, long long& h, long long& l) {
+// x = rint(v 2^shift), an integer-valued double with |x| <= 2^t (t <= 96),
+// split exactly as x = xh 2^48 + xl with |xh|, |xl| < 2^48.
+__device__ __forceinline__ void to_integer(double v, int shift, double& xh, double& xl) {
     const double x = rint(scalbn(v, shift));
-    const double hd = trunc(scalbn(x, -36));
-    h = (long long)hd;
-    l = (long long)(x - scalbn(hd, 36));
+    xh = trunc(scalbn(x, -48));
+    xl = x - scalbn(xh, 48);
 }
 
-// The symmetric residue of h 2^36 + l modulo p: in [-p/2, p - 1 - p/2].
-__device__ __forceinline__ int residue(long long h, long long l, int p, int pow36) {
-    int r = (int)(((h % p) * pow36 + l % p) % p);
-    const int half = p >> 1;
-    if (r > p - 1 - half) r -= p;
-    if (r < -half) r += p;
-    return r;
+// x - p rint(x / p) for an integer-valued |x| < 2^48 + 2^15: exact (the
+// quotient's rounding is decided correctly -- the product x * (1/p) is off by
+// under 2^-11, x/p is at least 1/(2p) > 2^-9 from a tie for odd p, and for
+// p = 256 either neighbour of a tie is a valid residue).
+__device__ __forceinline__ double reduce(double x, double p, double inv) { return fma(-rint(x * inv), p, x); }
+
+// The symmetric residue of xh 2^48 + xl modulo p, as a signed byte
+// (in [-p/2, p/2], +128 stored as its equivalent -128 for p = 256):
+// (xh mod p) (2^48 mod p) + xl is an exact integer below 2^48 + 2^15.
+__device__ __forceinline__ int8_t residue(double xh, double xl, double p, double inv, double pow48) {
+    int r = (int)reduce(fma(reduce(xh, p, inv), pow48, xl), p, inv);
+    if (r > 127) r -= 256;
+    return (int8_t)r;
 }
 
 struct ResDesc {
     const double* src;  // A (rows x k) or B (k x cols), column-major, ld elements
     int ld, m, k;       // logical rows (A) or columns (B); depth
+    int kh;             // complex: offset of the imaginary half in a residue row (k rounded up to 16)
     int rows_p, kp;     // padded residue extents: rows of a plane, bytes per row
     const int* e;       // exponents of the rows (A) or columns (B)
     int8_t* dst;        // nm x rows_p x kp
 };
 
-// A' planes: row i holds [Re A(i,:), Im A(i,:)] (real: A(i,:)); 16 bytes of
-// one row per thread, every modulus.
+// A' planes: row i holds [Re A(i,:), 0.., Im A(i,:), 0..] with the imaginary
+// half at kh (real: A(i,:)), zeros to kp; 16 bytes of one row per thread,
+// every modulus.
 template <bool CPLX>
 __global__ void residue_a_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.z);
@@ -175,67 +203,90 @@ __global__ void residue_a_kernel(const __grid_constant__ Batch<ResDesc> b, const
     const int c0 = blockIdx.y * 16;
     if (i >= d.rows_p || c0 >= d.kp) return;
     const int shift = cp.t - (i < d.m ? d.e[i] : 0);
-    long long h[16], l[16];
+    const bool imag = CPLX && c0 >= d.kh;
+    const int k0 = imag ? c0 - d.kh : c0;
+    double xh[16], xl[16];
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
-        const int kk = c0 + u;
+        const int k = k0 + u;
         double v = 0.0;
-        if (i < d.m) {
-            if (CPLX) {
-                if (kk < d.k) v = d.src[((size_t)kk * d.ld + i) * 2];
-                else if (kk < 2 * d.k) v = d.src[((size_t)(kk - d.k) * d.ld + i) * 2 + 1];
-            } else if (kk < d.k) {
-                v = d.src[(size_t)kk * d.ld + i];
-            }
-        }
-        to_integer(v, shift, h[u], l[u]);
+        if (i < d.m && k < d.k && (!CPLX || c0 < 2 * d.kh))
+            v = CPLX ? d.src[((size_t)k * d.ld + i) * 2 + (imag ? 1 : 0)] : d.src[(size_t)k * d.ld + i];
+        to_integer(v, shift, xh[u], xl[u]);
     }
     for (int q = 0; q < cp.nm; ++q) {
+        const double p = cp.p[q], inv = cp.inv[q], pw = cp.pow48[q];
         alignas(16) int8_t out[16];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) out[u] = (int8_t)residue(h[u], l[u], cp.p[q], cp.pow36[q]);
+        for (int u = 0; u < 16; ++u) out[u] = residue(xh[u], xl[u], p, inv, pw);
         *reinterpret_cast<int4*>(d.dst + ((size_t)q * d.rows_p + i) * d.kp + c0) = *reinterpret_cast<int4*>(out);
     }
 }
 
-// B' planes: row n of the right factor, K-major. Complex: row 2j =
-// [Re B(:,j); -Im B(:,j)], row 2j+1 = [Im B(:,j); Re B(:,j)]; real: row j =
-// B(:,j). 16 bytes of one row per thread, every modulus.
+// B' planes, K-major rows of the right factor. Complex: row 2j =
+// [Re B(:,j); -Im B(:,j)], row 2j+1 = [Im B(:,j); Re B(:,j)] (halves at 0 and
+// kh); real: row j = B(:,j); zeros to kp. One thread per 16 entries of one
+// column of B: it writes both rows of the column, both halves, every modulus
+// (residues of -x are the negated residues of x). Threads past the last
+// chunk write the zero tail [2 kh, kp) of both rows.
 template <bool CPLX>
 __global__ void residue_b_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.y);
-    const int chunks = d.kp / 16;
+    constexpr int DPE = CPLX ? 2 : 1;
+    const int width = CPLX ? 2 * d.kh : d.kp;         // bytes of a row the data chunks cover
+    const int chunks = (CPLX ? d.kh : d.kp) / 16 + (CPLX ? (d.kp - width) / 16 : 0);
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)chunks * d.rows_p) return;
-    const int n = (int)(idx / chunks), c0 = (int)(idx % chunks) * 16;
-    const int j = CPLX ? n / 2 : n;
+    const int jrows = d.rows_p / DPE;
+    if (idx >= (long long)chunks * jrows) return;
+    const int j = (int)(idx / chunks), c = (int)(idx % chunks);
     const bool live = j < d.m;
     const int shift = cp.t - (live ? d.e[j] : 0);
-    long long h[16], l[16];
+    int8_t* row0 = d.dst + (size_t)(DPE * j) * d.kp;
+    const size_t plane = (size_t)d.rows_p * d.kp;
+    if (CPLX && c >= d.kh / 16) {  // zero tail of both rows
+        const int c0 = width + (c - d.kh / 16) * 16;
+        for (int q = 0; q < cp.nm; ++q) {
+            *reinterpret_cast<int4*>(row0 + q * plane + c0) = make_int4(0, 0, 0, 0);
+            *reinterpret_cast<int4*>(row0 + q * plane + d.kp + c0) = make_int4(0, 0, 0, 0);
+        }
+        return;
+    }
+    const int k0 = c * 16;
+    double rh[16], rl[16], ih[16], il[16];
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
-        const int kk = c0 + u;
-        double v = 0.0;
-        if (live) {
+        const int k = k0 + u;
+        double re = 0.0, im = 0.0;
+        if (live && k < d.k) {
             if (CPLX) {
-                const bool top = kk < d.k;
-                const int k = top ? kk : kk - d.k;
-                if (kk < 2 * d.k) {
-                    const double2 z = reinterpret_cast<const double2*>(d.src)[(size_t)j * d.ld + k];
-                    // even rows: (Re; -Im), odd rows: (Im; Re)
-                    v = (n & 1) ? (top ? z.y : z.x) : (top ? z.x : -z.y);
-                }
-            } else if (kk < d.k) {
-                v = d.src[(size_t)j * d.ld + kk];
+                const double2 z = reinterpret_cast<const double2*>(d.src)[(size_t)j * d.ld + k];
+                re = z.x;
+                im = z.y;
+            } else {
+                re = d.src[(size_t)j * d.ld + k];
             }
         }
-        to_integer(v, shift, h[u], l[u]);
+        to_integer(re, shift, rh[u], rl[u]);
+        if (CPLX) to_integer(im, shift, ih[u], il[u]);
     }
     for (int q = 0; q < cp.nm; ++q) {
-        alignas(16) int8_t out[16];
+        const double p = cp.p[q], inv = cp.inv[q], pw = cp.pow48[q];
+        alignas(16) int8_t rr[16], ri[16], nri[16];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) out[u] = (int8_t)residue(h[u], l[u], cp.p[q], cp.pow36[q]);
-        *reinterpret_cast<int4*>(d.dst + ((size_t)q * d.rows_p + n) * d.kp + c0) = *reinterpret_cast<int4*>(out);
+        for (int u = 0; u < 16; ++u) {
+            rr[u] = residue(rh[u], rl[u], p, inv, pw);
+            if (CPLX) {
+                ri[u] = residue(ih[u], il[u], p, inv, pw);
+                nri[u] = ri[u] == -128 ? (int8_t)-128 : (int8_t)-ri[u];  // -(-128) = 128 = -128 (mod 256)
+            }
+        }
+        int8_t* r = row0 + q * plane;
+        *reinterpret_cast<int4*>(r + k0) = *reinterpret_cast<int4*>(rr);
+        if (CPLX) {
+            *reinterpret_cast<int4*>(r + d.kh + k0) = *reinterpret_cast<int4*>(nri);
+            *reinterpret_cast<int4*>(r + d.kp + k0) = *reinterpret_cast<int4*>(ri);
+            *reinterpret_cast<int4*>(r + d.kp + d.kh + k0) = *reinterpret_cast<int4*>(rr);
+        }
     }
 }
 
@@ -418,47 +469,48 @@ struct CrtDesc {
     int accumulate;     // 0: C = AB, 1: C += AB
 };
 
-// A'B' / P = frac(sum_q u_q / p_q) in double-double, then A'B' = frac * P.
-__device__ __forceinline__ double reconstruct(const uint8_t* us, int stride, const CrtParams& cp) {
-    double fh = 0.0, fl = 0.0;
-    for (int q = 0; q < cp.nm; ++q) {
-        const double u = (double)us[q * stride];
-        const double ph = u * cp.inv_hi[q];
-        const double pl = fma(u, cp.inv_hi[q], -ph) + u * cp.inv_lo[q];
-        // (fh, fl) += (ph, pl), then drop the integer part
-        const double s = fh + ph;
-        const double bb = s - fh;
-        const double e = (fh - (s - bb)) + (ph - bb) + fl + pl;
-        fh = s + e;
-        fl = e - (fh - s);
-        const double k = rint(fh);
-        fh -= k;
-        const double s2 = fh + fl;
-        fl = fl - (s2 - fh);
-        fh = s2;
-    }
+// A'B' / P = frac(sum_q u_q / p_q), then A'B' = frac * P. The sum is three
+// exact FP64 integer sums over the aligned digits of 1/p_q; the fraction is
+// taken of the leading one (exactly) and the two trailing ones are added in
+// double-double.
+__device__ __forceinline__ double from_digit_sums(double s1, double s2, double s3, const CrtParams& cp) {
+    const double f1 = scalbn(s1 - scalbn(rint(scalbn(s1, -47)), 47), -47);  // in [-1/2, 1/2]
+    const double f2 = scalbn(s2, -86), f3 = scalbn(s3, -125);
+    const double fh = f1 + f2;
+    const double bb = fh - f1;
+    const double fl = (f1 - (fh - bb)) + (f2 - bb) + f3;
     const double r = fh * cp.P_hi;
     return r + (fma(fh, cp.P_hi, -r) + fh * cp.P_lo + fl * cp.P_hi);
 }
 
 // One CTA per 32 x 32 output tile: the tile's residue bytes of every modulus
-// in shared memory (rows of the planes read contiguously), then warp w
-// computes output columns w, w + 8, ..., one row per lane (column-major stores
-// of 32 consecutive rows).
+// staged in shared memory (16-byte loads of plane rows; rows padded to an odd
+// number of words so that the 32 lanes, one row each, read distinct banks),
+// then warp w computes output columns w, w + 8, ..., one row per lane
+// (column-major stores of 32 consecutive rows). A complex entry's Re and Im
+// bytes are adjacent and read together.
 template <bool CPLX>
 __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<CrtDesc> b,
                                                   const __grid_constant__ CrtParams cp) {
     const CrtDesc& d = batch_item(b, blockIdx.z);
     constexpr int DPE = CPLX ? 2 : 1;
-    constexpr int TW = 32 * DPE;  // plane columns per tile
-    __shared__ uint8_t su[kMaxModuli][32][TW];
+    constexpr int TW = 32 * DPE;   // plane bytes per tile row
+    constexpr int PITCH = TW + 4;  // odd number of 4-byte words
+    __shared__ __align__(16) uint8_t su[kMaxModuli][32][PITCH];
     const int r0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
     if (r0 >= d.m || j0 >= d.n) return;
     const int nm = cp.nm;
-    for (int e = threadIdx.x; e < nm * 32 * TW; e += blockDim.x) {
-        const int q = e / (32 * TW), rr = (e / TW) % 32, cc = e % TW;
-        const int row = r0 + rr, col = j0 * DPE + cc;
-        su[q][rr][cc] = (row < d.mp && col < d.np) ? d.u[((size_t)q * d.mp + row) * d.np + col] : 0;
+    // Whole 16-byte pieces are in bounds: mp is a multiple of 128 and
+    // np >= DPE * round_up(n, 32).
+    constexpr int V = TW / 16;
+    for (int e = threadIdx.x; e < nm * 32 * V; e += blockDim.x) {
+        const int q = e / (32 * V), rr = (e / V) % 32, cv = e % V;
+        const int4 w = *reinterpret_cast<const int4*>(d.u + ((size_t)q * d.mp + r0 + rr) * d.np + j0 * DPE + cv * 16);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&su[q][rr][cv * 16]);
+        dst[0] = (uint32_t)w.x;
+        dst[1] = (uint32_t)w.y;
+        dst[2] = (uint32_t)w.z;
+        dst[3] = (uint32_t)w.w;
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -469,9 +521,28 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<
         const int j = j0 + jj;
         if (j >= d.n) break;
         const int sc = ei + d.eb[j] - 2 * cp.t;
-        const double re = scalbn(reconstruct(&su[0][lane][jj * DPE], 32 * TW, cp), sc);
+        double a1 = 0.0, a2 = 0.0, a3 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+        for (int q = 0; q < nm; ++q) {
+            double ur, ui = 0.0;
+            if (CPLX) {
+                const uint16_t v = *reinterpret_cast<const uint16_t*>(&su[q][lane][2 * jj]);
+                ur = (double)(v & 0xFF);
+                ui = (double)(v >> 8);
+            } else {
+                ur = (double)su[q][lane][jj];
+            }
+            a1 = fma(ur, cp.d1[q], a1);
+            a2 = fma(ur, cp.d2[q], a2);
+            a3 = fma(ur, cp.d3[q], a3);
+            if (CPLX) {
+                b1 = fma(ui, cp.d1[q], b1);
+                b2 = fma(ui, cp.d2[q], b2);
+                b3 = fma(ui, cp.d3[q], b3);
+            }
+        }
+        const double re = scalbn(from_digit_sums(a1, a2, a3, cp), sc);
         if (CPLX) {
-            const double im = scalbn(reconstruct(&su[0][lane][jj * DPE + 1], 32 * TW, cp), sc);
+            const double im = scalbn(from_digit_sums(b1, b2, b3, cp), sc);
             double2* p = reinterpret_cast<double2*>(d.c) + (size_t)j * d.ldc + i;
             double2 r = make_double2(re, im);
             if (d.accumulate) {
@@ -543,10 +614,15 @@ CrtParams crt_params(int nm, int kmax) {
             if (r != q) mq = (int)((long long)mq * (kModuli[r] % p) % p);
         cp.y[q] = inverse_mod(mq, p);
         long long pw = 1;
-        for (int s = 0; s < 36; ++s) pw = pw * 2 % p;
-        cp.pow36[q] = (int)pw;
-        cp.inv_hi[q] = 1.0 / p;
-        cp.inv_lo[q] = std::fma(-cp.inv_hi[q], (double)p, 1.0) / p;
+        for (int s = 0; s < 48; ++s) pw = pw * 2 % p;
+        cp.pow48[q] = (double)pw;
+        cp.inv[q] = 1.0 / p;
+        const unsigned long long d1 = (1ULL << 47) / p, r1 = (1ULL << 47) - d1 * p;
+        const unsigned long long d2 = (r1 << 39) / p, r2 = (r1 << 39) - d2 * p;
+        const unsigned long long d3 = (r2 << 39) / p;
+        cp.d1[q] = (double)d1;
+        cp.d2[q] = (double)d2;
+        cp.d3[q] = (double)d3;
         const double h = ph * p;
         const double l = std::fma(ph, (double)p, -h) + pl * p;
         ph = h + l;
@@ -569,7 +645,7 @@ template <bool CPLX>
 void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
     constexpr int DPE = CPLX ? 2 : 1;
     struct Sizes {
-        int m, n, k, mp, np, kp;
+        int m, n, k, kh, mp, np, kp;
         size_t a_off, b_off, u_off, ea_off, eb_off;
     };
     std::vector<Sizes> z;
@@ -587,7 +663,9 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         s.n = p.b->cols;
         s.mp = round_up(s.m, kTile);
         s.np = round_up(DPE * s.n, kTile);
-        s.kp = round_up(DPE * s.k, kKb);
+        // complex rows: the real half, zeros to kh, the imaginary half at kh
+        s.kh = CPLX ? round_up(s.k, 16) : s.k;
+        s.kp = round_up(CPLX ? 2 * s.kh : s.k, kKb);
         // Exact 32-bit sums of residue products (|r| <= 128).
         if ((double)s.kp * 128.0 * 128.0 >= 2147483647.0)
             fail(TNS_E_ARGUMENT, "split-precision product too deep for exact 32-bit accumulation");
@@ -621,8 +699,8 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         uint8_t* u8 = reinterpret_cast<uint8_t*>(at(s.u_off));
         rows.push_back(ExpDesc{p.a->p, p.a->ld(), s.m, s.k, ea});
         cols.push_back(ExpDesc{p.b->p, p.b->ld(), s.k, s.n, eb});
-        ra.push_back(ResDesc{p.a->p, p.a->ld(), s.m, s.k, s.mp, s.kp, ea, a8});
-        rb.push_back(ResDesc{p.b->p, p.b->ld(), s.n, s.k, s.np, s.kp, eb, b8});
+        ra.push_back(ResDesc{p.a->p, p.a->ld(), s.m, s.k, s.kh, s.mp, s.kp, ea, a8});
+        rb.push_back(ResDesc{p.b->p, p.b->ld(), s.n, s.k, s.kh, s.np, s.kp, eb, b8});
         md.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles, u8});
         cd.push_back(CrtDesc{u8, s.mp, s.np, s.m, s.n, ea, eb, p.c->p, p.c->ld(), p.beta != 0.0 ? 1 : 0});
         tiles += (s.mp / kTile) * (s.np / kTile);
@@ -632,7 +710,10 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
         max_chunks = std::max(max_chunks, s.kp / 16);
-        max_b_threads = std::max(max_b_threads, (long long)(s.kp / 16) * s.np);
+        // residue_b: one thread per 16 entries of a column of B (both rows of
+        // the column) plus the zero-tail chunks
+        const long long bchunks = CPLX ? s.kh / 16 + (s.kp - 2 * s.kh) / 16 : s.kp / 16;
+        max_b_threads = std::max(max_b_threads, bchunks * (s.np / DPE));
         max_out_rows = std::max(max_out_rows, s.m);
         max_out_cols = std::max(max_out_cols, s.n);
     }
