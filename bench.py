@@ -12,12 +12,19 @@ Multi-GPU (torchrun, one process per GPU): every rank runs its own sweep
 (weak scaling, independent matrices, no collective on the data path); the
 time is the max over ranks.
 
-`value` has the inputs resident in HBM (device entry point); `e2e` goes
-through the host-buffer entry point with pinned buffers, so every step copies
-each matrix in and each exponential out. The roofline figure is the DMMA GEMM
-kernel's algorithmic FLOP rate (CUDA events on the library's stream) against
-cuBLAS DGEMM measured in the same process. `--impl reference` times the CPU
-restatement of the reference's algorithm (the oracle) on the host cores.
+Two forms run on the same sweep. The split-precision form (`value`, `e2e`,
+`roofline`) computes the Pade-evaluation and squaring products from 8-bit
+residues modulo `--moduli` coprime moduli on the tcgen05 tensor cores; its
+error against the plain form is reported per matrix next to the matrix's
+own FP64 sensitivity floor (`split_accuracy`). The plain FP64 form
+(`plain_fp64`), every product on the FP64 DMMA path, is bit-identical to the
+reference. `value` has the inputs resident in HBM (device entry point); `e2e`
+goes through the host-buffer entry point with pinned buffers, so every step
+copies each matrix in and each exponential out. Rooflines: the split form's
+8-bit product kernel against cuBLASLt int8 measured in the same process, the
+plain form's DMMA GEMM against cuBLAS DGEMM (CUDA events on the library's
+stream). `--impl reference` times the CPU restatement of the reference's
+algorithm (the oracle) on the host cores.
 """
 from __future__ import annotations
 
@@ -289,22 +296,31 @@ def ours(args, world, rank, local, dist):
         ws.set_timing(False)
         st = ws.stats()
         ws.set_workers(args.groups)
-        e2e_ms = None
-        if not args.no_e2e:
-            barrier()
-            torch.cuda.synchronize()
-            e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e2.record(stream)
-            for _ in range(args.steps):
-                ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
-            e3.record(stream)
-            torch.cuda.synchronize()
-            e2e_ms = max_over_ranks(e2.elapsed_time(e3) / args.steps)
         return {"ms": ms, "st_step": st_step, "st": st, "clocks": clocks.summary(), "diags": diags,
-                "e2e_ms": e2e_ms, "outs": outs}
+                "e2e_ms": None, "outs": outs}
 
-    plain = run_form(0, dev_in)
+    def run_e2e(moduli):
+        """K end-to-end steps through the host-buffer entry point."""
+        ws.set_split_moduli(moduli)
+        ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)  # warm-up
+        barrier()
+        torch.cuda.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            ws.expm_batched_host(count, orders, hi_ptrs, orders, ho_ptrs, orders)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e2.elapsed_time(e3) / args.steps)
+
+    # Both forms' device-resident runs first (split, then plain), then both
+    # end-to-end runs, so that no host-buffer pass reshapes the memory pool
+    # between a form's warm-up and its timed steps.
     split = run_form(args.moduli, dev_in)
+    plain = run_form(0, dev_in)
+    if not args.no_e2e:
+        split["e2e_ms"] = run_e2e(args.moduli)
+        plain["e2e_ms"] = run_e2e(0)
     assert [(d.degree, d.squarings) for d in plain["diags"]] == [(d.degree, d.squarings) for d in split["diags"]]
 
     # Accuracy of the split form against the plain FP64 form (bit-identical to

@@ -70,11 +70,13 @@ Context::~Context() {
     workers.clear();
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
-    for (auto& pr : gemm_events) {
-        cudaEventDestroy(pr.first);
-        cudaEventDestroy(pr.second);
-    }
+    for (auto* evs : {&gemm_events, &split_events})
+        for (auto& pr : *evs) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
     for (auto e : event_pool) cudaEventDestroy(e);
+    if (split_scratch) cudaFree(split_scratch);
     if (h_ring) cudaFreeHost(h_ring);
     if (d_ring) cudaFree(d_ring);
     if (d_err) cudaFree(d_err);
@@ -149,6 +151,18 @@ DMat::~DMat() {
 }
 
 void DMat::zero() { TNS_CUDA(cudaMemsetAsync(p, 0, bytes(), ctx->stream)); }
+
+void* Context::scratch(size_t bytes) {
+    if (bytes > split_scratch_bytes) {
+        if (split_scratch) TNS_CUDA(cudaFreeAsync(split_scratch, stream));
+        split_scratch = nullptr;
+        split_scratch_bytes = 0;
+        const size_t grown = std::max(bytes, bytes + bytes / 4);  // headroom for the next, larger batch
+        TNS_CUDA(cudaMallocAsync(&split_scratch, grown, stream));
+        split_scratch_bytes = grown;
+    }
+    return split_scratch;
+}
 
 DBuf::DBuf(Context& c, size_t b) : ctx(&c), bytes(b) {
     TNS_CUDA(cudaMallocAsync(&p, std::max<size_t>(b, 16), c.stream));

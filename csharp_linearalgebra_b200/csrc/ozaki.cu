@@ -678,8 +678,8 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         z.push_back(s);
     }
     const CrtParams cp = crt_params(nm, kmax);
-    DBuf scratch(ctx, total);
-    auto at = [&](size_t off) { return static_cast<char*>(scratch.p) + off; };
+    char* scratch = static_cast<char*>(ctx.scratch(total));
+    auto at = [&](size_t off) { return scratch + off; };
 
     std::vector<ExpDesc> rows, cols;
     std::vector<ResDesc> ra, rb;

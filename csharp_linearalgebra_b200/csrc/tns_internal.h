@@ -96,6 +96,13 @@ struct Context {
     long long split_launches = 0;
     double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;
+    // The split product's residue planes (gigabytes for a batch) live in one
+    // grow-only buffer reused in stream order, instead of passing through the
+    // stream-ordered pool at every launch, where four streams' churn of such
+    // blocks can force fresh mappings.
+    void* split_scratch = nullptr;
+    size_t split_scratch_bytes = 0;
+    void* scratch(size_t bytes);
     cudaEvent_t take_event();
     void drain_events();        // sums finished event pairs into gemm_ms_done / split_ms_done
 
