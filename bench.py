@@ -143,6 +143,18 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def max_over_ranks_of(dist, value, device):
+    """The largest of every rank's `value` (a step time): the slowest rank
+    bounds a weak-scaling step. `dist` is torch.distributed or None (one rank);
+    the tensor lives on `device` (CUDA for NCCL, CPU for gloo)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def reference_arm(args, world, rank):
     """The reference's algorithm on the host cores (the oracle restatement)."""
     if rank != 0:
@@ -253,11 +265,7 @@ def ours(args, world, rank, local, dist):
             dist.barrier()
 
     def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(dist, ms, "cuda")
 
     def run_form(moduli, inputs):
         """Warm-up, K timed steps (inputs in HBM), one single-group sweep timed
