@@ -173,13 +173,22 @@ __device__ __forceinline__ void to_integer(double v, int shift, double& xh, doub
 // quotient's rounding is decided correctly -- the product x * (1/p) is off by
 // under 2^-11, x/p is at least 1/(2p) > 2^-9 from a tie for odd p, and for
 // p = 256 either neighbour of a tie is a valid residue).
-__device__ __forceinline__ double reduce(double x, double p, double inv) { return fma(-rint(x * inv), p, x); }
+// The quotient is rounded to the nearest integer by adding and subtracting
+// 1.5 2^52 (exact for |x/p| < 2^51; ties to even, as rint), which keeps the
+// reduction on the FP64 arithmetic pipe.
+constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
+__device__ __forceinline__ double reduce(double x, double p, double inv) {
+    const double q = (x * inv + kRoundMagic) - kRoundMagic;
+    return fma(-q, p, x);
+}
+// An integer-valued |r| < 2^31 as an int: the low word of r + 1.5 2^52.
+__device__ __forceinline__ int small_int(double r) { return __double2loint(r + kRoundMagic); }
 
 // The symmetric residue of xh 2^48 + xl modulo p, as a signed byte
 // (in [-p/2, p/2], +128 stored as its equivalent -128 for p = 256):
 // (xh mod p) (2^48 mod p) + xl is an exact integer below 2^48 + 2^15.
 __device__ __forceinline__ int8_t residue(double xh, double xl, double p, double inv, double pow48) {
-    int r = (int)reduce(fma(reduce(xh, p, inv), pow48, xl), p, inv);
+    int r = small_int(reduce(fma(reduce(xh, p, inv), pow48, xl), p, inv));
     if (r > 127) r -= 256;
     return (int8_t)r;
 }
@@ -419,7 +428,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             const bool got = mbar_wait_bounded(&accf[buf], (q >> 1) & 1, err, kErrSplitAcc);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after_sync();
-            const int p = cp.p[q], y = cp.y[q];
+            // u = (R y) mod p by one exact FP64 reduction: |R y| < 2^31 2^8, so
+            // R y and its quotient's rounding are exact (as in reduce()).
+            const double p = cp.p[q], y = cp.y[q], inv = cp.inv[q];
             uint8_t* plane = D.u + ((size_t)q * D.mp + m0 + row) * D.np + n0;
             for (int c0 = 0; c0 < kTile; c0 += 16) {
                 uint32_t v[16];
@@ -428,9 +439,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
                 alignas(16) uint8_t out[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
-                    int r = ((int)v[e] % p) * y % p;
-                    if (r < 0) r += p;
-                    out[e] = (uint8_t)r;
+                    double r = reduce((double)(int)v[e] * y, p, inv);  // in [-p/2, p/2]
+                    if (r < 0.0) r += p;
+                    out[e] = (uint8_t)small_int(r);
                 }
                 *reinterpret_cast<int4*>(plane + c0) = *reinterpret_cast<int4*>(out);
             }
