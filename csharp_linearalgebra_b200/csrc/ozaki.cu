@@ -30,10 +30,11 @@
 // multiplications per complex multiply-add, as the 4M method (never 3M).
 //
 // Kernels. Residues: one thread per 16 bytes of a residue row, all moduli.
-// Product: one CTA per 128 x 128 output tile and all moduli: a TMA producer
-// warp streams 128 x 128-byte residue tiles (128-byte swizzle) through a
-// 4-stage mbarrier ring; one thread issues tcgen05.mma kind::i8 (M = N = 128,
-// K = 32) into one of two TMEM accumulators; four epilogue warps reduce each
+// Product: one CTA per 128 x 256 output tile and all moduli: a TMA producer
+// warp streams 128- and 256-row x 128-byte residue tiles (128-byte swizzle)
+// through a 4-stage mbarrier ring; one thread issues tcgen05.mma kind::i8
+// (M = 128, N = 256, K = 32) into one of two TMEM accumulators (all 512
+// columns); four epilogue warps reduce each
 // finished accumulator to u_q (tcgen05.ld) and store it as a byte plane while
 // the next modulus' MMAs run. Every wait is bounded; TMEM is released on
 // every path. Reconstruction: one CTA per 32 x 32 output tile, all planes
@@ -68,13 +69,17 @@ constexpr int kMaxModuli = 22;
 constexpr int kModuli[kMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223,
                                      217, 211, 199, 197, 193, 191, 181, 179, 173, 167, 163};
 
-constexpr int kTile = 128;       // output tile rows and columns; residue tile rows
+constexpr int kTile = 128;       // output tile rows (the MMA's M); rows of an A residue tile
+// Output tile columns (the MMA's N, the rows of a B residue tile): 256 when a
+// launch's tiles fill the GPU (each A tile then feeds twice the columns),
+// else 128.
 constexpr int kKb = 128;         // bytes (8-bit elements) of K per stage
 constexpr int kStages = 4;
-constexpr uint32_t kStageBytes = 2u * kTile * kKb;  // A and B tiles, 16 KB each
+template <int TN>
+__host__ __device__ constexpr uint32_t stage_bytes() { return (uint32_t)(kTile + TN) * kKb; }  // A and B tiles
 constexpr int kSplitThreads = 192;                  // producer, MMA, 4 epilogue warps
-constexpr uint32_t kTmemCols = 256;                 // two 128-column accumulators
-constexpr int kSplitSmem = kStages * (int)kStageBytes + 1024 + 256;
+template <int TN>
+constexpr int split_smem() { return kStages * (int)stage_bytes<TN>() + 1024 + 256; }
 
 enum : int { kErrSplitFull = 11, kErrSplitEmpty = 12, kErrSplitAcc = 13, kErrSplitDrain = 14 };
 
@@ -309,15 +314,18 @@ struct ModDesc {
     uint8_t* u;              // nm planes of mp x np bytes, row-major: u_q of each product entry
 };
 struct ModMaps {
-    CUtensorMap a, b;  // residues as (kp bytes) x (rows) x nm, boxes of 128 x 128 x 1, 128-byte swizzle
+    CUtensorMap a, b;  // residues as (kp bytes) x (rows) x nm; boxes of 128 bytes x 128 (A) or 256 (B) rows, 128-byte swizzle
 };
 
+template <int TN>
 __global__ void __launch_bounds__(kSplitThreads, 1)
     modular_gemm_kernel(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps, int nprob,
                         const __grid_constant__ CrtParams cp, int* err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    constexpr uint32_t kStageBytes = stage_bytes<TN>();
+    constexpr uint32_t kTmemCols = 2 * TN;  // two accumulators (power of two >= 32)
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
     uint64_t* empty = full + kStages;
     uint64_t* accf = empty + kStages;   // accumulator b is complete (MMA -> epilogue)
@@ -336,7 +344,7 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     const ModDesc& D = descs[lo];
     const ModMaps& MP = maps[lo];
     const int local = blockIdx.x - D.tile_begin;
-    const int m0 = (local % D.tiles_m) * kTile, n0 = (local / D.tiles_m) * kTile;
+    const int m0 = (local % D.tiles_m) * kTile, n0 = (local / D.tiles_m) * TN;
     const int nkb = D.kp / kKb;
     const int nm = cp.nm;
 
@@ -387,14 +395,14 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr uint32_t idesc = i8_instr_desc(kTile, kTile);
+            constexpr uint32_t idesc = i8_instr_desc(kTile, TN);
             uint32_t it = 0;
             bool ok = true;
             for (int q = 0; q < nm && ok; ++q) {
                 const int buf = q & 1;
                 if (!mbar_wait_bounded(&acce[buf], ((q >> 1) & 1) ^ 1, err, kErrSplitAcc)) break;
                 tc_fence_after_sync();
-                const uint32_t dacc = tmem + buf * kTile;
+                const uint32_t dacc = tmem + buf * TN;
                 for (int kb = 0; kb < nkb; ++kb) {
                     const int st = it % kStages;
                     if (!mbar_wait_bounded(&full[st], (it / kStages) & 1, err, kErrSplitFull)) {
@@ -432,9 +440,9 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             // R y and its quotient's rounding are exact (as in reduce()).
             const double p = cp.p[q], y = cp.y[q], inv = cp.inv[q];
             uint8_t* plane = D.u + ((size_t)q * D.mp + m0 + row) * D.np + n0;
-            for (int c0 = 0; c0 < kTile; c0 += 16) {
+            for (int c0 = 0; c0 < TN; c0 += 16) {
                 uint32_t v[16];
-                tmem_ld16(tmem + lane_addr + buf * kTile + c0, v);
+                tmem_ld16(tmem + lane_addr + buf * TN + c0, v);
                 tmem_wait_ld();
                 alignas(16) uint8_t out[16];
 #pragma unroll
@@ -584,11 +592,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // The residues of one operand as a 3-D byte array (kp x rows_p x nm), boxes of
-// 128 x 128 x 1 with 128-byte swizzle.
-void encode_residues(CUtensorMap* map, const int8_t* base, int kp, int rows_p, int nm) {
+// 128 bytes x box_rows x 1 with 128-byte swizzle.
+void encode_residues(CUtensorMap* map, const int8_t* base, int kp, int rows_p, int nm, int box_rows) {
     cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows_p, (cuuint64_t)nm};
     cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)kp * rows_p};
-    cuuint32_t box[3] = {(cuuint32_t)kKb, (cuuint32_t)kTile, 1};
+    cuuint32_t box[3] = {(cuuint32_t)kKb, (cuuint32_t)box_rows, 1};
     cuuint32_t elem[3] = {1, 1, 1};
     CUresult r = tensor_map_encoder()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims, strides,
                                       box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -666,6 +674,10 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         total += (bytes + 255) & ~size_t(255);
         return off;
     };
+    // 256-column tiles when they fill the GPU.
+    long long tiles_wide = 0;
+    for (auto& p : v) tiles_wide += (long long)((p.a->rows + kTile - 1) / kTile) * ((DPE * p.b->cols + 255) / 256);
+    const int tn = tiles_wide >= ctx.num_sms ? 256 : 128;
     int kmax = 1;
     for (auto& p : v) {
         Sizes s{};
@@ -673,7 +685,7 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         s.k = p.a->cols;
         s.n = p.b->cols;
         s.mp = round_up(s.m, kTile);
-        s.np = round_up(DPE * s.n, kTile);
+        s.np = round_up(DPE * s.n, tn);
         // complex rows: the real half, zeros to kh, the imaginary half at kh
         s.kh = CPLX ? round_up(s.k, 16) : s.k;
         s.kp = round_up(CPLX ? 2 * s.kh : s.k, kKb);
@@ -714,9 +726,9 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         rb.push_back(ResDesc{p.b->p, p.b->ld(), s.n, s.k, s.kh, s.np, s.kp, eb, b8});
         md.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles, u8});
         cd.push_back(CrtDesc{u8, s.mp, s.np, s.m, s.n, ea, eb, p.c->p, p.c->ld(), p.beta != 0.0 ? 1 : 0});
-        tiles += (s.mp / kTile) * (s.np / kTile);
-        encode_residues(&maps[q].a, a8, s.kp, s.mp, nm);
-        encode_residues(&maps[q].b, b8, s.kp, s.np, nm);
+        tiles += (s.mp / kTile) * (s.np / tn);
+        encode_residues(&maps[q].a, a8, s.kp, s.mp, nm, kTile);
+        encode_residues(&maps[q].b, b8, s.kp, s.np, nm, tn);
         max_m = std::max(max_m, s.m);
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
@@ -745,11 +757,6 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches += 4;
     }
-    static bool configured[64] = {};
-    if (!configured[ctx.device]) {
-        TNS_CUDA(cudaFuncSetAttribute(modular_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSplitSmem));
-        configured[ctx.device] = true;
-    }
     const ModDesc* d_desc = static_cast<const ModDesc*>(ctx.upload(md.data(), sizeof(ModDesc) * md.size()));
     const ModMaps* d_maps = static_cast<const ModMaps*>(ctx.upload(maps.data(), sizeof(ModMaps) * maps.size()));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -758,9 +765,17 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         e1 = ctx.take_event();
         TNS_CUDA(cudaEventRecord(e0, ctx.stream));
     }
-    modular_gemm_kernel<<<tiles, kSplitThreads, kSplitSmem, ctx.stream>>>(d_desc, d_maps, (int)md.size(), cp,
-                                                                           ctx.d_err);
-    TNS_CUDA(cudaGetLastError());
+    auto launch = [&](auto kernel, int smem_bytes, bool& configured) {
+        if (!configured) {
+            TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+            configured = true;
+        }
+        kernel<<<tiles, kSplitThreads, smem_bytes, ctx.stream>>>(d_desc, d_maps, (int)md.size(), cp, ctx.d_err);
+        TNS_CUDA(cudaGetLastError());
+    };
+    static bool configured_wide[64] = {}, configured_narrow[64] = {};
+    if (tn == 256) launch(modular_gemm_kernel<256>, split_smem<256>(), configured_wide[ctx.device]);
+    else launch(modular_gemm_kernel<128>, split_smem<128>(), configured_narrow[ctx.device]);
     if (ctx.timing) {
         TNS_CUDA(cudaEventRecord(e1, ctx.stream));
         ctx.split_events.emplace_back(e0, e1);
