@@ -412,7 +412,9 @@ def ours(args, world, rank, local, dist):
                          "timing": "CUDA events around every split-product launch of one extra sweep run as a "
                                    "single group; int8 operations counted on the padded residue extents",
                          "split_launches_per_sweep": int(sst["split_launches"]),
-                         "split_int8_pops_per_sweep": sst["split_int8_ops"] / 1e15},
+                         "split_int8_pops_per_sweep": sst["split_int8_ops"] / 1e15,
+                         "algorithmic_bytes_per_launch": sst["split_bytes"] / sst["split_launches"]
+                         if sst["split_launches"] else None},
             "split_accuracy": {
                 "vs": "plain FP64 GPU form (bit-identical to the reference's CPU result)",
                 "rel_err_1norm_max": max(errs), "rel_err_1norm_median": statistics.median(errs),

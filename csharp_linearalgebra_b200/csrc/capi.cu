@@ -407,6 +407,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
     out->split_flops = ctx.split_flops;
     out->split_int8_ops = ctx.split_int8_ops;
     out->split_ms = ctx.split_ms_done;
+    out->split_bytes = ctx.split_bytes;
     for (auto& w : ctx.workers) {
         w->drain_events();
         out->kernel_launches += w->kernel_launches;
@@ -418,6 +419,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
         out->split_flops += w->split_flops;
         out->split_int8_ops += w->split_int8_ops;
         out->split_ms += w->split_ms_done;
+        out->split_bytes += w->split_bytes;
     }
 }
 
@@ -426,13 +428,13 @@ void reset_stats(Context& ctx) {
     ctx.kernel_launches = ctx.gemm_launches = 0;
     ctx.gemm_flops = ctx.gemm_ms_done = ctx.gemm_bytes = 0.0;
     ctx.split_launches = 0;
-    ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = 0.0;
+    ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = ctx.split_bytes = 0.0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
         w->gemm_flops = w->gemm_ms_done = w->gemm_bytes = 0.0;
         w->split_launches = 0;
-        w->split_flops = w->split_int8_ops = w->split_ms_done = 0.0;
+        w->split_flops = w->split_int8_ops = w->split_ms_done = w->split_bytes = 0.0;
     }
 }
 

@@ -89,8 +89,11 @@ struct CrtParams {
     int t;                        // integer bits of the scaled operands
     int p[kMaxModuli];            // moduli
     int y[kMaxModuli];            // (P / p)^-1 mod p
-    double pow48[kMaxModuli];     // 2^48 mod p
-    double inv[kMaxModuli];       // 1/p rounded (the residues' quotients)
+    // The product epilogue's constants: with R = h 2^16 + l, u = (h w16 + l w0) mod p,
+    // w0 = y mod p and w16 = 2^16 y mod p (symmetric), l w0 formed from l + 2^23
+    // as fma(l + 2^23, w0, -2^23 w0).
+    float w0[kMaxModuli], w16[kMaxModuli], w0_off[kMaxModuli];
+    float inv[kMaxModuli];        // 1/p rounded to FP32
     // 1/p = d1 2^-47 + d2 2^-86 + d3 2^-125 (+ under 2^-125), each digit an
     // integer below 2^40: every 1/p lies in [2^-8, 2^-7), so the digits of all
     // moduli are aligned and sum_q u_q d_q stays an exact FP64 integer.
@@ -166,37 +169,139 @@ __global__ void col_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
 
 // ---- residues ----------------------------------------------------------------------
 
-// x = rint(v 2^shift), an integer-valued double with |x| <= 2^t (t <= 96),
-// split exactly as x = xh 2^48 + xl with |xh|, |xl| < 2^48.
-__device__ __forceinline__ void to_integer(double v, int shift, double& xh, double& xl) {
-    const double x = rint(scalbn(v, shift));
-    xh = trunc(scalbn(x, -48));
-    xl = x - scalbn(xh, 48);
-}
-
-// x - p rint(x / p) for an integer-valued |x| < 2^48 + 2^15: exact (the
-// quotient's rounding is decided correctly -- the product x * (1/p) is off by
-// under 2^-11, x/p is at least 1/(2p) > 2^-9 from a tie for odd p, and for
-// p = 256 either neighbour of a tie is a valid residue).
-// The quotient is rounded to the nearest integer by adding and subtracting
-// 1.5 2^52 (exact for |x/p| < 2^51; ties to even, as rint), which keeps the
-// reduction on the FP64 arithmetic pipe.
+// Digits. y = v 2^shift (|y| < 2^t) is written as rint(y) = sum_{i<ND} c_i 2^(14 i)
+// with symmetric digits |c_i| <= 2^13, taken from the top in FP64: c_i is
+// rint(x 2^-14i) (adding 1.5 2^52 rounds to an integer and leaves it in the low
+// word), then x -= c_i 2^14i, which is exact (x keeps at most 53 significant
+// bits: it is a multiple of y's last bit and below 2^(14i - 1)). The last digit
+// rounds what is left, so the digits sum to rint(y) exactly. ND = 6 covers
+// t <= 83, ND = 7 covers t <= 97.
+//
+// Residues. For each modulus, s = sum_i c_i w_i with w_i the symmetric residue
+// of 2^(14 i) mod p (|w_i| <= 128) is an exact FP32 integer (|s| <= 2^13 +
+// (ND - 1) 2^20 < 0.8 2^23), congruent to rint(y) mod p. Then r = s - p rint(s/p)
+// with the quotient taken as s * fl(1/p) rounded to an integer by adding
+// 1.5 2^23: the product is off s/p by under |s| 2^-24 / p < 0.4 / p, and for odd
+// p the quotient s/p is at least 1/(2p) from a tie, so the rounding is the
+// exact one and r lies in [-(p-1)/2, (p-1)/2] (p = 256: 1/p is exact and r in
+// [-128, 128], 128 and -128 being the same byte). r + 1.5 2^23 holds r in the
+// low byte of its bit pattern. Two entries go through each FP32 instruction
+// (the f32x2 forms); the reduction never touches the FP64 pipe.
+constexpr int kDigitBits = 14;
+constexpr int kMaxDigits = 7;
 constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
-__device__ __forceinline__ double reduce(double x, double p, double inv) {
-    const double q = (x * inv + kRoundMagic) - kRoundMagic;
-    return fma(-q, p, x);
-}
-// An integer-valued |r| < 2^31 as an int: the low word of r + 1.5 2^52.
-__device__ __forceinline__ int small_int(double r) { return __double2loint(r + kRoundMagic); }
+constexpr float kRoundMagicF = 12582912.0f;          // 1.5 * 2^23
+constexpr int kRoundMagicBits = 0x4B400000;          // bit pattern of 1.5 * 2^23
 
-// The symmetric residue of xh 2^48 + xl modulo p, as a signed byte
-// (in [-p/2, p/2], +128 stored as its equivalent -128 for p = 256):
-// (xh mod p) (2^48 mod p) + xl is an exact integer below 2^48 + 2^15.
-__device__ __forceinline__ int8_t residue(double xh, double xl, double p, double inv, double pow48) {
-    int r = small_int(reduce(fma(reduce(xh, p, inv), pow48, xl), p, inv));
-    if (r > 127) r -= 256;
-    return (int8_t)r;
+__host__ __device__ constexpr double pow2_const(int k) {
+    double r = 1.0;
+    for (; k > 0; --k) r *= 2.0;
+    for (; k < 0; ++k) r *= 0.5;
+    return r;
 }
+
+int digits_for(int t) { return t <= kDigitBits * 5 + kDigitBits - 1 ? 6 : 7; }
+
+struct ResidueTable {
+    float2 w[kMaxModuli][kMaxDigits];  // {w, w}: symmetric residue of 2^(14 i) mod p
+    float2 inv[kMaxModuli];            // {1/p, 1/p} rounded to FP32
+    float2 negp[kMaxModuli];           // {-p, -p}
+};
+
+constexpr ResidueTable make_residue_table() {
+    ResidueTable t{};
+    for (int q = 0; q < kMaxModuli; ++q) {
+        const int p = kModuli[q];
+        long long r = 1 % p;
+        for (int i = 0; i < kMaxDigits; ++i) {
+            const long long s = 2 * r > p ? r - p : r;
+            t.w[q][i] = float2{(float)s, (float)s};
+            for (int b = 0; b < kDigitBits; ++b) r = r * 2 % p;
+        }
+        const float inv = (float)(1.0 / p);
+        t.inv[q] = float2{inv, inv};
+        t.negp[q] = float2{(float)-p, (float)-p};
+    }
+    return t;
+}
+__constant__ ResidueTable kResidueTable = make_residue_table();
+
+// 2^k as a double, |k| <= 1022.
+__device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// Digits of rint(v 2^shift) as FP32 bit patterns of 1.5 2^23 + c_i. The scale
+// goes in two exact power-of-two factors (shift can exceed the exponent range
+// of one double; a product that underflows belongs to an entry whose integer
+// image is 0 either way).
+template <int ND>
+__device__ __forceinline__ void digits_of(double v, double f1, double f2, float (&c)[ND]) {
+    double x = (v * f1) * f2;
+#pragma unroll
+    for (int i = ND - 1; i >= 1; --i) {
+        const double tm = fma(x, pow2_const(-kDigitBits * i), kRoundMagic);
+        c[i] = __int_as_float(__double2loint(tm) + kRoundMagicBits);
+        x = fma(-(tm - kRoundMagic), pow2_const(kDigitBits * i), x);
+    }
+    c[0] = __int_as_float(__double2loint(x + kRoundMagic) + kRoundMagicBits);
+}
+
+__device__ __forceinline__ uint32_t pack4(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3) {
+    return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+}
+// Byte-wise two's complement negation (no carries between bytes).
+__device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
+    const uint32_t n = ~w;
+    return ((n & 0x7f7f7f7fu) + 0x01010101u) ^ (n & 0x80808080u);
+}
+
+// Sixteen entries of one residue row: their digits (in pairs), then for each
+// modulus the residue bytes, handed to store(q, words).
+template <int ND>
+struct RowDigits {
+    float2 c[ND][8];
+
+    template <class Load>
+    __device__ __forceinline__ void take(Load load, int shift) {
+        const int h = shift >> 1;
+        const double f1 = pow2(h), f2 = pow2(shift - h);
+        const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            float d0[ND], d1[ND];
+            digits_of<ND>(load(2 * e), f1, f2, d0);
+            digits_of<ND>(load(2 * e + 1), f1, f2, d1);
+#pragma unroll
+            for (int i = 0; i < ND; ++i) c[i][e] = __fadd2_rn(make_float2(d0[i], d1[i]), neg_magic);
+        }
+    }
+
+    template <class Store>
+    __device__ __forceinline__ void residues(int nm, Store store) const {
+        const float2 magic = make_float2(kRoundMagicF, kRoundMagicF);
+        const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
+#pragma unroll
+        for (int q = 0; q < kMaxModuli; ++q) {
+            if (q >= nm) break;
+            uint32_t b[16];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                float2 s = c[0][e];
+#pragma unroll
+                for (int i = 1; i < ND; ++i) s = __ffma2_rn(c[i][e], kResidueTable.w[q][i], s);
+                const float2 t = __fadd2_rn(__ffma2_rn(s, kResidueTable.inv[q], magic), neg_magic);
+                const float2 r = __fadd2_rn(__ffma2_rn(t, kResidueTable.negp[q], s), magic);
+                b[2 * e] = __float_as_uint(r.x);
+                b[2 * e + 1] = __float_as_uint(r.y);
+            }
+            uint4 words;
+            words.x = pack4(b[0], b[1], b[2], b[3]);
+            words.y = pack4(b[4], b[5], b[6], b[7]);
+            words.z = pack4(b[8], b[9], b[10], b[11]);
+            words.w = pack4(b[12], b[13], b[14], b[15]);
+            store(q, words);
+        }
+    }
+};
 
 struct ResDesc {
     const double* src;  // A (rows x k) or B (k x cols), column-major, ld elements
@@ -210,8 +315,9 @@ struct ResDesc {
 // A' planes: row i holds [Re A(i,:), 0.., Im A(i,:), 0..] with the imaginary
 // half at kh (real: A(i,:)), zeros to kp; 16 bytes of one row per thread,
 // every modulus.
-template <bool CPLX>
-__global__ void residue_a_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
+template <bool CPLX, int ND>
+__global__ void __launch_bounds__(128) residue_a_kernel(const __grid_constant__ Batch<ResDesc> b,
+                                                        const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.z);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int c0 = blockIdx.y * 16;
@@ -219,88 +325,73 @@ __global__ void residue_a_kernel(const __grid_constant__ Batch<ResDesc> b, const
     const int shift = cp.t - (i < d.m ? d.e[i] : 0);
     const bool imag = CPLX && c0 >= d.kh;
     const int k0 = imag ? c0 - d.kh : c0;
-    double xh[16], xl[16];
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int k = k0 + u;
-        double v = 0.0;
-        if (i < d.m && k < d.k && (!CPLX || c0 < 2 * d.kh))
-            v = CPLX ? d.src[((size_t)k * d.ld + i) * 2 + (imag ? 1 : 0)] : d.src[(size_t)k * d.ld + i];
-        to_integer(v, shift, xh[u], xl[u]);
-    }
-    for (int q = 0; q < cp.nm; ++q) {
-        const double p = cp.p[q], inv = cp.inv[q], pw = cp.pow48[q];
-        alignas(16) int8_t out[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) out[u] = residue(xh[u], xl[u], p, inv, pw);
-        *reinterpret_cast<int4*>(d.dst + ((size_t)q * d.rows_p + i) * d.kp + c0) = *reinterpret_cast<int4*>(out);
-    }
+    const bool rows_live = i < d.m && (!CPLX || c0 < 2 * d.kh);
+    RowDigits<ND> g;
+    g.take(
+        [&](int u) {
+            const int k = k0 + u;
+            if (!rows_live || k >= d.k) return 0.0;
+            return CPLX ? d.src[((size_t)k * d.ld + i) * 2 + (imag ? 1 : 0)] : d.src[(size_t)k * d.ld + i];
+        },
+        shift);
+    int8_t* row = d.dst + (size_t)i * d.kp + c0;
+    const size_t plane = (size_t)d.rows_p * d.kp;
+    g.residues(cp.nm, [&](int q, uint4 w) { *reinterpret_cast<uint4*>(row + q * plane) = w; });
 }
 
 // B' planes, K-major rows of the right factor. Complex: row 2j =
 // [Re B(:,j); -Im B(:,j)], row 2j+1 = [Im B(:,j); Re B(:,j)] (halves at 0 and
-// kh); real: row j = B(:,j); zeros to kp. One thread per 16 entries of one
-// column of B: it writes both rows of the column, both halves, every modulus
-// (residues of -x are the negated residues of x). Threads past the last
+// kh); real: row j = B(:,j); zeros to kp. One thread per 16 entries of one part
+// of one column: a real-part thread writes them to row 2j at 0 and to row 2j+1
+// at kh, an imaginary-part thread to row 2j+1 at 0 and, negated, to row 2j at
+// kh (the residues of -x are the negated residues of x). Threads past the last
 // chunk write the zero tail [2 kh, kp) of both rows.
-template <bool CPLX>
-__global__ void residue_b_kernel(const __grid_constant__ Batch<ResDesc> b, const __grid_constant__ CrtParams cp) {
+template <bool CPLX, int ND>
+__global__ void __launch_bounds__(128) residue_b_kernel(const __grid_constant__ Batch<ResDesc> b,
+                                                        const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.y);
     constexpr int DPE = CPLX ? 2 : 1;
-    const int width = CPLX ? 2 * d.kh : d.kp;         // bytes of a row the data chunks cover
-    const int chunks = (CPLX ? d.kh : d.kp) / 16 + (CPLX ? (d.kp - width) / 16 : 0);
+    const int half = (CPLX ? d.kh : d.kp) / 16;  // data chunks of one part
+    const int items = CPLX ? 2 * half + (d.kp - 2 * d.kh) / 16 : half;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int jrows = d.rows_p / DPE;
-    if (idx >= (long long)chunks * jrows) return;
-    const int j = (int)(idx / chunks), c = (int)(idx % chunks);
+    if (idx >= (long long)items * jrows) return;
+    const int j = (int)(idx / items), it = (int)(idx % items);
     const bool live = j < d.m;
-    const int shift = cp.t - (live ? d.e[j] : 0);
     int8_t* row0 = d.dst + (size_t)(DPE * j) * d.kp;
     const size_t plane = (size_t)d.rows_p * d.kp;
-    if (CPLX && c >= d.kh / 16) {  // zero tail of both rows
-        const int c0 = width + (c - d.kh / 16) * 16;
+    if (CPLX && it >= 2 * half) {  // zero tail of both rows
+        const int c0 = 2 * d.kh + (it - 2 * half) * 16;
         for (int q = 0; q < cp.nm; ++q) {
             *reinterpret_cast<int4*>(row0 + q * plane + c0) = make_int4(0, 0, 0, 0);
             *reinterpret_cast<int4*>(row0 + q * plane + d.kp + c0) = make_int4(0, 0, 0, 0);
         }
         return;
     }
-    const int k0 = c * 16;
-    double rh[16], rl[16], ih[16], il[16];
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-        const int k = k0 + u;
-        double re = 0.0, im = 0.0;
-        if (live && k < d.k) {
-            if (CPLX) {
-                const double2 z = reinterpret_cast<const double2*>(d.src)[(size_t)j * d.ld + k];
-                re = z.x;
-                im = z.y;
-            } else {
-                re = d.src[(size_t)j * d.ld + k];
-            }
-        }
-        to_integer(re, shift, rh[u], rl[u]);
-        if (CPLX) to_integer(im, shift, ih[u], il[u]);
-    }
-    for (int q = 0; q < cp.nm; ++q) {
-        const double p = cp.p[q], inv = cp.inv[q], pw = cp.pow48[q];
-        alignas(16) int8_t rr[16], ri[16], nri[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-            rr[u] = residue(rh[u], rl[u], p, inv, pw);
-            if (CPLX) {
-                ri[u] = residue(ih[u], il[u], p, inv, pw);
-                nri[u] = ri[u] == -128 ? (int8_t)-128 : (int8_t)-ri[u];  // -(-128) = 128 = -128 (mod 256)
-            }
-        }
-        int8_t* r = row0 + q * plane;
-        *reinterpret_cast<int4*>(r + k0) = *reinterpret_cast<int4*>(rr);
-        if (CPLX) {
-            *reinterpret_cast<int4*>(r + d.kh + k0) = *reinterpret_cast<int4*>(nri);
-            *reinterpret_cast<int4*>(r + d.kp + k0) = *reinterpret_cast<int4*>(ri);
-            *reinterpret_cast<int4*>(r + d.kp + d.kh + k0) = *reinterpret_cast<int4*>(rr);
-        }
+    const bool imag = CPLX && it >= half;
+    const int k0 = (imag ? it - half : it) * 16;
+    const int shift = cp.t - (live ? d.e[j] : 0);
+    RowDigits<ND> g;
+    g.take(
+        [&](int u) {
+            const int k = k0 + u;
+            if (!live || k >= d.k) return 0.0;
+            return CPLX ? d.src[((size_t)j * d.ld + k) * 2 + (imag ? 1 : 0)] : d.src[(size_t)j * d.ld + k];
+        },
+        shift);
+    if (!CPLX) {
+        g.residues(cp.nm, [&](int q, uint4 w) { *reinterpret_cast<uint4*>(row0 + q * plane + k0) = w; });
+    } else if (!imag) {
+        g.residues(cp.nm, [&](int q, uint4 w) {
+            *reinterpret_cast<uint4*>(row0 + q * plane + k0) = w;
+            *reinterpret_cast<uint4*>(row0 + q * plane + d.kp + d.kh + k0) = w;
+        });
+    } else {
+        g.residues(cp.nm, [&](int q, uint4 w) {
+            *reinterpret_cast<uint4*>(row0 + q * plane + d.kp + k0) = w;
+            const uint4 n = make_uint4(neg_bytes(w.x), neg_bytes(w.y), neg_bytes(w.z), neg_bytes(w.w));
+            *reinterpret_cast<uint4*>(row0 + q * plane + d.kh + k0) = n;
+        });
     }
 }
 
@@ -436,22 +527,46 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
             const bool got = mbar_wait_bounded(&accf[buf], (q >> 1) & 1, err, kErrSplitAcc);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after_sync();
-            // u = (R y) mod p by one exact FP64 reduction: |R y| < 2^31 2^8, so
-            // R y and its quotient's rounding are exact (as in reduce()).
-            const double p = cp.p[q], y = cp.y[q], inv = cp.inv[q];
+            // u = (R y) mod p in [0, p] (p meaning 0), in FP32, two entries per
+            // instruction. R = h 2^16 + l with h = R >> 16 (arithmetic) and
+            // l = R & 0xffff, both read into floats through their bit patterns
+            // (2^23 + l; 1.5 2^23 + h, less 1.5 2^23). s = h w16 + l w0 is an
+            // exact FP32 integer, |s| <= 2^15 128 + 2^16 128 = 1.5 2^23. The
+            // quotient floor(s/p) is s * fl(1/p) rounded down by adding 1.5 2^23
+            // in round-toward-minus-infinity: the product is off s/p by under
+            // 0.75/p, so it is the exact floor, or one less when p divides s
+            // (u = p then). u + 1.5 2^23 holds u in its low byte.
+            const float2 w0 = make_float2(cp.w0[q], cp.w0[q]), w16 = make_float2(cp.w16[q], cp.w16[q]);
+            const float2 w0_off = make_float2(cp.w0_off[q], cp.w0_off[q]);
+            const float2 inv = make_float2(cp.inv[q], cp.inv[q]);
+            const float2 negp = make_float2((float)-cp.p[q], (float)-cp.p[q]);
+            const float2 magic = make_float2(kRoundMagicF, kRoundMagicF);
+            const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
             uint8_t* plane = D.u + ((size_t)q * D.mp + m0 + row) * D.np + n0;
             for (int c0 = 0; c0 < TN; c0 += 16) {
                 uint32_t v[16];
                 tmem_ld16(tmem + lane_addr + buf * TN + c0, v);
                 tmem_wait_ld();
-                alignas(16) uint8_t out[16];
+                uint32_t bytes[16];
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    double r = reduce((double)(int)v[e] * y, p, inv);  // in [-p/2, p/2]
-                    if (r < 0.0) r += p;
-                    out[e] = (uint8_t)small_int(r);
+                for (int e = 0; e < 8; ++e) {
+                    const uint32_t x0 = v[2 * e], x1 = v[2 * e + 1];
+                    const float2 lm = make_float2(__uint_as_float((x0 & 0xffffu) | 0x4B000000u),
+                                                  __uint_as_float((x1 & 0xffffu) | 0x4B000000u));
+                    const float2 hm = make_float2(__int_as_float(((int)x0 >> 16) + kRoundMagicBits),
+                                                  __int_as_float(((int)x1 >> 16) + kRoundMagicBits));
+                    const float2 sv = __ffma2_rn(__fadd2_rn(hm, neg_magic), w16, __ffma2_rn(lm, w0, w0_off));
+                    const float2 t = __fadd2_rn(__ffma2_rd(sv, inv, magic), neg_magic);
+                    const float2 u = __fadd2_rn(__ffma2_rn(t, negp, sv), magic);
+                    bytes[2 * e] = __float_as_uint(u.x);
+                    bytes[2 * e + 1] = __float_as_uint(u.y);
                 }
-                *reinterpret_cast<int4*>(plane + c0) = *reinterpret_cast<int4*>(out);
+                uint4 words;
+                words.x = pack4(bytes[0], bytes[1], bytes[2], bytes[3]);
+                words.y = pack4(bytes[4], bytes[5], bytes[6], bytes[7]);
+                words.z = pack4(bytes[8], bytes[9], bytes[10], bytes[11]);
+                words.w = pack4(bytes[12], bytes[13], bytes[14], bytes[15]);
+                *reinterpret_cast<uint4*>(plane + c0) = words;
             }
             tc_fence_before_sync();
             __syncwarp();
@@ -632,10 +747,11 @@ CrtParams crt_params(int nm, int kmax) {
         for (int r = 0; r < nm; ++r)
             if (r != q) mq = (int)((long long)mq * (kModuli[r] % p) % p);
         cp.y[q] = inverse_mod(mq, p);
-        long long pw = 1;
-        for (int s = 0; s < 48; ++s) pw = pw * 2 % p;
-        cp.pow48[q] = (double)pw;
-        cp.inv[q] = 1.0 / p;
+        auto sym = [p](long long r) { return (float)(2 * r > p ? r - p : r); };
+        cp.w0[q] = sym(cp.y[q] % p);
+        cp.w16[q] = sym((long long)cp.y[q] * (65536 % p) % p);
+        cp.w0_off[q] = -8388608.0f * cp.w0[q];
+        cp.inv[q] = (float)(1.0 / p);
         const unsigned long long d1 = (1ULL << 47) / p, r1 = (1ULL << 47) - d1 * p;
         const unsigned long long d2 = (r1 << 39) / p, r2 = (r1 << 39) - d2 * p;
         const unsigned long long d3 = (r2 << 39) / p;
@@ -733,9 +849,9 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
         max_chunks = std::max(max_chunks, s.kp / 16);
-        // residue_b: one thread per 16 entries of a column of B (both rows of
-        // the column) plus the zero-tail chunks
-        const long long bchunks = CPLX ? s.kh / 16 + (s.kp - 2 * s.kh) / 16 : s.kp / 16;
+        // residue_b: one thread per 16 entries of one part of a column of B
+        // plus the zero-tail chunks
+        const long long bchunks = CPLX ? 2 * (s.kh / 16) + (s.kp - 2 * s.kh) / 16 : s.kp / 16;
         max_b_threads = std::max(max_b_threads, bchunks * (s.np / DPE));
         max_out_rows = std::max(max_out_rows, s.m);
         max_out_cols = std::max(max_out_cols, s.n);
@@ -749,11 +865,14 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         col_exponent_kernel<CPLX><<<dim3((max_cols + 7) / 8, bc.count), 256, 0, ctx.stream>>>(bc);
         TNS_CUDA(cudaGetLastError());
         Batch<ResDesc> bra = make_batch(ctx, ra);
-        residue_a_kernel<CPLX><<<dim3((max_rows_a + 127) / 128, max_chunks, bra.count), 128, 0, ctx.stream>>>(bra, cp);
+        const dim3 grid_a((max_rows_a + 127) / 128, max_chunks, bra.count);
+        if (digits_for(cp.t) == 6) residue_a_kernel<CPLX, 6><<<grid_a, 128, 0, ctx.stream>>>(bra, cp);
+        else residue_a_kernel<CPLX, 7><<<grid_a, 128, 0, ctx.stream>>>(bra, cp);
         TNS_CUDA(cudaGetLastError());
         Batch<ResDesc> brb = make_batch(ctx, rb);
-        residue_b_kernel<CPLX><<<dim3((unsigned)((max_b_threads + 127) / 128), brb.count), 128, 0, ctx.stream>>>(brb,
-                                                                                                                 cp);
+        const dim3 grid_b((unsigned)((max_b_threads + 127) / 128), brb.count);
+        if (digits_for(cp.t) == 6) residue_b_kernel<CPLX, 6><<<grid_b, 128, 0, ctx.stream>>>(brb, cp);
+        else residue_b_kernel<CPLX, 7><<<grid_b, 128, 0, ctx.stream>>>(brb, cp);
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches += 4;
     }
@@ -792,6 +911,7 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         const auto& s = z[q];
         ctx.split_int8_ops += 2.0 * s.mp * (double)s.np * s.kp * nm;
         ctx.split_flops += (CPLX ? 8.0 : 2.0) * (double)s.m * s.n * s.k;
+        ctx.split_bytes += (double)nm * ((double)s.mp * s.kp + (double)s.np * s.kp + (double)s.mp * s.np);
     }
 }
 

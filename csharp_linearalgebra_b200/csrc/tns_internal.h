@@ -94,7 +94,7 @@ struct Context {
     // FP64 GEMM's): FP64-equivalent algorithmic flops and 8-bit operations.
     int split_moduli = 0;       // 0: Pade and squaring products in plain FP64
     long long split_launches = 0;
-    double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0;
+    double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0, split_bytes = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;
     // The split product's residue planes (gigabytes for a batch) live in one
     // grow-only buffer reused in stream order, instead of passing through the

@@ -262,6 +262,10 @@ typedef struct {
     double split_flops;
     double split_int8_ops;
     double split_ms;
+    /* algorithmic bytes of the modular GEMM launches: every modulus' 8-bit
+     * residue images of A and B read once and its 8-bit result plane written
+     * once, at the padded extents */
+    double split_bytes;
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
