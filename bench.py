@@ -47,6 +47,10 @@ METRIC = "batched complex expm/s: split-prec vs plain FP64 GPU at ≤1e-12 rel e
 # DRAM bytes of the GEMM launches per algorithmic byte, from one ncu capture of every GEMM launch of
 # the 16-matrix sweep (profiles/gemm_dmma_complex_sweep16.md): 109.1 MB measured / 153.4 MB.
 GEMM_TRAFFIC_RATIO = 109.1 / 153.35
+# The same for the modular GEMM of the split form: every modular_gemm launch of the 16-matrix sweep
+# (110 launches) read and wrote 105.59 GB of DRAM against 101.09 GB of algorithmic bytes
+# (profiles/modular_gemm_sweep16.md).
+SPLIT_TRAFFIC_RATIO = 105.585 / 101.086
 WORKLOAD = ("frequency sweep of 256 complex128 matrices A_k = -(G + i w_k C), n_k ~ U{64..1024}, "
             "G ~ N(0,1)/sqrt(n), C = Q^T D Q (D log-uniform [1e-3,1]), w_k log-spaced 1e2..1e6; Expm of each")
 
@@ -408,7 +412,12 @@ def ours(args, world, rank, local, dist):
                          "peak_source": peak8_src,
                          "fp64_equivalent_tflops": sst["split_flops"] / (sst["split_ms"] * 1e-3) / 1e12
                          if sst["split_ms"] > 0 else None,
-                         "traffic": None,
+                         "traffic": (SPLIT_TRAFFIC_RATIO * sst["split_bytes"] / sst["split_launches"])
+                         if sst["split_launches"] else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every modular_gemm "
+                                           "launch of the 16-matrix sweep = 1.044 x its algorithmic bytes "
+                                           "(profiles/modular_gemm_sweep16.md), scaled to this sweep's algorithmic "
+                                           "bytes per launch",
                          "timing": "CUDA events around every split-product launch of one extra sweep run as a "
                                    "single group; int8 operations counted on the padded residue extents",
                          "split_launches_per_sweep": int(sst["split_launches"]),
