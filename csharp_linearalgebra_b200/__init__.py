@@ -348,6 +348,51 @@ class Workspace:
             diagnostics.applications, diagnostics.early_exits = info.applications, info.early_exits
         return out[:, 0] if vec else out
 
+    # -- differentiation ------------------------------------------------------
+    def expm_frechet(self, a, e, diagnostics: ExpmDiagnostics | None = None):
+        """(exp(A), L(A, E)): the exponential and its Frechet derivative in the
+        direction E (Al-Mohy and Higham's algorithm; no reference counterpart,
+        which obtains L(A, E) from Expm of [[A, E], [0, A]])."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(e)
+        a, e = _fortran(a, cplx), _fortran(e, cplx)
+        if a.ndim != 2 or a.shape[0] != a.shape[1] or e.shape != a.shape:
+            raise ValueError(f"A and E must be square and of one shape, got {a.shape} and {e.shape}.")
+        n = a.shape[0]
+        x = np.zeros((n, n), dtype=a.dtype, order="F")
+        l = np.zeros((n, n), dtype=a.dtype, order="F")
+        info = N.ExpmInfo()
+        self._call("tns_zexpm_frechet" if cplx else "tns_dexpm_frechet", n, _p(a), _ld(a), _p(e), _ld(e),
+                   _p(x), _ld(x), _p(l), _ld(l), C.byref(info))
+        if diagnostics is not None:
+            diagnostics.degree, diagnostics.squarings = info.degree, info.squarings
+        return x, l
+
+    def expmv_gradient(self, a, b, y, t: float = 1.0):
+        """loss = ||exp(tA) B - Y||_F^2 and its gradients with respect to A, B
+        and t (complex gradients hold d/dRe + i d/dIm). Returns a dict with
+        loss, f = exp(tA) B, grad_a, grad_b, grad_t, degree, squarings."""
+        cplx = any(np.iscomplexobj(v) for v in (a, b, y))
+        a, b, y = _fortran(a, cplx), _fortran(b, cplx), _fortran(y, cplx)
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise ValueError(f"A must be square, got {a.shape}.")
+        if b.ndim != 2 or b.shape[0] != a.shape[0] or y.shape != b.shape:
+            raise ValueError(f"B and Y must be {a.shape[0]} x c and of one shape, got {b.shape} and {y.shape}.")
+        n, c = b.shape
+        ga = np.zeros((n, n), dtype=a.dtype, order="F")
+        gb = np.zeros((n, c), dtype=a.dtype, order="F")
+        f = np.zeros((n, c), dtype=a.dtype, order="F")
+        loss, gt = C.c_double(), C.c_double()
+        info = N.ExpmInfo()
+        self._call("tns_zexpmv_gradient" if cplx else "tns_dexpmv_gradient", n, c, float(t), _p(a), _ld(a),
+                   _p(b), _ld(b), _p(y), _ld(y), C.byref(loss), _p(ga), _ld(ga), _p(gb), _ld(gb), C.byref(gt),
+                   _p(f), _ld(f), C.byref(info))
+        return {"loss": loss.value, "f": f, "grad_a": ga, "grad_b": gb, "grad_t": gt.value,
+                "degree": info.degree, "squarings": info.squarings}
+
+    def set_checkpoint_bytes(self, nbytes: int):
+        """Device bytes the Frechet derivative may hold for its squarings (-1: automatic)."""
+        self._call("tns_set_checkpoint_bytes", int(nbytes))
+
 
 class LuDecomposition:
     """LuDecomposition<T> (src/Tensile/LuDecomposition.cs): packed factors,

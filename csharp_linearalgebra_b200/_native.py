@@ -79,6 +79,13 @@ SIGNATURES = {
     "tns_zexpm_batched_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "tns_dexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_dexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_zexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_dexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
+                                 C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_zexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
+                                 C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
+    "tns_set_checkpoint_bytes": (_I, [_P, _LL]),
     "tns_zgemm_device_noalloc": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
     "tns_set_workers": (_I, [_P, _I]),
     "tns_get_stats": (_I, [_P, C.POINTER(Stats)]),

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libtensile_b200.so")
 OBJ = os.path.join(HERE, "_build")
 
 SOURCES = ["context.cu", "gemm.cu", "blas1.cu", "lu.cu", "algos.cu", "expm_batched.cu", "capi.cu", "noalloc.cu",
-           "ozaki.cu"]
+           "ozaki.cu", "frechet.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -288,6 +288,70 @@ int expmv_entry(tns_context* c, bool cplx, int n, const double* a, int lda, int 
     });
 }
 
+int frechet_entry(tns_context* c, bool cplx, int n, const double* a, int lda, const double* e, int lde, double* expa,
+                  int ldx, double* l, int ldl, tns_expm_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(e, n, n, lde, "E");
+        check_operand(l, n, n, ldl, "L");
+        if (expa) check_operand(expa, n, n, ldx, "exp(A)");
+        tns_expm_info local{};
+        tns_expm_info* inf = info ? info : &local;
+        *inf = tns_expm_info{0, 0};
+        if (n == 0) return;
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the matrix to exponentiate");
+        DMat E = upload(ctx, e, n, n, lde, cplx, false, "the direction");
+        DMat X, L;
+        tns::ExpmInfo ei;
+        tns::expm_frechet(ctx, A, E, expa ? &X : nullptr, L, &ei);
+        tns::copy_out(ctx, L, l, ldl, false);
+        if (expa) tns::copy_out(ctx, X, expa, ldx, false);
+        ctx.sync();
+        inf->degree = ei.degree;
+        inf->squarings = ei.squarings;
+    });
+}
+
+int gradient_entry(tns_context* c, bool cplx, int n, int nc, double t, const double* a, int lda, const double* b,
+                   int ldb, const double* y, int ldy, double* loss, double* ga, int ldga, double* gb, int ldgb,
+                   double* gt, double* f, int ldf, tns_expm_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(b, n, nc, ldb, "B");
+        check_operand(y, n, nc, ldy, "Y");
+        check_operand(ga, n, n, ldga, "dloss/dA");
+        check_operand(gb, n, nc, ldgb, "dloss/dB");
+        if (f) check_operand(f, n, nc, ldf, "exp(tA) B");
+        require(loss != nullptr && gt != nullptr, TNS_E_NULL, "loss or grad_t is null");
+        require(std::isfinite(t), TNS_E_OUT_OF_RANGE, "t must be finite");
+        tns_expm_info local{};
+        tns_expm_info* inf = info ? info : &local;
+        *inf = tns_expm_info{0, 0};
+        *loss = 0.0;
+        *gt = 0.0;
+        if (n == 0 || nc == 0) {
+            // No entries: zero gradients (an empty B contributes nothing).
+            for (int j = 0; j < (nc == 0 ? n : 0); ++j)
+                for (int i = 0; i < n; ++i)
+                    for (int q = 0; q < (cplx ? 2 : 1); ++q) ga[((size_t)j * ldga + i) * (cplx ? 2 : 1) + q] = 0.0;
+            return;
+        }
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the operator");
+        DMat B = upload(ctx, b, n, nc, ldb, cplx, false, "the panel");
+        DMat Y = upload(ctx, y, n, nc, ldy, cplx, false, "the target");
+        DMat F, GA, GB;
+        tns::GradientResult r = tns::expmv_gradient(ctx, A, B, Y, t, f ? &F : nullptr, GA, GB);
+        tns::copy_out(ctx, GA, ga, ldga, false);
+        tns::copy_out(ctx, GB, gb, ldgb, false);
+        if (f) tns::copy_out(ctx, F, f, ldf, false);
+        ctx.sync();
+        *loss = r.loss;
+        *gt = r.grad_t;
+        inf->degree = r.info.degree;
+        inf->squarings = r.info.squarings;
+    });
+}
+
 int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
                         double* const* out, const int* ldo, tns_expm_info* infos) {
     return guarded(c, [&](Context& ctx) {
@@ -568,6 +632,32 @@ int tns_zexpm_batched(tns_context* c, int count, const int* orders, const double
 int tns_zexpm_batched_device(tns_context* c, int count, const int* orders, const double* const* a, const int* lda,
                              double* const* out, const int* ldo, tns_expm_info* infos) {
     return zexpm_batched_entry(c, true, count, orders, a, lda, out, ldo, infos);
+}
+int tns_dexpm_frechet(tns_context* c, int n, const double* a, int lda, const double* e, int lde, double* expa,
+                      int ldx, double* l, int ldl, tns_expm_info* info) {
+    return frechet_entry(c, false, n, a, lda, e, lde, expa, ldx, l, ldl, info);
+}
+int tns_zexpm_frechet(tns_context* c, int n, const double* a, int lda, const double* e, int lde, double* expa,
+                      int ldx, double* l, int ldl, tns_expm_info* info) {
+    return frechet_entry(c, true, n, a, lda, e, lde, expa, ldx, l, ldl, info);
+}
+int tns_dexpmv_gradient(tns_context* c, int n, int ncols, double t, const double* a, int lda, const double* b,
+                        int ldb, const double* y, int ldy, double* loss, double* grad_a, int ldga, double* grad_b,
+                        int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info) {
+    return gradient_entry(c, false, n, ncols, t, a, lda, b, ldb, y, ldy, loss, grad_a, ldga, grad_b, ldgb, grad_t, f,
+                          ldf, info);
+}
+int tns_zexpmv_gradient(tns_context* c, int n, int ncols, double t, const double* a, int lda, const double* b,
+                        int ldb, const double* y, int ldy, double* loss, double* grad_a, int ldga, double* grad_b,
+                        int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info) {
+    return gradient_entry(c, true, n, ncols, t, a, lda, b, ldb, y, ldy, loss, grad_a, ldga, grad_b, ldgb, grad_t, f,
+                          ldf, info);
+}
+int tns_set_checkpoint_bytes(tns_context* c, long long bytes) {
+    return guarded(c, [&](Context& ctx) {
+        require(bytes >= -1, TNS_E_OUT_OF_RANGE, "checkpoint bytes must be -1 (automatic) or a byte count");
+        ctx.checkpoint_bytes = bytes;
+    });
 }
 int tns_get_stats(tns_context* c, tns_stats* out) {
     return guarded(c, [&](Context& ctx) {

@@ -15,6 +15,7 @@
 // matrix is a batch of one.
 
 #include "estimator.h"
+#include "pade.h"
 #include "tns_internal.h"
 
 #include <algorithm>
@@ -28,22 +29,14 @@ namespace tns {
 
 namespace {
 
-// Constants, src/Tensile/MatrixExponential.cs:50-110, 441-449.
+// Constants, src/Tensile/MatrixExponential.cs:50-110, 441-449 (the Pade
+// coefficients are in pade.h).
 const double kTheta3 = 1.495585217958292e-2;
 const double kTheta5 = 2.539398330063230e-1;
 const double kTheta7 = 9.504178996162932e-1;
 const double kTheta9 = 2.097847961257068e0;
 const double kScalingThreshold = 4.25;
 const double kUnitRoundoff = 1.1102230246251565e-16;
-const double kPade3[] = {120, 60, 12, 1};
-const double kPade5[] = {30240, 15120, 3360, 420, 30, 1};
-const double kPade7[] = {17297280, 8648640, 1995840, 277200, 25200, 1512, 56, 1};
-const double kPade9[] = {17643225600.0, 8821612800.0, 2075673600.0, 302702400.0, 30270240.0,
-                         2162160.0,     110880.0,     3960.0,       90.0,        1.0};
-const double kPade13[] = {64764752532480000.0, 32382376266240000.0, 7771770303897600.0, 1187353796428800.0,
-                          129060195264000.0,   10559470521600.0,    670442572800.0,     33522128640.0,
-                          1323241920.0,        40840800.0,          960960.0,           16380.0,
-                          182.0,               1.0};
 const int kSeed = 20260915;
 
 double abs_coeff_reciprocal(int m) {

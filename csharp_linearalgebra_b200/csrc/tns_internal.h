@@ -93,6 +93,10 @@ struct Context {
     // The split-precision product's launches (counted and timed apart from the
     // FP64 GEMM's): FP64-equivalent algorithmic flops and 8-bit operations.
     int split_moduli = 0;       // 0: Pade and squaring products in plain FP64
+    // Device bytes the Frechet derivative may spend on keeping every squaring
+    // of its forward pass (else it keeps X_0 and squares again); -1: a quarter
+    // of the free device memory.
+    long long checkpoint_bytes = -1;
     long long split_launches = 0;
     double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0, split_bytes = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;
@@ -304,5 +308,18 @@ struct ExpmvInfo {
     int degree = 0, scaling = 0, applications = 0, early_exits = 0;
 };
 void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info);
+
+// ---- Frechet derivative and adjoint (frechet.cu) -----------------------------
+// exp(a) and, for a direction e, L(a, e) = d/dh exp(a + h e) at h = 0.
+void expm_frechet(Context& ctx, const DMat& a, const DMat& e, DMat* expa, DMat& l, ExpmInfo* info);
+// For F = exp(t a) b and loss = ||F - y||_F^2: the loss, F, and the gradients
+// dloss/da (n x n), dloss/db (n x c) and dloss/dt (complex: the gradients of a
+// real function with respect to Re and Im, as one complex matrix).
+struct GradientResult {
+    double loss = 0.0, grad_t = 0.0;
+    ExpmInfo info;
+};
+GradientResult expmv_gradient(Context& ctx, const DMat& a, const DMat& b, const DMat& y, double t, DMat* f,
+                              DMat& grad_a, DMat& grad_b);
 
 }  // namespace tns

@@ -213,6 +213,45 @@ int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, con
 int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
                double t, double* out, int ldo, tns_expmv_info* info);
 
+/* ---- differentiation: Frechet derivative and adjoint ---------------------- */
+
+/* exp(A) and its Frechet derivative L(A, E) = d/dh exp(A + hE) at h = 0, both
+ * n x n. No counterpart in the reference: Tensile obtains L(A, E) only as the
+ * upper right block of its Expm of the 2n x 2n matrix [[A, E], [0, A]]
+ * (MatrixExponential.ScalingAndSquaring, src/Tensile/MatrixExponential.cs:181-270);
+ * this computes the same quantity at about three times the cost of one Expm
+ * (Al-Mohy and Higham 2009, Algorithm 6.4). expa may be NULL (then ldx is not
+ * read). info (may be NULL) receives the Pade degree and the squarings of that
+ * algorithm, not the reference's Expm decisions. TNS_E_ARGUMENT for a
+ * non-finite A. */
+int tns_dexpm_frechet(tns_context* ctx, int n, const double* a, int lda, const double* e, int lde, double* expa,
+                      int ldx, double* l, int ldl, tns_expm_info* info);
+int tns_zexpm_frechet(tns_context* ctx, int n, const double* a, int lda, const double* e, int lde, double* expa,
+                      int ldx, double* l, int ldl, tns_expm_info* info);
+
+/* The gradient of loss = ||exp(tA) B - Y||_F^2 (A n x n, B and Y n x ncols):
+ * loss, and dloss/dA (n x n), dloss/dB (n x ncols), dloss/dt, with
+ * dloss = Re <grad, d.> and <X, Y> = trace(X^H Y), so that a complex gradient
+ * holds the derivatives with respect to the real and imaginary parts. f (may
+ * be NULL) receives exp(tA) B. No counterpart in the reference: it is the
+ * adjoint of MatrixExponentialAction.Expmv
+ * (src/Tensile/MatrixExponentialAction.cs:113-142), computed from one forward
+ * pass of the Frechet algorithm on t A^H and one derivative pass in the
+ * direction G B^H, G = 2 (exp(tA) B - Y). */
+int tns_dexpmv_gradient(tns_context* ctx, int n, int ncols, double t, const double* a, int lda, const double* b,
+                        int ldb, const double* y, int ldy, double* loss, double* grad_a, int ldga, double* grad_b,
+                        int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info);
+int tns_zexpmv_gradient(tns_context* ctx, int n, int ncols, double t, const double* a, int lda, const double* b,
+                        int ldb, const double* y, int ldy, double* loss, double* grad_a, int ldga, double* grad_b,
+                        int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info);
+
+/* Device bytes the Frechet derivative may hold for the squarings of its
+ * forward pass. Within the budget every squaring is kept for the derivative
+ * pass; beyond it only the first is, and the derivative pass squares again
+ * (more products, less memory). -1 (the default): a quarter of the free
+ * device memory at the time of the call. */
+int tns_set_checkpoint_bytes(tns_context* ctx, long long bytes);
+
 /* ---- complex product without allocation -------------------------------- */
 
 /* No counterpart in the reference: the reference's products run on the CPU

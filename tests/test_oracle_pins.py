@@ -34,7 +34,7 @@ def _shipped_tables():
     import re
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = {}
-    for path in ("csharp_linearalgebra_b200/csrc/expm_batched.cu", "oracle/tensile_oracle.cpp"):
+    for path in ("csharp_linearalgebra_b200/csrc/pade.h", "oracle/tensile_oracle.cpp"):
         src = open(os.path.join(root, path)).read()
         tabs = {}
         for m in (3, 5, 7, 9, 13):
