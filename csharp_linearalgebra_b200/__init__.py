@@ -389,6 +389,25 @@ class Workspace:
         return {"loss": loss.value, "f": f, "grad_a": ga, "grad_b": gb, "grad_t": gt.value,
                 "degree": info.degree, "squarings": info.squarings}
 
+    # -- precision form of the solve --------------------------------------------
+    def solve_mixed(self, a, b, moduli: int = 0, max_iter: int = 20):
+        """A^-1 B by a low-precision LU (trailing updates on the split-precision
+        product) and FP64 iterative refinement. Returns (X, info dict)."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+        a, b = _fortran(a, cplx), _fortran(b, cplx)
+        vec = b.ndim == 1
+        if vec:
+            b = b.reshape(-1, 1, order="F")
+        if a.ndim != 2 or a.shape[0] != a.shape[1] or b.shape[0] != a.shape[0]:
+            raise ValueError(f"A must be square and B have its order of rows, got {a.shape} and {b.shape}.")
+        n, c = b.shape
+        x = np.zeros((n, c), dtype=a.dtype, order="F")
+        info = N.MixedInfo()
+        self._call("tns_zgesv_mixed" if cplx else "tns_dgesv_mixed", n, c, _p(a), _ld(a), _p(b), _ld(b), _p(x),
+                   _ld(x), int(moduli), int(max_iter), C.byref(info))
+        d = {k: getattr(info, k) for k, _ in N.MixedInfo._fields_}
+        return (x[:, 0] if vec else x), d
+
     def set_checkpoint_bytes(self, nbytes: int):
         """Device bytes the Frechet derivative may hold for its squarings (-1: automatic)."""
         self._call("tns_set_checkpoint_bytes", int(nbytes))

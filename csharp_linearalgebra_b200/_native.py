@@ -42,6 +42,11 @@ class ExpmvInfo(C.Structure):
                 ("early_exits", C.c_int)]
 
 
+class MixedInfo(C.Structure):
+    _fields_ = [("moduli", C.c_int), ("factorizations", C.c_int), ("iterations", C.c_int),
+                ("backward_error", C.c_double), ("rcond", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
                 ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double),
@@ -86,6 +91,8 @@ SIGNATURES = {
     "tns_zexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
                                  C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
     "tns_set_checkpoint_bytes": (_I, [_P, _LL]),
+    "tns_dgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),
+    "tns_zgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),
     "tns_zgemm_device_noalloc": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),
     "tns_set_workers": (_I, [_P, _I]),
     "tns_get_stats": (_I, [_P, C.POINTER(Stats)]),

@@ -352,6 +352,29 @@ int gradient_entry(tns_context* c, bool cplx, int n, int nc, double t, const dou
     });
 }
 
+int gesv_mixed_entry(tns_context* c, bool cplx, int n, int nrhs, const double* a, int lda, const double* b, int ldb,
+                     double* x, int ldx, int moduli, int max_iter, tns_mixed_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(b, n, nrhs, ldb, "B");
+        check_operand(x, n, nrhs, ldx, "X");
+        require(moduli == 0 || (moduli >= 8 && moduli <= 22), TNS_E_OUT_OF_RANGE, "moduli must be 0 or 8..22");
+        require(max_iter >= 0, TNS_E_OUT_OF_RANGE, "max_iter must not be negative");
+        tns_mixed_info local{};
+        tns_mixed_info* inf = info ? info : &local;
+        *inf = tns_mixed_info{0, 0, 0, 0.0, 0.0};
+        if (n == 0 || nrhs == 0) return;
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the matrix");
+        DMat B = upload(ctx, b, n, nrhs, ldb, cplx, false, "the right-hand sides");
+        DMat X;
+        tns::MixedInfo mi;
+        tns::gesv_mixed(ctx, A, B, X, moduli, max_iter, mi);
+        tns::copy_out(ctx, X, x, ldx, false);
+        ctx.sync();
+        *inf = tns_mixed_info{mi.moduli, mi.factorizations, mi.iterations, mi.backward_error, mi.rcond};
+    });
+}
+
 int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
                         double* const* out, const int* ldo, tns_expm_info* infos) {
     return guarded(c, [&](Context& ctx) {
@@ -652,6 +675,14 @@ int tns_zexpmv_gradient(tns_context* c, int n, int ncols, double t, const double
                         int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info) {
     return gradient_entry(c, true, n, ncols, t, a, lda, b, ldb, y, ldy, loss, grad_a, ldga, grad_b, ldgb, grad_t, f,
                           ldf, info);
+}
+int tns_dgesv_mixed(tns_context* c, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
+                    int ldx, int moduli, int max_iter, tns_mixed_info* info) {
+    return gesv_mixed_entry(c, false, n, nrhs, a, lda, b, ldb, x, ldx, moduli, max_iter, info);
+}
+int tns_zgesv_mixed(tns_context* c, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
+                    int ldx, int moduli, int max_iter, tns_mixed_info* info) {
+    return gesv_mixed_entry(c, true, n, nrhs, a, lda, b, ldb, x, ldx, moduli, max_iter, info);
 }
 int tns_set_checkpoint_bytes(tns_context* c, long long bytes) {
     return guarded(c, [&](Context& ctx) {

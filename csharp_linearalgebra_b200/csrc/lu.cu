@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <vector>
 
 namespace tns {
@@ -193,6 +194,261 @@ __global__ void __launch_bounds__(512) panel_kernel(const __grid_constant__ Batc
             }
         }
         __syncthreads();
+    }
+}
+
+// The same factorization for one tall panel (thousands of rows), spread over
+// every SM: CTA g owns panel rows [g R, (g + 1) R) and keeps them in shared
+// memory for the whole panel (the single-CTA kernel re-reads and re-writes
+// the trailing panel through L2 for every column, which at 4096 rows is about
+// a millisecond per panel). Per column, one grid barrier:
+//   before it, every CTA posts its first-largest candidate (value, row) and
+//   that row's data, and the owner of row j posts row j (double-buffered by
+//   column parity, so one barrier per column suffices);
+//   after it, every CTA picks the same pivot p from the candidates (largest
+//   measure, lowest row on ties, the diagonal if no comparison succeeds), the
+//   owners of rows j and p swap them, and every CTA scales column j and
+//   updates its rows with the pivot row.
+// Each element sees exactly the single-CTA kernel's operations in the same
+// order, so factors and pivots are unchanged (tested bit for bit). The launch
+// is cooperative (all CTAs resident); the barrier gives up after 2 s with
+// kErrPanelBarrier in the context's error flag, and every CTA then returns.
+enum : int { kErrPanelBarrier = 21 };
+
+struct CoopPanelDesc {
+    double* a;
+    int ld, m, r0, w;
+    int* piv;
+    int* singular;
+    int rows;            // panel rows per CTA
+    double* cand_val;    // [2][G]
+    int* cand_idx;       // [2][G]
+    double* xch;         // [2][G + 1][128]: each CTA's candidate row, then row j
+    unsigned* bar;       // arrival count, generation
+    int* err;
+};
+
+__device__ bool grid_barrier_bounded(unsigned* bar, unsigned nblocks, int* err) {
+    __shared__ int s_ok;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        bool ok = true;
+        if (atomicAdd(bar, 1u) + 1 == nblocks) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const unsigned long long start = global_timer_ns();
+            for (uint32_t it = 1; *gen == g0; ++it) {
+                if ((it & 255u) == 0) {
+                    if (*reinterpret_cast<volatile int*>(err) != 0 || global_timer_ns() - start > kWaitTimeoutNs) {
+                        atomicCAS(err, 0, kErrPanelBarrier);
+                        ok = false;
+                        break;
+                    }
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) panel_coop_kernel(const CoopPanelDesc d) {
+    constexpr int ES = CPLX ? 2 : 1;
+    extern __shared__ double slab[];  // [c][r][q], rows R, columns w
+    __shared__ double s_prow[128], s_rowj[128];
+    __shared__ double s_val[8];
+    __shared__ int s_idx[8], s_own[8];
+    __shared__ int s_p, s_owner;
+    const int tid = threadIdx.x, G = gridDim.x, g = blockIdx.x;
+    const int ld = d.ld, w = d.w, R = d.rows;
+    const int M = d.m - d.r0;
+    const int rb = g * R, re = min(M, rb + R);
+    double* P = d.a + ((size_t)d.r0 * ld + d.r0) * ES;
+    auto S = [&](int r, int c) -> double* { return slab + ((size_t)c * R + (r - rb)) * ES; };
+    for (int e = tid; e < (re - rb) * w * ES; e += blockDim.x) {
+        const int q = e % ES, r = (e / ES) % (re - rb), c = e / (ES * (re - rb));
+        S(rb + r, c)[q] = P[((size_t)c * ld + rb + r) * ES + q];
+    }
+    __syncthreads();
+    const int limit = min(M, w);
+    for (int j = 0; j < limit; ++j) {
+        const int buf = j & 1;
+        // a. this CTA's first-largest candidate in column j, rows >= j
+        double best = -1.0;
+        int bidx = INT_MAX;
+        for (int i = max(j, rb) + tid; i < re; i += blockDim.x) {
+            const double* e = S(i, j);
+            const double v = CPLX ? add_rn(fabs(e[0]), fabs(e[1])) : fabs(e[0]);
+            if (v > best || (v == best && i < bidx)) {
+                best = v;
+                bidx = i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (ov > best || (ov == best && oi < bidx)) {
+                best = ov;
+                bidx = oi;
+            }
+        }
+        if ((tid & 31) == 0) {
+            s_val[tid >> 5] = best;
+            s_idx[tid >> 5] = bidx;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = s_val[0];
+            int bi = s_idx[0];
+            for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+                if (s_val[q] > bv || (s_val[q] == bv && s_idx[q] < bi)) {
+                    bv = s_val[q];
+                    bi = s_idx[q];
+                }
+            d.cand_val[buf * G + g] = bv;
+            d.cand_idx[buf * G + g] = bi;
+            s_p = bi;
+        }
+        __syncthreads();
+        double* slot = d.xch + ((size_t)buf * (G + 1) + g) * 128;
+        double* slotj = d.xch + ((size_t)buf * (G + 1) + G) * 128;
+        if (s_p != INT_MAX)
+            for (int e = tid; e < w * ES; e += blockDim.x) slot[e] = S(s_p, e / ES)[e % ES];
+        if (j >= rb && j < re)
+            for (int e = tid; e < w * ES; e += blockDim.x) slotj[e] = S(j, e / ES)[e % ES];
+        // b. one barrier per column
+        if (!grid_barrier_bounded(d.bar, G, d.err)) return;
+        // c. the pivot, the same in every CTA: every thread loads candidates
+        // (one L2 round trip in parallel), then a block reduction under the
+        // same order (larger measure, then lower row).
+        {
+            double bv = -1.0;
+            int bi = INT_MAX, owner = -1;
+            for (int q = tid; q < G; q += blockDim.x) {
+                const int i = __ldcg(d.cand_idx + buf * G + q);
+                const double v = __ldcg(d.cand_val + buf * G + q);
+                if (i != INT_MAX && (v > bv || (v == bv && i < bi))) {
+                    bv = v;
+                    bi = i;
+                    owner = q;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                const int oo = __shfl_xor_sync(0xffffffffu, owner, o);
+                if (oi != INT_MAX && (ov > bv || (ov == bv && oi < bi))) {
+                    bv = ov;
+                    bi = oi;
+                    owner = oo;
+                }
+            }
+            __syncthreads();  // s_val / s_idx are reused from step a
+            if ((tid & 31) == 0) {
+                s_val[tid >> 5] = bv;
+                s_idx[tid >> 5] = bi;
+                s_own[tid >> 5] = owner;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                bv = s_val[0];
+                bi = s_idx[0];
+                owner = s_own[0];
+                for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+                    if (s_idx[q] != INT_MAX && (s_val[q] > bv || (s_val[q] == bv && s_idx[q] < bi))) {
+                        bv = s_val[q];
+                        bi = s_idx[q];
+                        owner = s_own[q];
+                    }
+                if (bi == INT_MAX) {  // no comparison succeeded (NaNs): keep the diagonal
+                    bi = j;
+                    owner = -1;
+                }
+                s_p = bi;
+                s_owner = owner;
+                if (g == 0) d.piv[d.r0 + j] = d.r0 + bi;
+            }
+            __syncthreads();
+        }
+        const int p = s_p;
+        const double* prow = s_owner >= 0 ? d.xch + ((size_t)buf * (G + 1) + s_owner) * 128 : slotj;
+        for (int e = tid; e < w * ES; e += blockDim.x) {
+            s_prow[e] = __ldcg(prow + e);
+            s_rowj[e] = __ldcg(slotj + e);
+        }
+        __syncthreads();
+        // d. swap rows j and p (each owner writes the other's row)
+        if (p != j) {
+            if (p >= rb && p < re)
+                for (int e = tid; e < w * ES; e += blockDim.x) S(p, e / ES)[e % ES] = s_rowj[e];
+            if (j >= rb && j < re)
+                for (int e = tid; e < w * ES; e += blockDim.x) S(j, e / ES)[e % ES] = s_prow[e];
+        }
+        __syncthreads();
+        // e. scale column j below the diagonal, then the rank-1 update of columns j+1..w-1
+        const int i0 = max(j + 1, rb);
+        if (!CPLX) {
+            const double value = s_prow[j];
+            if (value == 0.0 && g == 0 && tid == 0) atomicMin(d.singular, d.r0 + j);
+            const bool recip = fabs(value) >= kSafeMin;
+            const double r = __ddiv_rn(1.0, value);
+            if (value != 0.0)
+                for (int i = i0 + tid; i < re; i += blockDim.x) {
+                    double* l = S(i, j);
+                    *l = recip ? mul_rn(*l, r) : __ddiv_rn(*l, value);
+                }
+            __syncthreads();
+            const int nr = re - i0, nc = w - j - 1;
+            for (int e = tid; e < nr * max(nc, 0); e += blockDim.x) {
+                const int i = i0 + e % nr, c = j + 1 + e / nr;
+                const double mult = s_prow[c];
+                if (mult != 0.0) {
+                    double* t = S(i, c);
+                    *t = add_rn(*t, mul_rn(-mult, *S(i, j)));
+                }
+            }
+        } else {
+            const Z value{s_prow[2 * j], s_prow[2 * j + 1]};
+            const bool zero = value.re == 0.0 && value.im == 0.0;
+            if (zero && g == 0 && tid == 0) atomicMin(d.singular, d.r0 + j);
+            const bool recip = cabs_net(value.re, value.im) >= kSafeMin;
+            const Z r = zdiv(Z{1.0, 0.0}, value);
+            if (!zero)
+                for (int i = i0 + tid; i < re; i += blockDim.x) {
+                    double* l = S(i, j);
+                    const Z lv{l[0], l[1]};
+                    const Z o = recip ? zmul(lv, r) : zdiv(lv, value);
+                    l[0] = o.re;
+                    l[1] = o.im;
+                }
+            __syncthreads();
+            const int nr = re - i0, nc = w - j - 1;
+            for (int e = tid; e < nr * max(nc, 0); e += blockDim.x) {
+                const int i = i0 + e % nr, c = j + 1 + e / nr;
+                const Z mult{s_prow[2 * c], s_prow[2 * c + 1]};
+                if (mult.re == 0.0 && mult.im == 0.0) continue;
+                double* t = S(i, c);
+                const double* l = S(i, j);
+                const Z o = zadd(Z{t[0], t[1]}, zmul(Z{-mult.re, -mult.im}, Z{l[0], l[1]}));
+                t[0] = o.re;
+                t[1] = o.im;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < (re - rb) * w * ES; e += blockDim.x) {
+        const int q = e % ES, r = (e / ES) % (re - rb), c = e / (ES * (re - rb));
+        P[((size_t)c * ld + rb + r) * ES + q] = S(rb + r, c)[q];
     }
 }
 
@@ -560,8 +816,109 @@ __global__ void fill_int_kernel(int* p, int count, int v) {
 
 // ---- launchers ---------------------------------------------------------------
 
+// P B for a solve with few right-hand sides: laswp gives each column one
+// thread and n sequential swaps, which leaves the GPU idle when B is narrow.
+// Instead one CTA per item replays the swaps on an index array in shared
+// memory (row k of P B is row perm[k] of B), and a gather moves every row
+// once. The result is the same values in the same places.
+struct PermDesc {
+    const int* piv;
+    int n;
+    int* perm;
+};
+__global__ void build_perm_kernel(const __grid_constant__ Batch<PermDesc> b) {
+    const PermDesc& d = batch_item(b, blockIdx.x);
+    extern __shared__ int sp[];  // perm [n], pivots [n]
+    int* pv = sp + d.n;
+    for (int i = threadIdx.x; i < d.n; i += blockDim.x) {
+        sp[i] = i;
+        pv[i] = d.piv[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < d.n; ++k) {
+            const int p = pv[k];
+            if (p != k) {
+                const int t = sp[k];
+                sp[k] = sp[p];
+                sp[p] = t;
+            }
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < d.n; i += blockDim.x) d.perm[i] = sp[i];
+}
+struct GatherDesc {
+    const double* src;
+    double* dst;
+    int ld, rows, cols;
+    const int* perm;
+};
+template <bool CPLX>
+__global__ void gather_rows_kernel(const __grid_constant__ Batch<GatherDesc> b) {
+    const GatherDesc& d = batch_item(b, blockIdx.y);
+    constexpr int ES = CPLX ? 2 : 1;
+    const size_t total = (size_t)d.rows * d.cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % d.rows), c = (int)(e / d.rows);
+        const double* s = d.src + ((size_t)c * d.ld + d.perm[i]) * ES;
+        double* t = d.dst + ((size_t)c * d.ld + i) * ES;
+        t[0] = s[0];
+        if (CPLX) t[1] = s[1];
+    }
+}
+constexpr int kGatherMaxCols = 128;
+constexpr int kGatherMaxRows = 24576;  // perm + pivots in 192 KB of shared memory
+
+// One tall panel over all SMs (panel_coop_kernel), when it has enough rows
+// to pay for a barrier per column and every CTA's slab fits shared memory.
+constexpr int kCoopPanelRows = 1024;
+
+template <bool CPLX>
+bool launch_panel_coop(Context& ctx, const PanelFactorDesc& p) {
+    constexpr int ES = CPLX ? 2 : 1;
+    const int M = p.m - p.r0;
+    const int G = ctx.num_sms;
+    const int R = (M + G - 1) / G;
+    const size_t smem = (size_t)R * p.w * ES * sizeof(double);
+    if (smem > 160 * 1024) return false;
+    static bool configured[2][64] = {};
+    if (!configured[CPLX][ctx.device]) {
+        TNS_CUDA(cudaFuncSetAttribute(panel_coop_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      160 * 1024));
+        configured[CPLX][ctx.device] = true;
+    }
+    int per_sm = 0;
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_coop_kernel<CPLX>, 256, smem));
+    if (per_sm < 1) return false;
+    DBuf scratch(ctx, sizeof(double) * 2 * G + sizeof(int) * 2 * G + sizeof(double) * 2 * (G + 1) * 128 + 64);
+    char* base = scratch.as<char>();
+    CoopPanelDesc d{};
+    d.a = p.a;
+    d.ld = p.ld;
+    d.m = p.m;
+    d.r0 = p.r0;
+    d.w = p.w;
+    d.piv = p.piv;
+    d.singular = p.singular;
+    d.rows = R;
+    d.xch = reinterpret_cast<double*>(base);
+    d.cand_val = d.xch + 2 * (size_t)(G + 1) * 128;
+    d.cand_idx = reinterpret_cast<int*>(d.cand_val + 2 * G);
+    d.bar = reinterpret_cast<unsigned*>(d.cand_idx + 2 * G);
+    d.err = ctx.d_err;
+    TNS_CUDA(cudaMemsetAsync(d.bar, 0, 2 * sizeof(unsigned), ctx.stream));
+    void* args[] = {&d};
+    TNS_CUDA(cudaLaunchCooperativeKernel((const void*)panel_coop_kernel<CPLX>, dim3(G), dim3(256), args, smem,
+                                         ctx.stream));
+    ctx.kernel_launches++;
+    return true;
+}
+
 void launch_panels(Context& ctx, bool cplx, std::vector<PanelFactorDesc>& v) {
     if (v.empty()) return;
+    if (v.size() == 1 && v[0].m - v[0].r0 >= kCoopPanelRows && v[0].w <= 64) {
+        if (cplx ? launch_panel_coop<true>(ctx, v[0]) : launch_panel_coop<false>(ctx, v[0])) return;
+    }
     Batch<PanelFactorDesc> b = make_batch(ctx, v);
     if (cplx) panel_kernel<true><<<b.count, 512, 0, ctx.stream>>>(b);
     else panel_kernel<false><<<b.count, 512, 0, ctx.stream>>>(b);
@@ -764,15 +1121,61 @@ void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
         // the reference's order (Lu.Solve, Lu.cs:336-351; BlockedLu.Solve,
         // BlockedLu.cs:105-118): the result matches the reference bit for bit.
         std::vector<LaswpDesc> swaps;
+        std::vector<SolveItem*> narrow;
         constexpr int B = kSubstBlock;
         int steps = 0;
         for (auto& it : items) {
             int n = it.lu->rows;
             if (n == 0 || it.nrhs == 0) continue;
-            swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
+            if (it.nrhs < kGatherMaxCols && n <= kGatherMaxRows) narrow.push_back(&it);
+            else swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
             steps = std::max(steps, (n + B - 1) / B);
         }
         launch_laswp(ctx, cplx, swaps);
+        if (!narrow.empty()) {
+            size_t total = 0;
+            int maxn = 0;
+            for (auto* it : narrow) {
+                total += (size_t)it->lu->rows;
+                maxn = std::max(maxn, it->lu->rows);
+            }
+            DBuf perms(ctx, sizeof(int) * total);
+            std::vector<DMat> tmp;
+            tmp.reserve(narrow.size());
+            std::vector<PermDesc> pd;
+            std::vector<GatherDesc> gd;
+            size_t off = 0;
+            long long maxe = 0;
+            for (auto* it : narrow) {
+                const int n = it->lu->rows;
+                tmp.emplace_back(ctx, it->b->rows, it->b->cols, cplx, "the permuted right-hand sides");
+                pd.push_back(PermDesc{it->d_piv, n, perms.as<int>() + off});
+                gd.push_back(GatherDesc{it->b->p, tmp.back().p, it->b->ld(), n, it->nrhs, perms.as<int>() + off});
+                off += (size_t)n;
+                maxe = std::max(maxe, (long long)n * it->nrhs);
+            }
+            Batch<PermDesc> bp = make_batch(ctx, pd);
+            const size_t smem = sizeof(int) * 2 * (size_t)maxn;
+            static bool configured[64] = {};
+            if (!configured[ctx.device]) {
+                TNS_CUDA(cudaFuncSetAttribute(build_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)(sizeof(int) * 2 * kGatherMaxRows)));
+                configured[ctx.device] = true;
+            }
+            build_perm_kernel<<<bp.count, 256, smem, ctx.stream>>>(bp);
+            TNS_CUDA(cudaGetLastError());
+            Batch<GatherDesc> bg = make_batch(ctx, gd);
+            const dim3 grid((unsigned)std::min<long long>((maxe + 255) / 256, ctx.num_sms * 8), bg.count);
+            if (cplx) gather_rows_kernel<true><<<grid, 256, 0, ctx.stream>>>(bg);
+            else gather_rows_kernel<false><<<grid, 256, 0, ctx.stream>>>(bg);
+            TNS_CUDA(cudaGetLastError());
+            ctx.kernel_launches += 2;
+            // back into B, only the solve's nrhs columns (contiguous: ld = rows_p)
+            for (size_t q = 0; q < narrow.size(); ++q)
+                TNS_CUDA(cudaMemcpyAsync(narrow[q]->b->p, tmp[q].p,
+                                         (size_t)narrow[q]->b->ld() * narrow[q]->nrhs * narrow[q]->b->esz(),
+                                         cudaMemcpyDeviceToDevice, ctx.stream));
+        }
         // Lower: blocks from the top; upper: each item's blocks from its last.
         for (int upper = 0; upper < 2; ++upper)
             for (int s = 0; s < steps; ++s) {
@@ -878,6 +1281,215 @@ LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint) {
     std::vector<SolveItem> items{SolveItem{&lu, d_piv, &b, nrhs}};
     getrs_batch(ctx, items, adjoint);
+}
+
+// ---------------------------------------------------------------------------
+// The precision form of the solve (no counterpart in the reference, whose
+// solves are FP64 throughout: Lu.Factor + Lu.Solve, Lu.cs:230-351).
+//
+// Factorization. Right-looking in blocks of 512 columns: the 512-wide panel
+// is factored by getrf_batch (its own 64-column steps, FP64 panels and DMMA
+// updates), its row interchanges are applied either side, U12 := L11^-1 A12
+// by 64-row triangular blocks and DMMA updates, and the trailing update
+// A22 -= L21 U12 -- almost all of the (2/3) n^3 flops -- runs on the
+// split-precision product (8-bit residues on the tensor cores) with depth
+// 512. Its precision is set by the moduli: the integer images keep t bits
+// (26 with 8 moduli, 49 with 14), so the factors are those of A + dA with
+// |dA| about 2^-t of the operands' scales per update.
+// Refinement. x = U^-1 L^-1 P b, then r = b - A x in FP64 (DMMA GEMM),
+// d = U^-1 L^-1 P r, x += d, until the normwise backward error
+// max_j |r_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf) reaches 4 u (u = 2^-53),
+// stops halving, or max_iter steps are done. The refinement converges while
+// kappa(A) 2^-t is well below 1 (each step multiplies the error by about
+// that); with moduli = 0 the moduli are chosen from the condition estimate
+// kappa_1 of the first (8-moduli) factors so that t >= log2(kappa_1) + 7,
+// refactoring once if that needs more than 8.
+
+namespace {
+
+// A non-owning view of the rows x cols block of `a` at (i, j): same leading
+// dimension, and it frees nothing.
+DMat block_view(const DMat& a, int i, int j, int rows, int cols) {
+    DMat v;
+    v.p = const_cast<double*>(a.at(i, j));
+    v.rows = rows;
+    v.cols = cols;
+    v.rows_p = a.rows_p;
+    v.cols_p = cols;
+    v.cplx = a.cplx;
+    return v;
+}
+
+__global__ void add_offset_kernel(int* p, int count, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] += v;
+}
+
+// dst := f * src for a rows x cols block (es doubles per element).
+__global__ void scaled_block_copy_kernel(double* dst, int ldd, const double* src, int lds, int rows, int cols,
+                                         double f, int es) {
+    const size_t h = (size_t)rows * es;
+    const size_t total = h * cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = e % h, c = e / h;
+        dst[c * ldd * es + r] = mul_rn(src[c * lds * es + r], f);
+    }
+}
+
+// out[j] = max_i |x_ij| (complex: the modulus), one warp per column.
+template <bool CPLX>
+__global__ void col_absmax_kernel(const double* x, int ld, int rows, int cols, double* out) {
+    const int j = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (j >= cols) return;
+    double m = 0.0;
+    for (int i = lane; i < rows; i += 32) {
+        const double v = CPLX ? hypot(x[((size_t)j * ld + i) * 2], x[((size_t)j * ld + i) * 2 + 1])
+                              : fabs(x[(size_t)j * ld + i]);
+        m = fmax(m, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) out[j] = m;
+}
+
+std::vector<double> col_absmax(Context& ctx, const DMat& x) {
+    DBuf buf(ctx, sizeof(double) * std::max(1, x.cols));
+    const int warps = 8;
+    if (x.cplx)
+        col_absmax_kernel<true><<<(x.cols + warps - 1) / warps, 32 * warps, 0, ctx.stream>>>(x.p, x.ld(), x.rows,
+                                                                                          x.cols, buf.as<double>());
+    else
+        col_absmax_kernel<false><<<(x.cols + warps - 1) / warps, 32 * warps, 0, ctx.stream>>>(x.p, x.ld(), x.rows,
+                                                                                           x.cols, buf.as<double>());
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+    std::vector<double> out(x.cols);
+    TNS_CUDA(cudaMemcpyAsync(out.data(), buf.p, sizeof(double) * x.cols, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    return out;
+}
+
+constexpr int kMixedOuter = 512;  // depth of the split-precision trailing updates
+
+}  // namespace
+
+void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli) {
+    const int n = a.rows, ld = a.ld();
+    const bool cplx = a.cplx;
+    const int es = cplx ? 2 : 1;
+    const int blocks = (n + kMixedOuter - 1) / kMixedOuter;
+    DBuf sing(ctx, sizeof(int) * std::max(1, blocks));
+    for (int q = 0; q < blocks; ++q) {
+        const int j = q * kMixedOuter, w = std::min(kMixedOuter, n - j);
+        DMat panel = block_view(a, j, j, n - j, w);
+        int* piv = d_piv + j;  // rows relative to row j until the offset below
+        {
+            std::vector<LuItem> items{LuItem{&panel, n - j, w, 64, piv, sing.as<int>() + q}};
+            getrf_batch(ctx, items);
+        }
+        std::vector<LaswpDesc> sw;
+        double* rowj = a.p + (size_t)j * es;
+        if (j > 0) sw.push_back(LaswpDesc{rowj, ld, 0, j, piv, 0, w, 0});
+        if (j + w < n) sw.push_back(LaswpDesc{rowj, ld, j + w, n, piv, 0, w, 0});
+        launch_laswp(ctx, cplx, sw);
+        add_offset_kernel<<<(w + 255) / 256, 256, 0, ctx.stream>>>(piv, w, j);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+        if (j + w >= n) break;
+        const int rest = n - j - w;
+        // U12 := L11^-1 A12: 64-row unit-lower blocks, DMMA updates below each.
+        for (int b0 = 0; b0 < w; b0 += 64) {
+            const int bw = std::min(64, w - b0);
+            std::vector<TrsmDesc> t{TrsmDesc{a.at(j + b0, j + b0), ld, a.at(j + b0, j + w), ld, bw, rest, 1, 1, 0}};
+            launch_trsm(ctx, cplx, 1, t);
+            if (b0 + bw < w) {
+                GemmProblem p{};
+                p.A = a.at(j + b0 + bw, j + b0);
+                p.B = a.at(j + b0, j + w);
+                p.C = a.at(j + b0 + bw, j + w);
+                p.lda = p.ldb = p.ldc = ld;
+                p.M = round_up(w - b0 - bw, 2);
+                p.N = round_up(rest, 2);
+                p.K = round_up(bw, 16);
+                p.alpha_re = -1.0;
+                p.beta_re = 1.0;
+                p.work = (long long)(w - b0 - bw) * rest * bw;
+                std::vector<GemmProblem> g{p};
+                gemm_grouped(ctx, g, cplx);
+            }
+        }
+        // A22 -= L21 U12 on the split-precision product: C += (-L21) U12.
+        DMat negl(ctx, rest, w, cplx, "the negated L21 block of a mixed-precision factorization");
+        {
+            const size_t total = (size_t)rest * es * w;
+            const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)ctx.num_sms * 16);
+            scaled_block_copy_kernel<<<grid, 256, 0, ctx.stream>>>(negl.p, negl.ld(), a.at(j + w, j), ld, rest, w,
+                                                                  -1.0, es);
+            TNS_CUDA(cudaGetLastError());
+            ctx.kernel_launches++;
+        }
+        DMat u12 = block_view(a, j, j + w, w, rest);
+        DMat a22 = block_view(a, j + w, j + w, rest, rest);
+        std::vector<SplitProduct> sp{SplitProduct{&negl, &u12, &a22, 1.0}};
+        gemm_split_batch(ctx, sp, moduli);
+    }
+    std::vector<int> flags(blocks);
+    TNS_CUDA(cudaMemcpyAsync(flags.data(), sing.p, sizeof(int) * blocks, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    for (int q = 0; q < blocks; ++q)
+        if (flags[q] != INT_MAX)
+            fail(TNS_E_SINGULAR, "The low-precision factorization met an exactly zero pivot at column " +
+                                     std::to_string(q * kMixedOuter + flags[q]) + ".");
+}
+
+void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter, MixedInfo& info) {
+    const int n = a.rows, nrhs = b.cols;
+    const bool cplx = a.cplx;
+    info = MixedInfo{};
+    DMat f(ctx, n, n, cplx, "the low-precision factors");
+    DBuf piv(ctx, sizeof(int) * (size_t)std::max(1, n));
+    auto factor = [&](int m) {
+        copy_dmat(ctx, f, a);
+        getrf_mixed(ctx, f, piv.as<int>(), m);
+        info.factorizations++;
+        info.moduli = m;
+    };
+    factor(moduli > 0 ? moduli : 8);
+    const double anorm1 = norm1(ctx, a);
+    const NormestResult est = normest_lu_inverse(ctx, f, piv.as<int>(), 2, 5, 20260915);
+    info.rcond = (anorm1 > 0.0 && est.value > 0.0) ? 1.0 / (anorm1 * est.value) : 0.0;
+    if (moduli == 0) {
+        const double kappa = info.rcond > 0.0 ? 1.0 / info.rcond : 1e300;
+        const int need = (int)std::ceil(std::log2(std::max(1.0, kappa))) + 7;
+        const int depth = cplx ? 2 * kMixedOuter : kMixedOuter;
+        int m = info.moduli;
+        while (m < 22 && split_integer_bits(m, depth) < need) ++m;
+        if (m > info.moduli) factor(m);
+    }
+    x = DMat(ctx, n, nrhs, cplx, "the solution");
+    copy_dmat(ctx, x, b);
+    getrs(ctx, f, piv.as<int>(), x, nrhs, false);
+    const double ainf = norminf(ctx, a);
+    const std::vector<double> bmax = col_absmax(ctx, b);
+    DMat r(ctx, n, nrhs, cplx, "the refinement residual");
+    double prev = INFINITY;
+    for (int it = 0;; ++it) {
+        copy_dmat(ctx, r, b);
+        std::vector<GemmProblem> g{make_gemm(a, x, r, -1.0, 0.0, 1.0, 0.0)};
+        gemm_grouped(ctx, g, cplx);
+        const std::vector<double> rmax = col_absmax(ctx, r), xmax = col_absmax(ctx, x);
+        double berr = 0.0;
+        for (int j = 0; j < nrhs; ++j) {
+            const double den = ainf * xmax[j] + bmax[j];
+            berr = std::max(berr, den > 0.0 ? rmax[j] / den : (rmax[j] > 0.0 ? INFINITY : 0.0));
+        }
+        info.backward_error = berr;
+        if (berr <= 4.0 * 1.1102230246251565e-16 || it >= max_iter || !(berr < 0.5 * prev)) break;
+        prev = berr;
+        getrs(ctx, f, piv.as<int>(), r, nrhs, false);
+        std::vector<EwDesc> add{ew_add_scaled(x, r, 1.0)};
+        ew_batch(ctx, add);
+        info.iterations++;
+    }
 }
 
 }  // namespace tns

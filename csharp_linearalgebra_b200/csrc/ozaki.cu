@@ -917,6 +917,12 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
 
 }  // namespace
 
+int split_integer_bits(int moduli, int kmax) {
+    if (moduli < 8 || moduli > kMaxModuli)
+        fail(TNS_E_ARGUMENT, "split-precision products take 8 to " + std::to_string(kMaxModuli) + " moduli");
+    return crt_params(moduli, kmax).t;
+}
+
 void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int moduli) {
     std::vector<SplitProduct> live;
     for (auto& p : v) {

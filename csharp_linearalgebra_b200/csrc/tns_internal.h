@@ -187,6 +187,8 @@ struct SplitProduct {
     double beta;
 };
 void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int moduli);
+// Integer bits t of the operands' images for `moduli` moduli and products of depth kmax.
+int split_integer_bits(int moduli, int kmax);
 // The thread's message for errors raised outside any context (tns_last_error(NULL)).
 void set_detached_error(const std::string& msg);
 
@@ -286,6 +288,17 @@ struct SolveItem {
 void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint);
 // B := A^-1 B or A^-H B from factors (valid n x n), in place on the valid rows of b.
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
+
+// The precision form of the solve: LU whose trailing updates (depth 512) run
+// on the split-precision product with `moduli` moduli, panels of 512 columns
+// factored by getrf_batch; pivots absolute. Then FP64 iterative refinement.
+void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli);
+struct MixedInfo {
+    int moduli = 0, factorizations = 0, iterations = 0;
+    double backward_error = 0.0, rcond = 0.0;
+};
+// x := A^-1 b (x shaped as b). moduli 0: from the condition estimate.
+void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter, MixedInfo& info);
 
 // ---- algorithms (algos.cu) -------------------------------------------------
 struct NormestResult {

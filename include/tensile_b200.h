@@ -213,6 +213,32 @@ int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, con
 int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
                double t, double* out, int ldo, tns_expmv_info* info);
 
+/* ---- precision form of the solve ----------------------------------------- */
+
+typedef struct {
+    int moduli;            /* moduli of the factorization the refinement used */
+    int factorizations;    /* 1, or 2 when the condition estimate asked for more precision */
+    int iterations;        /* refinement steps taken */
+    double backward_error; /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) at the end */
+    double rcond;          /* 1 / (||A||_1 est ||A^-1||_1) from the first factors */
+} tns_mixed_info;
+
+/* X := A^-1 B (A n x n, B and X n x nrhs) by a low-precision LU and FP64
+ * iterative refinement. The LU's trailing updates (depth 512), nearly all of
+ * its flops, run on the split-precision product with `moduli` moduli (8..22;
+ * the integer images keep 26 bits with 8, 49 with 14); panels of 512 columns
+ * use the FP64 LU. The refinement computes residuals in FP64 and stops when
+ * the backward error reaches 4 u, stops halving, or after max_iter steps.
+ * moduli = 0: chosen from the condition estimate kappa_1 of a first 8-moduli
+ * factorization so that the images keep log2(kappa_1) + 7 bits (refactoring
+ * once when that needs more). No counterpart in the reference, whose solve
+ * (Lu.Factor + Lu.Solve, src/Tensile.Kernels/Lu.cs:230-351) is FP64 throughout;
+ * this is its precision form. TNS_E_SINGULAR for an exactly zero pivot. */
+int tns_dgesv_mixed(tns_context* ctx, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
+                    int ldx, int moduli, int max_iter, tns_mixed_info* info);
+int tns_zgesv_mixed(tns_context* ctx, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
+                    int ldx, int moduli, int max_iter, tns_mixed_info* info);
+
 /* ---- differentiation: Frechet derivative and adjoint ---------------------- */
 
 /* exp(A) and its Frechet derivative L(A, E) = d/dh exp(A + hE) at h = 0, both

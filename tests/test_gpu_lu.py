@@ -37,6 +37,18 @@ def test_complex_lu_matches_oracle(ws, orc, m, n):
     assert np.array_equal(lu.factors, f)  # bit for bit
 
 
+@pytest.mark.parametrize("m,n,cplx", [(2048, 2048, False), (3000, 200, False), (1600, 1600, True)])
+def test_tall_panels_match_oracle(ws, orc, m, n, cplx):
+    """Panels of 1536 rows or more run on every SM (one CTA per slab of rows,
+    a grid barrier per column); factors and pivots stay bit-identical."""
+    rng = np.random.default_rng(m + n)
+    a = rng.uniform(-0.5, 0.5, (m, n)) + (1j * rng.uniform(-0.5, 0.5, (m, n)) if cplx else 0)
+    lu = ws.factor_lu(a)
+    f, piv, info = orc.getrf(a)
+    assert np.array_equal(lu.pivots, piv)
+    assert np.array_equal(lu.factors, f)  # bit for bit
+
+
 def test_pivot_maximises_sum_of_absolute_parts(ws):
     a = np.array([[3.0, 1.0], [2.0 + 2.0j, 1.0]])
     assert ws.factor_lu(a).pivots[0] == 1
