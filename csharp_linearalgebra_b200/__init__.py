@@ -348,6 +348,46 @@ class Workspace:
             diagnostics.applications, diagnostics.early_exits = info.applications, info.early_exits
         return out[:, 0] if vec else out
 
+    def expmv_operator(self, apply, n: int, b, t: float, one_norm_bound: float, complex_: bool = False,
+                       diagnostics: ExpmvDiagnostics | None = None):
+        """exp(tA)B for a matrix-free operator (MatrixExponentialAction.Expmv over
+        ILinearOperator<T>): apply(x_ptr, y_ptr, ncols, ld, stream) must write
+        y := A x for device panels (column-major, leading dimension ld
+        elements, complex interleaved) on the given CUDA stream. No trace
+        shift; one_norm_bound bounds ||A||_1."""
+        cplx = complex_ or np.iscomplexobj(b)
+        b = _fortran(b, cplx)
+        vec = b.ndim == 1
+        if vec:
+            b = b.reshape(-1, 1, order="F")
+        if b.shape[0] != n:
+            raise ValueError(f"B has {b.shape[0]} rows, expected the operator's order {n}.")
+        c = b.shape[1]
+        out = np.zeros((n, c), dtype=b.dtype, order="F")
+        info = N.ExpmvInfo()
+        failure = []
+
+        def trampoline(user, ncols, x, y, ld, stream):
+            try:
+                apply(x, y, ncols, ld, stream)
+                return 0
+            except BaseException as e:  # reported as TNS_E_OPERATOR, then re-raised below
+                failure.append(e)
+                return 1
+
+        cb = N.APPLY_FN(trampoline)
+        try:
+            self._call("tns_zexpmv_operator" if cplx else "tns_dexpmv_operator", n, cb, None, c, _p(b), _ld(b),
+                       float(t), float(one_norm_bound), _p(out), _ld(out), C.byref(info))
+        except Exception:
+            if failure:
+                raise failure[0]
+            raise
+        if diagnostics is not None:
+            diagnostics.degree, diagnostics.scaling = info.degree, info.scaling
+            diagnostics.applications, diagnostics.early_exits = info.applications, info.early_exits
+        return out[:, 0] if vec else out
+
     # -- differentiation ------------------------------------------------------
     def expm_frechet(self, a, e, diagnostics: ExpmDiagnostics | None = None):
         """(exp(A), L(A, E)): the exponential and its Frechet derivative in the

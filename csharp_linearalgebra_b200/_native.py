@@ -22,6 +22,7 @@ TNS_E_TIMEOUT = 6
 TNS_E_DISPOSED = 7
 TNS_E_OUT_OF_RANGE = 8
 TNS_E_NULL = 9
+TNS_E_OPERATOR = 10
 
 
 class LuInfo(C.Structure):
@@ -53,6 +54,9 @@ class Stats(C.Structure):
                 ("split_launches", C.c_longlong), ("split_flops", C.c_double), ("split_int8_ops", C.c_double),
                 ("split_ms", C.c_double), ("split_bytes", C.c_double)]
 
+
+# y := A x on device panels: (user, ncols, x, y, ld, stream) -> status
+APPLY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
 
 # name -> (restype, argtypes)
 _P, _I, _D, _LL, _CH = C.c_void_p, C.c_int, C.c_double, C.c_longlong, C.c_char
@@ -91,6 +95,8 @@ SIGNATURES = {
     "tns_zexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
                                  C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
     "tns_set_checkpoint_bytes": (_I, [_P, _LL]),
+    "tns_dexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_zexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_dgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),
     "tns_zgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),
     "tns_zgemm_device_noalloc": (_I, [_P, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P, _I]),

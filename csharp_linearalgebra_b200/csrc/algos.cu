@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <string>
 #include <limits>
 #include <vector>
 
@@ -138,6 +140,80 @@ NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv,
 // MatrixExponentialAction.Dense + Run + SelectParameters,
 // src/Tensile/MatrixExponentialAction.cs:149-178, 239-410 (trace shift at the
 // typed entry points :138-141 and MatrixExponentialAction.Complex.cs:57-61).
+namespace {
+
+// (m, s) as MatrixExponentialAction.SelectParameters (:347-398): minimise m s
+// over the Taylor degrees subject to the backward error bound; below
+// condition 3.13, or without the sharp bounds (a matrix-free operator), the
+// crude bound from ||tA||_1 over every degree.
+void select_parameters(double scaled_norm, const std::function<double(int)>* alpha, double scale, int cols, int& m,
+                       int& s) {
+    m = 0;
+    s = 1;
+    if (scaled_norm == 0.0) return;
+    int best_degree = 0;
+    double best_scaling = 0.0, best_cost = std::numeric_limits<double>::infinity();
+    auto consider = [&](int index, double norm) {
+        double scaling = std::ceil(norm / kThetas[index]);
+        double cost = kDegrees[index] * scaling;
+        if (cost >= best_cost) return;
+        best_cost = cost;
+        best_degree = kDegrees[index];
+        best_scaling = scaling;
+    };
+    double ca = 2.0 * kEllProbe * kMaxPower * (kMaxPower + 3);
+    double cb = kThetas[kNumDegrees - 1] / (cols * (double)kMaxDegree);
+    if (alpha == nullptr || scaled_norm <= ca * cb) {
+        for (int index = 0; index < kNumDegrees; ++index) consider(index, scaled_norm);
+    } else {
+        for (int p = 2; p <= kMaxPower; ++p) {
+            double alpha_p = scale * (*alpha)(p);
+            for (int index = 0; index < kNumDegrees; ++index) {
+                if (kDegrees[index] < (p * (p - 1)) - 1) continue;
+                consider(index, alpha_p);
+            }
+        }
+    }
+    double steps = std::max(best_scaling, 1.0);
+    if (!std::isfinite(best_cost) || steps > 2147483647.0)
+        fail(TNS_E_OUT_OF_RANGE, "||tA||_1 would need more operator applications than this method can finish. "
+                                 "Reduce t, or shift the operator.");
+    m = best_degree;
+    s = (int)steps;
+}
+
+// Run (:239-320): the scaled Taylor recurrence with early exit, over
+// y := A x for (n x cols) panels of leading dimension ld in device memory.
+void taylor_run(Context& ctx, const std::function<void(const double*, double*, int)>& apply, const DMat& b,
+                double t, int m, int s, double eta_re, double eta_im, ExpmvInfo* info, DMat& result) {
+    const bool cplx = b.cplx;
+    DMat f = like(ctx, b), work = like(ctx, b), next = like(ctx, b);
+    copy_dmat(ctx, f, b);
+    copy_dmat(ctx, work, b);
+    const int ldb = b.ld();
+    for (int i = 0; i < s; ++i) {
+        double c1 = norminf(ctx, work);
+        for (int j = 0; j < m; ++j) {
+            double coefficient = t / (s * (double)(j + 1));
+            apply(work.p, next.p, ldb);
+            scaled_copy(ctx, work, next, coefficient);
+            double c2 = norminf(ctx, work);
+            add_scaled(ctx, f, work, 1.0);
+            info->applications++;
+            if (c1 + c2 <= kUnitRoundoff * norminf(ctx, f)) {
+                info->early_exits++;
+                break;
+            }
+            c1 = c2;
+        }
+        if (!(eta_re == 1.0 && eta_im == 0.0)) scale_inplace(ctx, f.p, f.rows_p, f.cols_p, f.ld(), cplx, eta_re, eta_im);
+        copy_dmat(ctx, work, f);
+    }
+    result = std::move(f);
+}
+
+}  // namespace
+
 void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info) {
     ExpmvInfo local;
     if (!info) info = &local;
@@ -160,48 +236,12 @@ void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, E
         if (std::isnan(d[p])) d[p] = std::pow(normest_power(ctx, sh, p, kEllProbe, 5, kSeed).value, 1.0 / p);
         return d[p];
     };
-    auto alpha = [&](int p) { return net::max(D(p), D(p + 1)); };
+    const std::function<double(int)> alpha = [&](int p) { return net::max(D(p), D(p + 1)); };
 
-    double scale = std::fabs(t);
-    double scaled_norm = scale * one_norm;
     int m = 0, s = 1;
-    if (scaled_norm != 0.0) {
-        int best_degree = 0;
-        double best_scaling = 0.0, best_cost = std::numeric_limits<double>::infinity();
-        auto consider = [&](int index, double norm) {
-            double scaling = std::ceil(norm / kThetas[index]);
-            double cost = kDegrees[index] * scaling;
-            if (cost >= best_cost) return;
-            best_cost = cost;
-            best_degree = kDegrees[index];
-            best_scaling = scaling;
-        };
-        double ca = 2.0 * kEllProbe * kMaxPower * (kMaxPower + 3);
-        double cb = kThetas[kNumDegrees - 1] / (cols * (double)kMaxDegree);
-        if (scaled_norm <= ca * cb) {
-            for (int index = 0; index < kNumDegrees; ++index) consider(index, scaled_norm);
-        } else {
-            for (int p = 2; p <= kMaxPower; ++p) {
-                double alpha_p = scale * alpha(p);
-                for (int index = 0; index < kNumDegrees; ++index) {
-                    if (kDegrees[index] < (p * (p - 1)) - 1) continue;
-                    consider(index, alpha_p);
-                }
-            }
-        }
-        double steps = std::max(best_scaling, 1.0);
-        if (!std::isfinite(best_cost) || steps > 2147483647.0)
-            fail(TNS_E_OUT_OF_RANGE, "||tA||_1 would need more operator applications than this method can finish. "
-                                     "Reduce t, or shift the operator.");
-        m = best_degree;
-        s = (int)steps;
-    }
+    select_parameters(std::fabs(t) * one_norm, &alpha, std::fabs(t), cols, m, s);
     info->degree = m;
     info->scaling = s;
-
-    DMat f = like(ctx, b), work = like(ctx, b), next = like(ctx, b);
-    copy_dmat(ctx, f, b);
-    copy_dmat(ctx, work, b);
     // eta = exp(t*mu/s): real (mu*t)/s; complex Complex(mu.re*t, mu.im*t) / (s + 0i).
     double eta_re, eta_im = 0.0;
     if (!cplx) {
@@ -211,27 +251,31 @@ void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, E
         eta_re = e.re;
         eta_im = e.im;
     }
-    // Panel product on the padded b layout: x and y are (n x cols) with ld rows_p.
-    const int ldb = b.ld();
-    for (int i = 0; i < s; ++i) {
-        double c1 = norminf(ctx, work);
-        for (int j = 0; j < m; ++j) {
-            double coefficient = t / (s * (double)(j + 1));
-            panel_product(ctx, sh, work.p, ldb, next.p, ldb, cols, false);
-            scaled_copy(ctx, work, next, coefficient);
-            double c2 = norminf(ctx, work);
-            add_scaled(ctx, f, work, 1.0);
-            info->applications++;
-            if (c1 + c2 <= kUnitRoundoff * norminf(ctx, f)) {
-                info->early_exits++;
-                break;
-            }
-            c1 = c2;
-        }
-        if (!(eta_re == 1.0 && eta_im == 0.0)) scale_inplace(ctx, f.p, f.rows_p, f.cols_p, f.ld(), cplx, eta_re, eta_im);
-        copy_dmat(ctx, work, f);
-    }
-    result = std::move(f);
+    const int cols_b = b.cols;
+    taylor_run(
+        ctx, [&](const double* x, double* y, int ld) { panel_product(ctx, sh, x, ld, y, ld, cols_b, false); }, b, t,
+        m, s, eta_re, eta_im, info, result);
+}
+
+void expmv_operator(Context& ctx, int n, ApplyFn apply, void* user, const DMat& b, double t, double bound,
+                    DMat& result, ExpmvInfo* info) {
+    ExpmvInfo local;
+    if (!info) info = &local;
+    *info = ExpmvInfo{};
+    if (b.rows != n) fail(TNS_E_ARGUMENT, "B has the wrong number of rows for the operator");
+    int m = 0, s = 1;
+    select_parameters(std::fabs(t) * bound, nullptr, std::fabs(t), b.cols, m, s);
+    info->degree = m;
+    info->scaling = s;
+    const int cols = b.cols;
+    // No trace, so no shift: mu = 0 and eta = 1 (:227-228).
+    taylor_run(
+        ctx,
+        [&](const double* x, double* y, int ld) {
+            const int rc = apply(user, cols, x, y, ld, ctx.stream);
+            if (rc != 0) fail(TNS_E_OPERATOR, "the operator's apply callback returned " + std::to_string(rc));
+        },
+        b, t, m, s, 1.0, 0.0, info, result);
 }
 
 }  // namespace tns

@@ -375,6 +375,32 @@ int gesv_mixed_entry(tns_context* c, bool cplx, int n, int nrhs, const double* a
     });
 }
 
+int expmv_operator_entry(tns_context* c, bool cplx, int n, tns_apply_fn apply, void* user, int ncols,
+                         const double* b, int ldb, double t, double bound, double* out, int ldo, tns_expmv_info* info) {
+    return guarded(c, [&](Context& ctx) {
+        require(apply != nullptr, TNS_E_NULL, "The operator is null.");
+        check_operand(b, n, ncols, ldb, "B");
+        check_operand(out, n, ncols, ldo, "the result");
+        require(std::isfinite(bound) && bound >= 0.0, TNS_E_OUT_OF_RANGE,
+                "The norm bound must be finite and not negative.");
+        require(std::isfinite(t), TNS_E_OUT_OF_RANGE, "t must be finite");
+        tns_expmv_info local{};
+        tns_expmv_info* inf = info ? info : &local;
+        *inf = tns_expmv_info{0, 0, 0, 0};
+        if (n == 0 || ncols == 0) return;
+        DMat B = upload(ctx, b, n, ncols, ldb, cplx, false, "the panel");
+        DMat R;
+        tns::ExpmvInfo ei;
+        tns::expmv_operator(ctx, n, apply, user, B, t, bound, R, &ei);
+        tns::copy_out(ctx, R, out, ldo, false);
+        ctx.sync();
+        inf->degree = ei.degree;
+        inf->scaling = ei.scaling;
+        inf->applications = ei.applications;
+        inf->early_exits = ei.early_exits;
+    });
+}
+
 int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
                         double* const* out, const int* ldo, tns_expm_info* infos) {
     return guarded(c, [&](Context& ctx) {
@@ -675,6 +701,14 @@ int tns_zexpmv_gradient(tns_context* c, int n, int ncols, double t, const double
                         int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info) {
     return gradient_entry(c, true, n, ncols, t, a, lda, b, ldb, y, ldy, loss, grad_a, ldga, grad_b, ldgb, grad_t, f,
                           ldf, info);
+}
+int tns_dexpmv_operator(tns_context* c, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
+                        double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info) {
+    return expmv_operator_entry(c, false, n, apply, user, ncols, b, ldb, t, one_norm_bound, out, ldo, info);
+}
+int tns_zexpmv_operator(tns_context* c, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
+                        double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info) {
+    return expmv_operator_entry(c, true, n, apply, user, ncols, b, ldb, t, one_norm_bound, out, ldo, info);
 }
 int tns_dgesv_mixed(tns_context* c, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
                     int ldx, int moduli, int max_iter, tns_mixed_info* info) {

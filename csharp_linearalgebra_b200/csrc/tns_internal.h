@@ -321,6 +321,10 @@ struct ExpmvInfo {
     int degree = 0, scaling = 0, applications = 0, early_exits = 0;
 };
 void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info);
+// The matrix-free form: y := A x by a caller's function on device panels.
+using ApplyFn = int (*)(void* user, int ncols, const double* x, double* y, int ld, void* stream);
+void expmv_operator(Context& ctx, int n, ApplyFn apply, void* user, const DMat& b, double t, double bound,
+                    DMat& result, ExpmvInfo* info);
 
 // ---- Frechet derivative and adjoint (frechet.cu) -----------------------------
 // exp(a) and, for a direction e, L(a, e) = d/dh exp(a + h e) at h = 0.

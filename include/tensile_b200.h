@@ -44,6 +44,7 @@ extern "C" {
 #define TNS_E_DISPOSED 7         /* ObjectDisposedException: null or destroyed context */
 #define TNS_E_OUT_OF_RANGE 8     /* ArgumentOutOfRangeException */
 #define TNS_E_NULL 9             /* ArgumentNullException */
+#define TNS_E_OPERATOR 10        /* a caller's operator callback reported failure */
 
 typedef struct tns_context tns_context;
 
@@ -277,6 +278,32 @@ int tns_zexpmv_gradient(tns_context* ctx, int n, int ncols, double t, const doub
  * (more products, less memory). -1 (the default): a quarter of the free
  * device memory at the time of the call. */
 int tns_set_checkpoint_bytes(tns_context* ctx, long long bytes);
+
+/* ---- matrix-free exponential action ------------------------------------- */
+
+/* A matrix-free operator: the device-side ILinearOperator<T>.Apply
+ * (src/Tensile/LinearOperators.cs:37-75). It must write y := A x for the
+ * n x ncols panel x. Both panels are in device memory, column-major with
+ * leading dimension ld in elements (complex: interleaved (re, im) pairs).
+ * The work goes on `stream` (a cudaStream_t, the context's stream), in stream
+ * order; the callback may launch its own kernels there. It returns 0 on
+ * success; any other value ends the call with TNS_E_OPERATOR. The panels
+ * stay on the device from one application to the next: no host copy per
+ * application. */
+typedef int (*tns_apply_fn)(void* user, int ncols, const double* x, double* y, int ld, void* stream);
+
+/* exp(tA)B for an operator known only through `apply`
+ * (MatrixExponentialAction.Expmv(ILinearOperator<T>, B, t, oneNormBound),
+ * src/Tensile/MatrixExponentialAction.cs:203-230; complex .Complex.cs:85-111).
+ * The reference's semantics: no trace shift (mu = 0), one_norm_bound an upper
+ * bound on ||A||_1 (finite, >= 0, else TNS_E_OUT_OF_RANGE), and the degree and
+ * scaling from the crude bound |t| one_norm_bound alone, with no norm
+ * estimation, so (m, s) are the reference's exactly. apply NULL:
+ * TNS_E_NULL. */
+int tns_dexpmv_operator(tns_context* ctx, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
+                        double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info);
+int tns_zexpmv_operator(tns_context* ctx, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
+                        double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info);
 
 /* ---- complex product without allocation -------------------------------- */
 

@@ -85,6 +85,8 @@ def lib():
             getattr(L, name).argtypes = [i, P, i, P, i, C.POINTER(ExpmInfo)]
         for name in ("orc_dexpmv", "orc_zexpmv"):
             getattr(L, name).argtypes = [i, P, i, i, P, i, d, P, i, C.POINTER(ExpmvInfo)]
+        for name in ("orc_dexpmv_bound", "orc_zexpmv_bound"):
+            getattr(L, name).argtypes = [i, P, i, i, P, i, d, d, P, i, C.POINTER(ExpmvInfo)]
         _lib = L
     return _lib
 
@@ -243,6 +245,23 @@ def expm(a):
         raise ZeroDivisionError("singular Pade denominator")
     assert rc == 0
     return out, {k: getattr(info, k) for k, _ in ExpmInfo._fields_}
+
+
+def expmv_bound(a, b, t, bound):
+    """exp(tA)B by the matrix-free Expmv (mu = 0, the caller's bound on
+    ||A||_1, no estimator), A applied as a dense operator. Returns (result, info dict)."""
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+    dt = np.complex128 if cplx else np.float64
+    a, b = _f(a, dt), _f(b, dt)
+    n, c = b.shape
+    out = np.zeros((n, c), dtype=dt, order="F")
+    info = ExpmvInfo()
+    fn = lib().orc_zexpmv_bound if cplx else lib().orc_dexpmv_bound
+    rc = fn(n, _p(a), _ld(a), c, _p(b), _ld(b), float(t), float(bound), _p(out), _ld(out), C.byref(info))
+    if rc == 8:
+        raise OverflowError("||tA|| too large for the exponential action")
+    assert rc == 0
+    return out, {k: getattr(info, k) for k, _ in ExpmvInfo._fields_}
 
 
 def expmv(a, b, t=1.0):

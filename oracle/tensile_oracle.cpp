@@ -1636,6 +1636,68 @@ int expmv_dense(int n, const typename K::T* a, int lda, int ncols, const typenam
     return 0;
 }
 
+// The matrix-free Expmv (MatrixExponentialAction.Expmv(ILinearOperator<T>, B, t,
+// oneNormBound), src/Tensile/MatrixExponentialAction.cs:203-230 and
+// .Complex.cs:85-111): no trace, so mu = 0; the caller's bound on ||A||_1; no
+// estimator, so the crude bound over every degree (alpha null in
+// SelectParameters, :347-398); then Run (:239-320) with op.Apply. The
+// operator here is a dense A applied as DenseMatrixOperator does.
+template <typename K>
+int expmv_matrix_free(int n, const typename K::T* a, int lda, int ncols, const typename K::T* b, int ldb, double t,
+                      double bound, typename K::T* out, int ldo, orc_expmv_info* info) {
+    using T = typename K::T;
+    orc_expmv_info local{};
+    if (!info) info = &local;
+    *info = orc_expmv_info{};
+    if (n == 0 || ncols == 0) {
+        for (int j = 0; j < ncols; j++)
+            for (int i = 0; i < n; i++) out[(size_t)j * ldo + i] = b[(size_t)j * ldb + i];
+        return 0;
+    }
+    Mat<K> am(n);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++) am.at(i, j) = a[(size_t)j * lda + i];
+    double scale = std::fabs(t);
+    double scaled_norm = scale * bound;
+    int m, s;
+    if (scaled_norm == 0.0) {
+        m = 0;
+        s = 1;
+    } else {
+        auto no_alpha = [](int) { return 0.0; };
+        int rc = select_parameters(scaled_norm, false, no_alpha, scale, ncols, &m, &s);
+        if (rc) return rc;
+    }
+    info->degree = m;
+    info->scaling = s;
+    size_t ext = (size_t)n * ncols;
+    std::vector<T> f(ext), work(ext), next(ext);
+    for (int j = 0; j < ncols; j++)
+        for (int i = 0; i < n; i++) f[(size_t)j * n + i] = work[(size_t)j * n + i] = b[(size_t)j * ldb + i];
+    typename std::conditional<std::is_same_v<T, double>, DenseRealOperator, DenseComplexOperator>::type op(
+        n, am.p(), n, 1);
+    for (int i = 0; i < s; i++) {
+        double c1 = K::inf_norm(n, ncols, work.data(), n);
+        for (int j = 0; j < m; j++) {
+            double coefficient = t / (s * (double)(j + 1));
+            op.apply(work.data(), next.data(), ncols);
+            for (size_t q = 0; q < ext; q++) work[q] = K::scale(next[q], coefficient);
+            double c2 = K::inf_norm(n, ncols, work.data(), n);
+            for (size_t q = 0; q < ext; q++) f[q] = K::add(f[q], work[q]);
+            info->applications++;
+            if (c1 + c2 <= UnitRoundoff * K::inf_norm(n, ncols, f.data(), n)) {
+                info->early_exits++;
+                break;
+            }
+            c1 = c2;
+        }
+        work = f;  // eta = exp(0) = 1: no scaling
+    }
+    for (int j = 0; j < ncols; j++)
+        for (int i = 0; i < n; i++) out[(size_t)j * ldo + i] = f[(size_t)j * n + i];
+    return 0;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1771,6 +1833,15 @@ int orc_dexpm(int n, const double* a, int lda, double* out, int ldo, orc_expm_in
 }
 int orc_zexpm(int n, const double* a, int lda, double* out, int ldo, orc_expm_info* info) {
     return expm<ComplexK>(n, (const cplx*)a, lda, (cplx*)out, ldo, info);
+}
+int orc_dexpmv_bound(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t, double bound,
+                     double* out, int ldo, orc_expmv_info* info) {
+    return expmv_matrix_free<RealK>(n, a, lda, ncols, b, ldb, t, bound, out, ldo, info);
+}
+int orc_zexpmv_bound(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t, double bound,
+                     double* out, int ldo, orc_expmv_info* info) {
+    return expmv_matrix_free<ComplexK>(n, (const cplx*)a, lda, ncols, (const cplx*)b, ldb, t, bound, (cplx*)out, ldo,
+                                       info);
 }
 int orc_dexpmv(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
                double* out, int ldo, orc_expmv_info* info) {

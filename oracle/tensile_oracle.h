@@ -103,6 +103,12 @@ typedef struct {
 
 int orc_dexpm(int n, const double* a, int lda, double* out, int ldo, orc_expm_info* info);
 int orc_zexpm(int n, const double* a, int lda, double* out, int ldo, orc_expm_info* info);
+/* Matrix-free Expmv: mu = 0, the caller's bound on ||A||_1, no estimator
+ * (MatrixExponentialAction.cs:203-230, .Complex.cs:85-111); A applied densely. */
+int orc_dexpmv_bound(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t, double bound,
+                     double* out, int ldo, orc_expmv_info* info);
+int orc_zexpmv_bound(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t, double bound,
+                     double* out, int ldo, orc_expmv_info* info);
 int orc_dexpmv(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
                double* out, int ldo, orc_expmv_info* info);
 int orc_zexpmv(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,

@@ -298,3 +298,18 @@ def test_gemm_is_thread_count_invariant(orc):
     orc.set_threads(0)
     c2 = orc.gemm(a, b)
     assert np.array_equal(c1, c2)
+
+
+@pytest.mark.parametrize("norm,t", [(0.05, 1.0), (3.0, 0.5), (40.0, 1.0), (40.0, -1.0)])
+def test_matrix_free_expmv_oracle(orc, norm, t):
+    """The oracle's matrix-free Expmv (mu = 0, crude bound, no estimator;
+    MatrixExponentialAction.cs:203-230) against scipy's expm(tA) B."""
+    import scipy.linalg
+    rng = np.random.default_rng(int(norm * 10))
+    a = rng.standard_normal((50, 50))
+    a *= norm / np.abs(a).sum(axis=0).max()
+    b = rng.standard_normal((50, 4))
+    r, info = orc.expmv_bound(a, b, t, np.abs(a).sum(axis=0).max())
+    ref = scipy.linalg.expm(t * a) @ b
+    assert np.abs(r - ref).sum(axis=0).max() / max(np.abs(ref).sum(axis=0).max(), 1.0) <= 1e-12
+    assert info["degree"] > 0 and info["scaling"] >= 1
