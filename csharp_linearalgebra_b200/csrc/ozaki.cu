@@ -279,9 +279,11 @@ struct RowDigits {
     __device__ __forceinline__ void residues(int nm, Store store) const {
         const float2 magic = make_float2(kRoundMagicF, kRoundMagicF);
         const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
-#pragma unroll
-        for (int q = 0; q < kMaxModuli; ++q) {
-            if (q >= nm) break;
+        // One modulus per trip (not unrolled over the moduli: the unrolled
+        // body outgrew the instruction cache); the constants are uniform
+        // constant-bank loads.
+#pragma unroll 1
+        for (int q = 0; q < nm; ++q) {
             uint32_t b[16];
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
