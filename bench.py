@@ -262,6 +262,7 @@ def ours(args, world, rank, local, dist):
 
     ws = Workspace(local)
     ws.set_workers(args.groups)
+    ws.set_autotune(bool(args.autotune))
     stream = torch.cuda.ExternalStream(ws.stream)
 
     def barrier():
@@ -397,7 +398,7 @@ def ours(args, world, rank, local, dist):
             "dtype": f"f64 results; Pade/squaring products from int8 residues modulo {args.moduli} moduli "
                      "(exact int32 sums, CRT reconstruction in f64); decisions, LU and solve in f64",
             "data": "synthetic, seeded",
-            "config": {"workload": WORKLOAD, "count": count, "seed": args.seed,
+            "config": {"workload": WORKLOAD, "count": count, "seed": args.seed, "autotune": bool(args.autotune),
                        "form": f"split precision, {args.moduli} moduli (tcgen05 kind::i8, Chinese remainder "
                                "reconstruction) for the Pade-evaluation and squaring products; A^2, A^4, A^6, norms, "
                                "normest1, LU and the Pade solve in plain FP64",
@@ -460,6 +461,7 @@ def main():
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     p.add_argument("--no-peak", action="store_true", help="skip the measured FP64/INT8 peaks (profiling runs)")
     p.add_argument("--moduli", type=int, default=20, help="moduli of the split-precision form (8..22)")
+    p.add_argument("--autotune", type=int, default=0, help="1: GEMM launch shapes chosen by timing (tns_set_autotune)")
     args = p.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:

@@ -448,6 +448,11 @@ class Workspace:
         d = {k: getattr(info, k) for k, _ in N.MixedInfo._fields_}
         return (x[:, 0] if vec else x), d
 
+    def set_autotune(self, enabled: bool):
+        """Choose the GEMMs' launch shapes by timing them on each size class's
+        first launch (identical results either way)."""
+        self._call("tns_set_autotune", int(bool(enabled)))
+
     def set_checkpoint_bytes(self, nbytes: int):
         """Device bytes the Frechet derivative may hold for its squarings (-1: automatic)."""
         self._call("tns_set_checkpoint_bytes", int(nbytes))

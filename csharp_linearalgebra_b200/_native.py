@@ -52,7 +52,7 @@ class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
                 ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double),
                 ("split_launches", C.c_longlong), ("split_flops", C.c_double), ("split_int8_ops", C.c_double),
-                ("split_ms", C.c_double), ("split_bytes", C.c_double)]
+                ("split_ms", C.c_double), ("split_bytes", C.c_double), ("autotune_trials", C.c_longlong)]
 
 
 # y := A x on device panels: (user, ncols, x, y, ld, stream) -> status
@@ -95,6 +95,7 @@ SIGNATURES = {
     "tns_zexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
                                  C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
     "tns_set_checkpoint_bytes": (_I, [_P, _LL]),
+    "tns_set_autotune": (_I, [_P, _I]),
     "tns_dexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_dgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),

@@ -472,6 +472,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             wc.max_elements = ctx.max_elements;
             wc.timing = ctx.timing;
             wc.split_moduli = ctx.split_moduli;
+            wc.autotune = ctx.autotune;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
                 run_group(wc, groups[w]);
@@ -521,6 +522,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
     out->split_int8_ops = ctx.split_int8_ops;
     out->split_ms = ctx.split_ms_done;
     out->split_bytes = ctx.split_bytes;
+    out->autotune_trials = ctx.autotune_trials;
     for (auto& w : ctx.workers) {
         w->drain_events();
         out->kernel_launches += w->kernel_launches;
@@ -533,6 +535,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
         out->split_int8_ops += w->split_int8_ops;
         out->split_ms += w->split_ms_done;
         out->split_bytes += w->split_bytes;
+        out->autotune_trials += w->autotune_trials;
     }
 }
 
@@ -542,12 +545,14 @@ void reset_stats(Context& ctx) {
     ctx.gemm_flops = ctx.gemm_ms_done = ctx.gemm_bytes = 0.0;
     ctx.split_launches = 0;
     ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = ctx.split_bytes = 0.0;
+    ctx.autotune_trials = 0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
         w->gemm_flops = w->gemm_ms_done = w->gemm_bytes = 0.0;
         w->split_launches = 0;
         w->split_flops = w->split_int8_ops = w->split_ms_done = w->split_bytes = 0.0;
+        w->autotune_trials = 0;
     }
 }
 
@@ -717,6 +722,12 @@ int tns_dgesv_mixed(tns_context* c, int n, int nrhs, const double* a, int lda, c
 int tns_zgesv_mixed(tns_context* c, int n, int nrhs, const double* a, int lda, const double* b, int ldb, double* x,
                     int ldx, int moduli, int max_iter, tns_mixed_info* info) {
     return gesv_mixed_entry(c, true, n, nrhs, a, lda, b, ldb, x, ldx, moduli, max_iter, info);
+}
+int tns_set_autotune(tns_context* c, int enabled) {
+    return guarded(c, [&](Context& ctx) {
+        ctx.autotune = enabled != 0;
+        for (auto& w : ctx.workers) w->autotune = ctx.autotune;
+    });
 }
 int tns_set_checkpoint_bytes(tns_context* c, long long bytes) {
     return guarded(c, [&](Context& ctx) {

@@ -38,6 +38,7 @@
 
 #include "device_util.cuh"
 #include "tns_internal.h"
+#include "autotune.h"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -606,20 +607,35 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
     // Heaviest tiles (deepest K) first: CTAs take tiles in list order as they
     // free up, so the launch ends on light tiles.
     std::stable_sort(work.begin(), work.end(), [](const GemmProblem& x, const GemmProblem& y) { return x.K > y.K; });
-    // Big tiles only when they fill the machine.
-    if (cplx) {
-        long long tiles = 0;
-        for (auto& p : work)
-            tiles += (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN);
-        if (tiles >= ctx.num_sms) launch_cfg<CplxBig>(ctx, work);
-        else launch_cfg<CplxSmall>(ctx, work);
-    } else {
-        long long tiles = 0;
-        for (auto& p : work)
-            tiles += (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
-        if (tiles >= ctx.num_sms) launch_cfg<RealBig>(ctx, work);
-        else launch_cfg<RealSmall>(ctx, work);
+    // Big tiles only when they fill the machine, or as the autotuner found.
+    long long tiles = 0;
+    int depth = 0;
+    bool overwrite = true;  // every C is overwritten (beta = 0): a trial may run twice
+    for (auto& p : work) {
+        tiles += cplx ? (long long)((p.M + CplxBig::BM - 1) / CplxBig::BM) * ((p.N + CplxBig::BN - 1) / CplxBig::BN)
+                      : (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
+        depth = std::max(depth, p.K);
+        if (p.beta_re != 0.0 || p.beta_im != 0.0) overwrite = false;
     }
+    auto run = [&](int big) {
+        if (cplx) big ? launch_cfg<CplxBig>(ctx, work) : launch_cfg<CplxSmall>(ctx, work);
+        else big ? launch_cfg<RealBig>(ctx, work) : launch_cfg<RealSmall>(ctx, work);
+    };
+    int variant = tiles >= ctx.num_sms ? 1 : 0;
+    if (ctx.autotune) {
+        const TuneKind kind = cplx ? TuneKind::kDmmaComplex : TuneKind::kDmmaReal;
+        const int known = tuned_variant(ctx.device, kind, tiles, depth);
+        if (known >= 0) {
+            variant = known;
+        } else if (overwrite) {
+            const float small = time_launches(ctx, [&] { run(0); });
+            const float big = time_launches(ctx, [&] { run(1); });  // the same values again
+            record_variant(ctx.device, kind, tiles, depth, big <= small ? 1 : 0);
+            ctx.autotune_trials++;
+            return;
+        }
+    }
+    run(variant);
 }
 
 void gemm(Context& ctx, const GemmProblem& p, bool cplx) {

@@ -49,6 +49,7 @@
 #include "device_util.cuh"
 #include "tcgen05.cuh"
 #include "tns_internal.h"
+#include "autotune.h"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -792,10 +793,17 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         total += (bytes + 255) & ~size_t(255);
         return off;
     };
-    // 256-column tiles when they fill the GPU.
-    long long tiles_wide = 0;
-    for (auto& p : v) tiles_wide += (long long)((p.a->rows + kTile - 1) / kTile) * ((DPE * p.b->cols + 255) / 256);
-    const int tn = tiles_wide >= ctx.num_sms ? 256 : 128;
+    // 256-column tiles when they fill the GPU, or as the autotuner found; a
+    // trial lays out for 256 and runs both widths over the same residues.
+    long long tiles_wide = 0, depth = 0;
+    for (auto& p : v) {
+        tiles_wide += (long long)((p.a->rows + kTile - 1) / kTile) * ((DPE * p.b->cols + 255) / 256);
+        depth = std::max<long long>(depth, round_up(CPLX ? 2 * round_up(p.a->cols, 16) : p.a->cols, kKb));
+    }
+    const TuneKind tune_kind = CPLX ? TuneKind::kSplitComplex : TuneKind::kSplitReal;
+    const int known = ctx.autotune ? tuned_variant(ctx.device, tune_kind, tiles_wide, depth) : -1;
+    const bool trial = ctx.autotune && known < 0;
+    const int tn = trial ? 256 : known >= 0 ? (known ? 256 : 128) : (tiles_wide >= ctx.num_sms ? 256 : 128);
     int kmax = 1;
     for (auto& p : v) {
         Sizes s{};
@@ -827,9 +835,11 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
     std::vector<ModDesc> md;
     std::vector<CrtDesc> cd;
     std::vector<ModMaps> maps(v.size());
+    std::vector<ModDesc> md_narrow;              // a trial's 128-column tiles over the same layout
+    std::vector<ModMaps> maps_narrow(trial ? v.size() : 0);
     int max_m = 0, max_cols = 0, max_rows_a = 0, max_chunks = 0, max_out_rows = 0, max_out_cols = 0;
     long long max_b_threads = 0;
-    int tiles = 0;
+    int tiles = 0, tiles_narrow = 0;
     for (size_t q = 0; q < v.size(); ++q) {
         const auto& p = v[q];
         const auto& s = z[q];
@@ -847,6 +857,12 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         tiles += (s.mp / kTile) * (s.np / tn);
         encode_residues(&maps[q].a, a8, s.kp, s.mp, nm, kTile);
         encode_residues(&maps[q].b, b8, s.kp, s.np, nm, tn);
+        if (trial) {
+            md_narrow.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles_narrow, u8});
+            tiles_narrow += (s.mp / kTile) * (s.np / 128);
+            maps_narrow[q].a = maps[q].a;
+            encode_residues(&maps_narrow[q].b, b8, s.kp, s.np, nm, 128);
+        }
         max_m = std::max(max_m, s.m);
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
@@ -886,17 +902,35 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         e1 = ctx.take_event();
         TNS_CUDA(cudaEventRecord(e0, ctx.stream));
     }
-    auto launch = [&](auto kernel, int smem_bytes, bool& configured) {
+    auto launch = [&](auto kernel, int smem_bytes, bool& configured, const ModDesc* descs, const ModMaps* mps,
+                      int ntiles) {
         if (!configured) {
             TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
             configured = true;
         }
-        kernel<<<tiles, kSplitThreads, smem_bytes, ctx.stream>>>(d_desc, d_maps, (int)md.size(), cp, ctx.d_err);
+        kernel<<<ntiles, kSplitThreads, smem_bytes, ctx.stream>>>(descs, mps, (int)md.size(), cp, ctx.d_err);
         TNS_CUDA(cudaGetLastError());
     };
     static bool configured_wide[64] = {}, configured_narrow[64] = {};
-    if (tn == 256) launch(modular_gemm_kernel<256>, split_smem<256>(), configured_wide[ctx.device]);
-    else launch(modular_gemm_kernel<128>, split_smem<128>(), configured_narrow[ctx.device]);
+    if (trial) {
+        // Both widths over the same residues; each writes the same byte planes.
+        const ModDesc* nd = static_cast<const ModDesc*>(ctx.upload(md_narrow.data(), sizeof(ModDesc) * md_narrow.size()));
+        const ModMaps* nmaps =
+            static_cast<const ModMaps*>(ctx.upload(maps_narrow.data(), sizeof(ModMaps) * maps_narrow.size()));
+        const float narrow = time_launches(ctx, [&] {
+            launch(modular_gemm_kernel<128>, split_smem<128>(), configured_narrow[ctx.device], nd, nmaps, tiles_narrow);
+        });
+        const float wide = time_launches(ctx, [&] {
+            launch(modular_gemm_kernel<256>, split_smem<256>(), configured_wide[ctx.device], d_desc, d_maps, tiles);
+        });
+        record_variant(ctx.device, tune_kind, tiles_wide, depth, wide <= narrow ? 1 : 0);
+        ctx.autotune_trials++;
+        ctx.kernel_launches++;
+    } else if (tn == 256) {
+        launch(modular_gemm_kernel<256>, split_smem<256>(), configured_wide[ctx.device], d_desc, d_maps, tiles);
+    } else {
+        launch(modular_gemm_kernel<128>, split_smem<128>(), configured_narrow[ctx.device], d_desc, d_maps, tiles);
+    }
     if (ctx.timing) {
         TNS_CUDA(cudaEventRecord(e1, ctx.stream));
         ctx.split_events.emplace_back(e0, e1);

@@ -97,6 +97,10 @@ struct Context {
     // of its forward pass (else it keeps X_0 and squares again); -1: a quarter
     // of the free device memory.
     long long checkpoint_bytes = -1;
+    // Launch shapes of the GEMMs chosen by timing both on a size class's
+    // first launch (autotune.h) instead of the fixed rule.
+    bool autotune = false;
+    long long autotune_trials = 0;
     long long split_launches = 0;
     double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0, split_bytes = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;

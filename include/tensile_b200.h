@@ -101,6 +101,14 @@ int tns_zgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int 
  * and s remain the reference's, as do the LU and the solve of the Pade
  * denominator. */
 int tns_set_split_moduli(tns_context* ctx, int moduli);
+/* 1: the GEMMs' launch shapes (the DMMA GEMM's small or big tiles, the
+ * modular GEMM's 128- or 256-column tiles) are chosen by timing both on the
+ * first launch of each size class (product kind, log2 of its tiles, log2 of its
+ * depth) and remembered per device for the process; the shapes give identical
+ * results, so only speed depends on the choice. A timed first launch of a
+ * class waits for the stream. 0 (the default): big tiles when they fill the
+ * GPU. No counterpart in the reference (its CPU blocking is fixed). */
+int tns_set_autotune(tns_context* ctx, int enabled);
 
 /* ---- exact norms -------------------------------------------------------- */
 
@@ -358,6 +366,8 @@ typedef struct {
      * residue images of A and B read once and its 8-bit result plane written
      * once, at the padded extents */
     double split_bytes;
+    /* size classes the autotuner timed (tns_set_autotune) */
+    long long autotune_trials;
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
