@@ -654,10 +654,26 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<
     const int i = r0 + lane;
     if (i >= d.m) return;
     const int ei = d.ea[i];
-    for (int jj = warp; jj < 32; jj += 8) {
+    // The four columns' exponents and (when accumulating) old C entries are
+    // loaded before the digit sums, so their latency overlaps the arithmetic.
+    int sc4[4];
+    double2 old4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int j = j0 + warp + 8 * u;
+        sc4[u] = j < d.n ? ei + d.eb[j] - 2 * cp.t : 0;
+        old4[u] = make_double2(0.0, 0.0);
+        if (d.accumulate && j < d.n) {
+            if (CPLX) old4[u] = reinterpret_cast<const double2*>(d.c)[(size_t)j * d.ldc + i];
+            else old4[u].x = d.c[(size_t)j * d.ldc + i];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int jj = warp + 8 * u;
         const int j = j0 + jj;
         if (j >= d.n) break;
-        const int sc = ei + d.eb[j] - 2 * cp.t;
+        const int sc = sc4[u];
         double a1 = 0.0, a2 = 0.0, a3 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
         for (int q = 0; q < nm; ++q) {
             double ur, ui = 0.0;
@@ -682,14 +698,11 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<
             const double im = scalbn(from_digit_sums(b1, b2, b3, cp), sc);
             double2* p = reinterpret_cast<double2*>(d.c) + (size_t)j * d.ldc + i;
             double2 r = make_double2(re, im);
-            if (d.accumulate) {
-                const double2 o = *p;
-                r = make_double2(o.x + r.x, o.y + r.y);
-            }
+            if (d.accumulate) r = make_double2(old4[u].x + r.x, old4[u].y + r.y);
             *p = r;
         } else {
             double* p = d.c + (size_t)j * d.ldc + i;
-            *p = d.accumulate ? *p + re : re;
+            *p = d.accumulate ? old4[u].x + re : re;
         }
     }
 }
