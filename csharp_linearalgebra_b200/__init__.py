@@ -292,6 +292,35 @@ class Workspace:
                    int(power), int(columns), int(max_iterations), int(seed), C.byref(out))
         return NormEstimateResult(out.value, out.iterations, out.products)
 
+    def estimate_operator_norm(self, apply, adjoint, n: int, complex_: bool = False,
+                               columns: int = DEFAULT_COLUMNS, max_iterations: int = DEFAULT_MAX_ITERATIONS,
+                               seed: int = DEFAULT_SEED) -> NormEstimateResult:
+        """NormEstimate.Of(IAdjointOperator<T>, ...) for a matrix-free operator:
+        apply(x_ptr, y_ptr, ncols, ld, stream) writes y := A x and
+        adjoint(...) writes y := A^H x on device panels."""
+        failure = []
+
+        def wrap(fn):
+            def trampoline(user, ncols, x, y, ld, stream):
+                try:
+                    fn(x, y, ncols, ld, stream)
+                    return 0
+                except BaseException as e:  # reported as TNS_E_OPERATOR, then re-raised below
+                    failure.append(e)
+                    return 1
+            return N.APPLY_FN(trampoline)
+
+        ap, ad = wrap(apply), wrap(adjoint)
+        out = N.NormestResult()
+        try:
+            self._call("tns_znormest1_operator" if complex_ else "tns_dnormest1_operator", int(n), ap, ad, None,
+                       int(columns), int(max_iterations), int(seed), C.byref(out))
+        except Exception:
+            if failure:
+                raise failure[0]
+            raise
+        return NormEstimateResult(out.value, out.iterations, out.products)
+
     # -- exponentials -------------------------------------------------------
     def expm(self, a, diagnostics: ExpmDiagnostics | None = None):
         """exp(A) (MatrixExponential.Expm)."""

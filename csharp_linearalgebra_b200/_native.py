@@ -96,6 +96,8 @@ SIGNATURES = {
                                  C.POINTER(_D), _P, _I, C.POINTER(ExpmInfo)]),
     "tns_set_checkpoint_bytes": (_I, [_P, _LL]),
     "tns_set_autotune": (_I, [_P, _I]),
+    "tns_dnormest1_operator": (_I, [_P, _I, APPLY_FN, APPLY_FN, _P, _I, _I, _I, C.POINTER(NormestResult)]),
+    "tns_znormest1_operator": (_I, [_P, _I, APPLY_FN, APPLY_FN, _P, _I, _I, _I, C.POINTER(NormestResult)]),
     "tns_dexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv_operator": (_I, [_P, _I, APPLY_FN, _P, _I, _P, _I, _D, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_dgesv_mixed": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I, C.POINTER(MixedInfo)]),

@@ -79,6 +79,33 @@ struct LuInverseProbe : Probe<TE> {
     }
 };
 
+// A caller's operator (IAdjointOperator<T>, src/Tensile/LinearOperators.cs:37-75):
+// the probe panel goes to the device, the caller's apply or adjoint callback
+// writes the result there on the context's stream, and it comes back.
+template <class TE>
+struct OperatorProbe : Probe<TE> {
+    Context& ctx;
+    int n;
+    ApplyFn apply_fn, adjoint_fn;
+    void* user;
+    DMat x, y;
+    OperatorProbe(Context& c, int n_, ApplyFn ap, ApplyFn adj, void* u, int t)
+        : ctx(c), n(n_), apply_fn(ap), adjoint_fn(adj), user(u), x(c, n_, t, TE::kDoubles == 2, "an estimator probe panel"),
+          y(c, n_, t, TE::kDoubles == 2, "an estimator probe panel") {}
+    void apply(const typename TE::T* xs, typename TE::T* ys, int t, bool adjoint) override {
+        const size_t esz = sizeof(double) * TE::kDoubles;
+        TNS_CUDA(cudaMemcpy2DAsync(x.p, (size_t)x.ld() * esz, xs, (size_t)n * esz, (size_t)n * esz, t,
+                                   cudaMemcpyHostToDevice, ctx.stream));
+        const int rc = (adjoint ? adjoint_fn : apply_fn)(user, t, x.p, y.p, x.ld(), ctx.stream);
+        if (rc != 0)
+            fail(TNS_E_OPERATOR, std::string("the operator's ") + (adjoint ? "adjoint" : "apply") +
+                                     " callback returned " + std::to_string(rc));
+        TNS_CUDA(cudaMemcpy2DAsync(ys, (size_t)n * esz, y.p, (size_t)y.ld() * esz, (size_t)n * esz, t,
+                                   cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+    }
+};
+
 // Drive one estimator to completion through a probe (NormEstimate.Estimate).
 template <class TE>
 NormestResult estimate(Probe<TE>& op, int n, int columns, int max_iterations, int seed) {
@@ -122,6 +149,18 @@ NormestResult normest_power(Context& ctx, const DMat& a, int power, int t, int i
         return estimate<CplxE>(op, n, t, itmax, seed);
     }
     PowerProbe<RealE> op(ctx, a, power, tt);
+    return estimate<RealE>(op, n, t, itmax, seed);
+}
+
+NormestResult normest_operator(Context& ctx, int n, bool cplx, ApplyFn apply, ApplyFn adjoint, void* user, int t,
+                               int itmax, int seed) {
+    if (n == 0) return {};
+    int tt = std::clamp(t, 1, n);
+    if (cplx) {
+        OperatorProbe<CplxE> op(ctx, n, apply, adjoint, user, tt);
+        return estimate<CplxE>(op, n, t, itmax, seed);
+    }
+    OperatorProbe<RealE> op(ctx, n, apply, adjoint, user, tt);
     return estimate<RealE>(op, n, t, itmax, seed);
 }
 

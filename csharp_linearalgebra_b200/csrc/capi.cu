@@ -375,6 +375,23 @@ int gesv_mixed_entry(tns_context* c, bool cplx, int n, int nrhs, const double* a
     });
 }
 
+int normest_operator_entry(tns_context* c, bool cplx, int n, tns_apply_fn apply, tns_apply_fn adjoint, void* user,
+                           int t, int itmax, int seed, tns_normest_result* out) {
+    return guarded(c, [&](Context& ctx) {
+        require(apply != nullptr && adjoint != nullptr, TNS_E_NULL, "The operator is null.");
+        require(out != nullptr, TNS_E_NULL, "out is null");
+        require(n >= 0, TNS_E_ARGUMENT, "negative order");
+        *out = tns_normest_result{0.0, 0, 0};
+        if (n == 0) return;
+        require((long long)n * std::clamp(t, 1, n) <= 2147483647LL, TNS_E_OUT_OF_RANGE, "probe panel too large");
+        ctx.check_limit((long long)n * std::clamp(t, 1, n), "an estimator probe panel");
+        tns::NormestResult r = tns::normest_operator(ctx, n, cplx, apply, adjoint, user, t, itmax, seed);
+        out->value = r.value;
+        out->iterations = r.iterations;
+        out->products = r.products;
+    });
+}
+
 int expmv_operator_entry(tns_context* c, bool cplx, int n, tns_apply_fn apply, void* user, int ncols,
                          const double* b, int ldb, double t, double bound, double* out, int ldo, tns_expmv_info* info) {
     return guarded(c, [&](Context& ctx) {
@@ -706,6 +723,14 @@ int tns_zexpmv_gradient(tns_context* c, int n, int ncols, double t, const double
                         int ldgb, double* grad_t, double* f, int ldf, tns_expm_info* info) {
     return gradient_entry(c, true, n, ncols, t, a, lda, b, ldb, y, ldy, loss, grad_a, ldga, grad_b, ldgb, grad_t, f,
                           ldf, info);
+}
+int tns_dnormest1_operator(tns_context* c, int n, tns_apply_fn apply, tns_apply_fn adjoint, void* user, int t,
+                           int itmax, int seed, tns_normest_result* out) {
+    return normest_operator_entry(c, false, n, apply, adjoint, user, t, itmax, seed, out);
+}
+int tns_znormest1_operator(tns_context* c, int n, tns_apply_fn apply, tns_apply_fn adjoint, void* user, int t,
+                           int itmax, int seed, tns_normest_result* out) {
+    return normest_operator_entry(c, true, n, apply, adjoint, user, t, itmax, seed, out);
 }
 int tns_dexpmv_operator(tns_context* c, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
                         double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info) {

@@ -329,6 +329,9 @@ void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, E
 using ApplyFn = int (*)(void* user, int ncols, const double* x, double* y, int ld, void* stream);
 void expmv_operator(Context& ctx, int n, ApplyFn apply, void* user, const DMat& b, double t, double bound,
                     DMat& result, ExpmvInfo* info);
+// normest1 of a caller's operator, through its apply and adjoint callbacks.
+NormestResult normest_operator(Context& ctx, int n, bool cplx, ApplyFn apply, ApplyFn adjoint, void* user, int t,
+                               int itmax, int seed);
 
 // ---- Frechet derivative and adjoint (frechet.cu) -----------------------------
 // exp(a) and, for a direction e, L(a, e) = d/dh exp(a + h e) at h = 0.

@@ -313,6 +313,18 @@ int tns_dexpmv_operator(tns_context* ctx, int n, tns_apply_fn apply, void* user,
 int tns_zexpmv_operator(tns_context* ctx, int n, tns_apply_fn apply, void* user, int ncols, const double* b, int ldb,
                         double t, double one_norm_bound, double* out, int ldo, tns_expmv_info* info);
 
+/* NormEstimate.Of(IAdjointOperator<T>, columns, maxIterations, seed)
+ * (src/Tensile/NormEstimate.cs:70-93, the estimator :104-274) for a caller's
+ * operator: `apply` writes y := A x and `adjoint` writes y := A^H x, both as
+ * tns_apply_fn on device panels (n x t). The estimator's bookkeeping is the
+ * reference's. When the operator's products are exact, the estimate, iteration
+ * count and product count equal the reference's exactly. apply or adjoint
+ * NULL: TNS_E_NULL; a callback's failure: TNS_E_OPERATOR. */
+int tns_dnormest1_operator(tns_context* ctx, int n, tns_apply_fn apply, tns_apply_fn adjoint, void* user, int t,
+                           int itmax, int seed, tns_normest_result* out);
+int tns_znormest1_operator(tns_context* ctx, int n, tns_apply_fn apply, tns_apply_fn adjoint, void* user, int t,
+                           int itmax, int seed, tns_normest_result* out);
+
 /* ---- complex product without allocation -------------------------------- */
 
 /* No counterpart in the reference: the reference's products run on the CPU

@@ -82,3 +82,38 @@ def test_operator_failure_and_bad_bound(ws):
         ws.expmv_operator(broken, 10, b, 1.0, -1.0)
     # the workspace stays usable
     assert rel1(ws.expmv_operator(dense_operator(np.zeros((10, 10))), 10, b, 1.0, 0.0), b) == 0.0
+
+
+def adjoint_pair(a):
+    """apply and adjoint callbacks of a dense A (torch on the library's stream)."""
+    cplx = np.iscomplexobj(a)
+    n = a.shape[0]
+    at = torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+    def make(mat):
+        def fn(x, y, ncols, ld, stream):
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                xv = torch.as_tensor(Panel(x, ncols, ld, cplx), device="cuda")
+                yv = torch.as_tensor(Panel(y, ncols, ld, cplx), device="cuda")
+                yv[:, :n] = xv[:, :n] @ mat.T
+        return fn
+    return make(at), make(at.conj().T.contiguous())
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("n", [64, 128])
+def test_operator_normest_matches_oracle(ws, orc, cplx, n):
+    """Small-integer entries and the estimator's probes (1/n, +-1, unit
+    vectors) make every product exact in any summation order, so the estimate,
+    iterations and products equal the oracle's exactly."""
+    rng = np.random.default_rng(n + 5 * cplx)
+    a = rng.integers(-5, 6, (n, n)).astype(float)
+    if cplx:
+        a = a + 1j * rng.integers(-5, 6, (n, n))
+    a = np.asfortranarray(a)
+    apply, adjoint = adjoint_pair(a)
+    got = ws.estimate_operator_norm(apply, adjoint, n, complex_=cplx)
+    ref = orc.normest_power(a, 1)
+    exact = np.abs(a).sum(axis=0).max()
+    assert got.value <= exact * (1 + 1e-15)
+    assert (got.value, got.iterations, got.products) == ref
