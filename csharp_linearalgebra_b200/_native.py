@@ -52,7 +52,8 @@ class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("gemm_launches", C.c_longlong),
                 ("gemm_flops", C.c_double), ("gemm_ms", C.c_double), ("gemm_bytes", C.c_double),
                 ("split_launches", C.c_longlong), ("split_flops", C.c_double), ("split_int8_ops", C.c_double),
-                ("split_ms", C.c_double), ("split_bytes", C.c_double), ("autotune_trials", C.c_longlong)]
+                ("split_ms", C.c_double), ("split_bytes", C.c_double), ("autotune_trials", C.c_longlong),
+                ("exact_fallbacks", C.c_longlong)]
 
 
 # y := A x on device panels: (user, ncols, x, y, ld, stream) -> status

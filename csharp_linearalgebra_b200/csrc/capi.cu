@@ -540,6 +540,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
     out->split_ms = ctx.split_ms_done;
     out->split_bytes = ctx.split_bytes;
     out->autotune_trials = ctx.autotune_trials;
+    out->exact_fallbacks = ctx.exact_fallbacks;
     for (auto& w : ctx.workers) {
         w->drain_events();
         out->kernel_launches += w->kernel_launches;
@@ -553,6 +554,7 @@ void collect_stats(Context& ctx, tns_stats* out) {
         out->split_ms += w->split_ms_done;
         out->split_bytes += w->split_bytes;
         out->autotune_trials += w->autotune_trials;
+        out->exact_fallbacks += w->exact_fallbacks;
     }
 }
 
@@ -563,6 +565,7 @@ void reset_stats(Context& ctx) {
     ctx.split_launches = 0;
     ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = ctx.split_bytes = 0.0;
     ctx.autotune_trials = 0;
+    ctx.exact_fallbacks = 0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
@@ -570,6 +573,7 @@ void reset_stats(Context& ctx) {
         w->split_launches = 0;
         w->split_flops = w->split_int8_ops = w->split_ms_done = w->split_bytes = 0.0;
         w->autotune_trials = 0;
+        w->exact_fallbacks = 0;
     }
 }
 

@@ -56,7 +56,21 @@ struct Job {
     double d4 = 0, d6 = 0, d8 = 0, d10 = 0, eta1 = 0, eta3 = 0;
     int degree = 0, s = 0;
     DMat result;
+    // Split form: A^2, A^4, A^6 from the split product, with intervals that
+    // hold the reference's d4 and d6 (exact: the reference's own products).
+    bool exact = true;
+    double d4_lo = 0, d4_hi = 0, d6_lo = 0, d6_hi = 0;
 };
+
+// An interval [lo, hi] that holds a value the reference computes.
+struct Iv {
+    double lo, hi;
+};
+Iv point(double x) { return {x, x}; }
+Iv iv_max(Iv a, Iv b) { return {net::max(a.lo, b.lo), net::max(a.hi, b.hi)}; }
+Iv iv_min(Iv a, Iv b) { return {net::min(a.lo, b.lo), net::min(a.hi, b.hi)}; }
+// Whether x < theta has one answer over the whole interval.
+bool certain_below(Iv x, double theta) { return x.hi < theta || x.lo >= theta; }
 
 DMat like(Context& ctx, const DMat& a) { return DMat(ctx, a.rows, a.cols, a.cplx, "an exponential work matrix"); }
 
@@ -175,47 +189,100 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
         jobs[k].a = inputs[k];
         jobs[k].n = inputs[k]->rows;
     }
-    // A^2, A^4, A^6 (:190-192).
-    {
+    // A^2, A^4, A^6 (:190-192) and d4, d6 (:198-199). The split form takes
+    // the products from the split product and bounds the reference's d4 and
+    // d6 (below); the plain form computes them as the reference does.
+    auto powers = [&](std::vector<Job*>& js, Form form) {
         std::vector<std::pair<const DMat*, const DMat*>> ab;
         std::vector<DMat*> c;
-        for (auto& j : jobs) {
-            j.a2 = like(ctx, *j.a);
-            ab.push_back({j.a, j.a});
-            c.push_back(&j.a2);
+        for (auto* j : js) {
+            j->a2 = like(ctx, *j->a);
+            ab.push_back({j->a, j->a});
+            c.push_back(&j->a2);
         }
-        product_batch(ctx, ab, c, 0.0);
+        product_batch(ctx, ab, c, 0.0, form);
         ab.clear();
         c.clear();
-        for (auto& j : jobs) {
-            j.a4 = like(ctx, *j.a);
-            ab.push_back({&j.a2, &j.a2});
-            c.push_back(&j.a4);
+        for (auto* j : js) {
+            j->a4 = like(ctx, *j->a);
+            ab.push_back({&j->a2, &j->a2});
+            c.push_back(&j->a4);
         }
-        product_batch(ctx, ab, c, 0.0);
+        product_batch(ctx, ab, c, 0.0, form);
         ab.clear();
         c.clear();
-        for (auto& j : jobs) {
-            j.a6 = like(ctx, *j.a);
-            ab.push_back({&j.a2, &j.a4});
-            c.push_back(&j.a6);
+        for (auto* j : js) {
+            j->a6 = like(ctx, *j->a);
+            ab.push_back({&j->a2, &j->a4});
+            c.push_back(&j->a6);
         }
-        product_batch(ctx, ab, c, 0.0);
-    }
-    // d4, d6 exact (:198-199).
-    {
+        product_batch(ctx, ab, c, 0.0, form);
         std::vector<const DMat*> m4, m6;
-        for (auto& j : jobs) {
-            m4.push_back(&j.a4);
-            m6.push_back(&j.a6);
+        for (auto* j : js) {
+            m4.push_back(&j->a4);
+            m6.push_back(&j->a6);
         }
         std::vector<double> n4 = norm1_batch(ctx, m4), n6 = norm1_batch(ctx, m6);
-        for (size_t k = 0; k < cnt; ++k) {
-            jobs[k].d4 = std::pow(n4[k], 1.0 / 4.0);
-            jobs[k].d6 = std::pow(n6[k], 1.0 / 6.0);
-            jobs[k].eta1 = net::max(jobs[k].d4, jobs[k].d6);
+        for (size_t k = 0; k < js.size(); ++k) {
+            Job& j = *js[k];
+            j.d4 = std::pow(n4[k], 1.0 / 4.0);
+            j.d6 = std::pow(n6[k], 1.0 / 6.0);
+            j.eta1 = net::max(j.d4, j.d6);
+            j.exact = form == Form::kExact;
+            j.d4_lo = j.d4_hi = j.d4;
+            j.d6_lo = j.d6_hi = j.d6;
         }
-    }
+        if (form == Form::kExact) return;
+        // Bounds on |X_ref - X_split|_1 for X = A^2, A^4, A^6, where X_ref is
+        // the reference's FP64 product. An FP64 product deviates from the
+        // exact one by at most gamma_n |X||Y| entrywise in any summation
+        // order, 2 gamma_2n in modulus for the complex 4M product; with
+        // |(|X||Y|)|_1 <= |X|_1 |Y|_1 that is g |X|_1 |Y|_1 with g = 4 gamma_n
+        // covering both. The split product's own error, about n 2^-t of the
+        // same scale, is far inside; the 1-norms' own sums add g of the norm.
+        // The widths carry a further factor 2.
+        std::vector<const DMat*> m1, m2;
+        for (auto* j : js) {
+            m1.push_back(j->a);
+            m2.push_back(&j->a2);
+        }
+        std::vector<double> n1 = norm1_batch(ctx, m1), n2 = norm1_batch(ctx, m2);
+        for (size_t k = 0; k < js.size(); ++k) {
+            Job& j = *js[k];
+            const double un = (double)j.n * 1.1102230246251565e-16;
+            const double g = 4.0 * un / (1.0 - un);
+            const double a1 = n1[k], p2 = n2[k], p4 = n4[k], p6 = n6[k];
+            const double e2 = g * a1 * a1;
+            const double q2 = p2 + e2;
+            const double e4 = g * q2 * q2 + 2.0 * q2 * e2 + e2 * e2;
+            const double q4 = p4 + e4;
+            const double e6 = g * q2 * q4 + q2 * e4 + e2 * q4 + e2 * e4;
+            const double w4 = 2.0 * (e4 + g * p4), w6 = 2.0 * (e6 + g * p6);  // safety factor 2
+            j.d4_lo = std::pow(std::max(0.0, p4 - w4), 1.0 / 4.0);
+            j.d4_hi = std::pow(p4 + w4, 1.0 / 4.0);
+            j.d6_lo = std::pow(std::max(0.0, p6 - w6), 1.0 / 6.0);
+            j.d6_hi = std::pow(p6 + w6, 1.0 / 6.0);
+        }
+    };
+    std::vector<Job*> all;
+    for (auto& j : jobs) all.push_back(&j);
+    powers(all, ctx.split_moduli > 0 ? Form::kSplittable : Form::kExact);
+    // Jobs whose next decision could differ from the reference's on the
+    // intervals: their powers again, exactly (the reference's arithmetic).
+    auto make_exact = [&](std::vector<Job*>& js) {
+        if (js.empty()) return;
+        powers(js, Form::kExact);
+        for (auto* j : js)
+            if (j->d8 > 0.0 || j->degree == 0) j->eta3 = net::max(j->d6, j->d8);
+        ctx.exact_fallbacks += (long long)js.size();
+    };
+    auto eta1_iv = [](const Job& j) { return iv_max(Iv{j.d4_lo, j.d4_hi}, Iv{j.d6_lo, j.d6_hi}); };
+    auto settle_eta1 = [&](double theta) {
+        std::vector<Job*> js;
+        for (auto& j : jobs)
+            if (j.degree == 0 && !j.exact && !certain_below(eta1_iv(j), theta)) js.push_back(&j);
+        make_exact(js);
+    };
     // The low-degree ladder (:202-231), stage by stage over the undecided.
     auto stage_ell = [&](int m, auto&& eligible) {
         std::vector<Job*> js;
@@ -229,7 +296,9 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
         for (size_t k = 0; k < js.size(); ++k)
             if (e[k] == 0) js[k]->degree = m;
     };
+    settle_eta1(kTheta3);
     stage_ell(3, [](const Job& j) { return j.eta1 < kTheta3; });
+    settle_eta1(kTheta5);
     stage_ell(5, [](const Job& j) { return j.eta1 < kTheta5; });
     {
         std::vector<Job*> js;
@@ -245,7 +314,16 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
             js[k]->eta3 = net::max(js[k]->d6, js[k]->d8);
         }
     }
+    auto eta3_iv = [](const Job& j) { return iv_max(Iv{j.d6_lo, j.d6_hi}, point(j.d8)); };
+    auto settle_eta3 = [&](double theta) {
+        std::vector<Job*> js;
+        for (auto& j : jobs)
+            if (j.degree == 0 && !j.exact && !certain_below(eta3_iv(j), theta)) js.push_back(&j);
+        make_exact(js);
+    };
+    settle_eta3(kTheta7);
     stage_ell(7, [](const Job& j) { return j.eta3 < kTheta7; });
+    settle_eta3(kTheta9);
     stage_ell(9, [](const Job& j) { return j.eta3 < kTheta9; });
     // Degree 13: d10, eta5, s and the ell correction on the scaled matrix (:233-247).
     std::vector<Job*> top;
@@ -255,12 +333,26 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
         std::vector<const DMat*> mats;
         for (auto* j : top) mats.push_back(j->a);
         std::vector<double> e10 = power_norms(ctx, mats, 10);
+        for (size_t k = 0; k < top.size(); ++k) top[k]->d10 = std::pow(e10[k], 1.0 / 10.0);
+        {
+            // s = max(ceil(log2(eta5 / 4.25)), 0) is monotone in eta5: it is
+            // settled when both ends of eta5's interval give the same s.
+            auto s_of = [](double eta5) {
+                return eta5 == 0.0 ? 0 : std::max((int)std::ceil(std::log2(eta5 / kScalingThreshold)), 0);
+            };
+            std::vector<Job*> js;
+            for (auto* j : top) {
+                if (j->exact) continue;
+                const Iv e5 = iv_min(eta3_iv(*j), point(net::max(j->d8, j->d10)));
+                if (s_of(e5.lo) != s_of(e5.hi)) js.push_back(j);
+            }
+            make_exact(js);
+        }
         std::vector<DMat> scaled;
         std::vector<EwDesc> ew;
         scaled.reserve(top.size());
         for (size_t k = 0; k < top.size(); ++k) {
             Job& j = *top[k];
-            j.d10 = std::pow(e10[k], 1.0 / 10.0);
             double eta4 = net::max(j.d8, j.d10);
             double eta5 = net::min(j.eta3, eta4);
             j.s = eta5 == 0.0 ? 0 : std::max((int)std::ceil(std::log2(eta5 / kScalingThreshold)), 0);

@@ -101,6 +101,9 @@ struct Context {
     // first launch (autotune.h) instead of the fixed rule.
     bool autotune = false;
     long long autotune_trials = 0;
+    // Split form: matrices whose A^2, A^4, A^6 were recomputed in plain FP64
+    // because a decision was not settled on the split values' intervals.
+    long long exact_fallbacks = 0;
     long long split_launches = 0;
     double split_flops = 0.0, split_int8_ops = 0.0, split_ms_done = 0.0, split_bytes = 0.0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_events;

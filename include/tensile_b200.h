@@ -95,11 +95,14 @@ int tns_dgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int 
 int tns_zgemm_split(tns_context* ctx, int m, int n, int k, const double* a, int lda, const double* b, int ldb,
                     double* c, int ldc, int moduli);
 /* 0 (the default): every product of Expm in plain FP64, the reference's
- * rounding. 8..22: Expm's Pade-evaluation and squaring products in the
- * split-precision form with that many moduli; A^2, A^4, A^6 and every norm
- * estimate that selects the degree and s stay in plain FP64, so the degree
- * and s remain the reference's, as do the LU and the solve of the Pade
- * denominator. */
+ * rounding. 8..22: Expm's products in the split-precision form with that
+ * many moduli. The degree and s remain the reference's: the norm estimates
+ * that select them stay in plain FP64, and d4, d6 come from A^4, A^6 in the
+ * split form with bounds that hold the reference's values (its FP64
+ * rounding included); a matrix whose decision is not settled on those
+ * bounds has its A^2, A^4, A^6 recomputed as the reference computes them.
+ * The LU and the solve of the Pade denominator keep the reference's
+ * arithmetic. */
 int tns_set_split_moduli(tns_context* ctx, int moduli);
 /* 1: the GEMMs' launch shapes (the DMMA GEMM's small or big tiles, the
  * modular GEMM's 128- or 256-column tiles) are chosen by timing both on the
@@ -380,6 +383,9 @@ typedef struct {
     double split_bytes;
     /* size classes the autotuner timed (tns_set_autotune) */
     long long autotune_trials;
+    /* split form: matrices whose A^2, A^4, A^6 were recomputed in plain FP64
+     * because a degree or s decision was not settled on the split values */
+    long long exact_fallbacks;
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
