@@ -97,3 +97,28 @@ def test_plain_form_is_restored(ws, orc):
     ws.set_split_moduli(0)
     ref, _ = orc.expm(a)
     assert np.array_equal(ws.expm(a), ref)
+
+
+@pytest.mark.parametrize("theta", [1.495585217958292e-2, 2.539398330063230e-1])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_decision_on_a_threshold_takes_exact_powers(split_ws, orc, theta, cplx):
+    """A scaled so that eta1 = max(||A^4||^(1/4), ||A^6||^(1/6)) lies on a
+    degree threshold to within rounding: the split form cannot settle the
+    comparison on its bounds, recomputes A^2, A^4, A^6 as the reference does,
+    and takes the reference's degree and s."""
+    from csharp_linearalgebra_b200 import ExpmDiagnostics
+    rng = np.random.default_rng(int(theta * 1000) + cplx)
+    n = 60
+    a = rng.standard_normal((n, n)) + (1j * rng.standard_normal((n, n)) if cplx else 0)
+    a2 = a @ a
+    a4 = a2 @ a2
+    a6 = a2 @ a4
+    eta1 = max(np.abs(a4).sum(axis=0).max() ** 0.25, np.abs(a6).sum(axis=0).max() ** (1 / 6))
+    a = np.asfortranarray(a * (theta / eta1))
+    split_ws.reset_stats()
+    d = ExpmDiagnostics()
+    e = split_ws.expm(a, d)
+    ref, info = orc.expm(a)
+    assert split_ws.stats()["exact_fallbacks"] >= 1
+    assert (d.degree, d.squarings) == (info["degree"], info["squarings"])
+    assert rel1(e, ref) <= 1e-12
