@@ -94,6 +94,54 @@ __global__ void ew_kernel(const __grid_constant__ Batch<EwDesc> b) {
     }
 }
 
+// The Pade numerator's parts in one pass over the elements
+// (EvaluateDegree13 / EvaluateLowDegree, MatrixExponential.cs:284-360): each
+// element goes through exactly the Scaled / AddScaled / Identity steps of the
+// reference, in its order, so every rounding is the same; the scaled powers
+// B^2, B^4 are never stored.
+//   degree 13: B = f A, B6 = f^6 A^6 (kept for the products), and
+//     inner      = c13 B6 + c11 B4 + c9 B2
+//     w          = c1 I + c3 B2 + c5 B4 + c7 B6
+//     inner_even = c12 B6 + c10 B4 + c8 B2
+//     v          = c0 I + c2 B2 + c4 B4 + c6 B6
+//   degree 3..9: w = c1 I + c3 A2 (+ c5 A4 + c7 A6 + c9 A8), v likewise.
+__global__ void pade_assemble_kernel(const __grid_constant__ Batch<PadeDesc> bt) {
+    const PadeDesc& d = batch_item(bt, blockIdx.y);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const double* c = d.c;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < d.count; e += stride) {
+        const size_t el = d.cplx ? e / 2 : e;
+        const int i = (int)(el % d.rows_p), j = (int)(el / d.rows_p);
+        const bool diag = i == j && i < d.n && (!d.cplx || (e % 2 == 0));
+        if (d.degree == 13) {
+            const double x2 = mul_rn(d.a2[e], d.f2), x4 = mul_rn(d.a4[e], d.f4), x6 = mul_rn(d.a6[e], d.f6);
+            d.b[e] = mul_rn(d.a[e], d.f);
+            d.b6[e] = x6;
+            d.inner[e] = add_rn(add_rn(mul_rn(x6, c[13]), mul_rn(x4, c[11])), mul_rn(x2, c[9]));
+            d.w[e] = add_rn(add_rn(add_rn(diag ? c[1] : 0.0, mul_rn(x2, c[3])), mul_rn(x4, c[5])), mul_rn(x6, c[7]));
+            d.inner_even[e] = add_rn(add_rn(mul_rn(x6, c[12]), mul_rn(x4, c[10])), mul_rn(x2, c[8]));
+            d.v[e] = add_rn(add_rn(add_rn(diag ? c[0] : 0.0, mul_rn(x2, c[2])), mul_rn(x4, c[4])), mul_rn(x6, c[6]));
+        } else {
+            double w = add_rn(diag ? c[1] : 0.0, mul_rn(d.a2[e], c[3]));
+            double v = add_rn(diag ? c[0] : 0.0, mul_rn(d.a2[e], c[2]));
+            if (d.degree >= 5) {
+                w = add_rn(w, mul_rn(d.a4[e], c[5]));
+                v = add_rn(v, mul_rn(d.a4[e], c[4]));
+            }
+            if (d.degree >= 7) {
+                w = add_rn(w, mul_rn(d.a6[e], c[7]));
+                v = add_rn(v, mul_rn(d.a6[e], c[6]));
+            }
+            if (d.degree == 9) {
+                w = add_rn(w, mul_rn(d.a8[e], c[9]));
+                v = add_rn(v, mul_rn(d.a8[e], c[8]));
+            }
+            d.w[e] = w;
+            d.v[e] = v;
+        }
+    }
+}
+
 // ---- norms ------------------------------------------------------------------
 
 // One thread per column: sequential sum of moduli in row order.
@@ -437,6 +485,18 @@ void launch_panel(Context& ctx, std::vector<PanelDesc>& v, bool adjoint) {
 // ---------------------------------------------------------------------------
 // Batched host entry points
 // ---------------------------------------------------------------------------
+
+void pade_assemble_batch(Context& ctx, std::vector<PadeDesc>& v) {
+    if (v.empty()) return;
+    long long maxc = 0;
+    for (auto& d : v) maxc = std::max(maxc, (long long)d.count);
+    if (maxc == 0) return;
+    Batch<PadeDesc> b = make_batch(ctx, v);
+    int bx = blocks_for(maxc, kThreads, std::max(1, 148 * 8 / (int)v.size()) + 1);
+    pade_assemble_kernel<<<dim3(bx, b.count), kThreads, 0, ctx.stream>>>(b);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
 
 void ew_batch(Context& ctx, std::vector<EwDesc>& v) {
     if (v.empty()) return;

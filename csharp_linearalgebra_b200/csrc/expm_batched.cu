@@ -371,39 +371,60 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
     // Per job: u (numerator odd part times A) and v (even part); then
     // den = v - u, num = v + u.
     struct Eval {
-        DMat b, b2, b4, b6, inner, inner_even, w, u, v;
+        DMat b, b6, inner, inner_even, w, u, v;
     };
     std::vector<Eval> ev(cnt);
     {
-        std::vector<EwDesc> ew;
-        for (size_t k = 0; k < cnt; ++k) {
-            Job& j = jobs[k];
-            Eval& e = ev[k];
-            if (j.degree == 9) {
-                j.a8 = like(ctx, *j.a);
-            }
-            if (j.degree == 13) {
-                double f = std::ldexp(1.0, -j.s);
-                e.b = like(ctx, *j.a);
-                e.b2 = like(ctx, *j.a);
-                e.b4 = like(ctx, *j.a);
-                e.b6 = like(ctx, *j.a);
-                ew.push_back(ew_scaled_copy(e.b, *j.a, f));
-                ew.push_back(ew_scaled_copy(e.b2, j.a2, f * f));
-                ew.push_back(ew_scaled_copy(e.b4, j.a4, std::pow(f, 4)));
-                ew.push_back(ew_scaled_copy(e.b6, j.a6, std::pow(f, 6)));
-            }
-        }
-        ew_batch(ctx, ew);
         // A^8 for degree 9 (:229).
         std::vector<std::pair<const DMat*, const DMat*>> ab;
         std::vector<DMat*> c;
         for (auto& j : jobs)
             if (j.degree == 9) {
+                j.a8 = like(ctx, *j.a);
                 ab.push_back({&j.a4, &j.a4});
                 c.push_back(&j.a8);
             }
         product_batch(ctx, ab, c, 0.0, Form::kSplittable);
+        // The numerator's parts, one pass for all jobs (blas1.cu).
+        std::vector<PadeDesc> pd;
+        for (size_t k = 0; k < cnt; ++k) {
+            Job& j = jobs[k];
+            Eval& e = ev[k];
+            e.w = like(ctx, *j.a);
+            e.v = like(ctx, *j.a);
+            PadeDesc d{};
+            d.a = j.a->p;
+            d.a2 = j.a2.p;
+            d.a4 = j.a4.p;
+            d.a6 = j.a6.p;
+            d.a8 = j.degree == 9 ? j.a8.p : nullptr;
+            d.w = e.w.p;
+            d.v = e.v.p;
+            d.count = e.w.bytes() / 8;
+            d.rows_p = e.w.rows_p;
+            d.n = e.w.rows;
+            d.cplx = e.w.cplx ? 1 : 0;
+            d.degree = j.degree;
+            const double* b = pade_coefficients(j.degree);
+            for (int q = 0; q <= j.degree; ++q) d.c[q] = b[q];
+            if (j.degree == 13) {
+                const double f = std::ldexp(1.0, -j.s);
+                e.b = like(ctx, *j.a);
+                e.b6 = like(ctx, *j.a);
+                e.inner = like(ctx, *j.a);
+                e.inner_even = like(ctx, *j.a);
+                d.b = e.b.p;
+                d.b6 = e.b6.p;
+                d.inner = e.inner.p;
+                d.inner_even = e.inner_even.p;
+                d.f = f;
+                d.f2 = f * f;
+                d.f4 = std::pow(f, 4);
+                d.f6 = std::pow(f, 6);
+            }
+            pd.push_back(d);
+        }
+        pade_assemble_batch(ctx, pd);
         // The powers of degree-13 jobs are no longer needed.
         for (auto& j : jobs)
             if (j.degree == 13) {
@@ -413,62 +434,6 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
             }
     }
     {
-        // Elementwise assembly, in the reference's order of operations.
-        std::vector<EwDesc> s1, s2, s3, s4;  // sequential rounds (each op in a round touches distinct targets)
-        for (size_t k = 0; k < cnt; ++k) {
-            Job& j = jobs[k];
-            Eval& e = ev[k];
-            e.w = like(ctx, *j.a);
-            e.v = like(ctx, *j.a);
-            if (j.degree == 13) {
-                const double* b = kPade13;
-                e.inner = like(ctx, *j.a);
-                e.inner_even = like(ctx, *j.a);
-                // inner = b13 B6 + b11 B4 + b9 B2; w = b1 I + b3 B2 + b5 B4 + b7 B6;
-                // inner_even = b12 B6 + b10 B4 + b8 B2; v = b0 I + b2 B2 + b4 B4 + b6 B6.
-                s1.push_back(ew_scaled_copy(e.inner, e.b6, b[13]));
-                s1.push_back(ew_identity(e.w, b[1]));
-                s1.push_back(ew_scaled_copy(e.inner_even, e.b6, b[12]));
-                s1.push_back(ew_identity(e.v, b[0]));
-                s2.push_back(ew_add_scaled(e.inner, e.b4, b[11]));
-                s2.push_back(ew_add_scaled(e.w, e.b2, b[3]));
-                s2.push_back(ew_add_scaled(e.inner_even, e.b4, b[10]));
-                s2.push_back(ew_add_scaled(e.v, e.b2, b[2]));
-                s3.push_back(ew_add_scaled(e.inner, e.b2, b[9]));
-                s3.push_back(ew_add_scaled(e.w, e.b4, b[5]));
-                s3.push_back(ew_add_scaled(e.inner_even, e.b2, b[8]));
-                s3.push_back(ew_add_scaled(e.v, e.b4, b[4]));
-                s4.push_back(ew_add_scaled(e.w, e.b6, b[7]));
-                s4.push_back(ew_add_scaled(e.v, e.b6, b[6]));
-            } else {
-                const double* b = j.degree == 3 ? kPade3 : j.degree == 5 ? kPade5 : j.degree == 7 ? kPade7 : kPade9;
-                int m = j.degree;
-                s1.push_back(ew_identity(e.w, b[1]));
-                s1.push_back(ew_identity(e.v, b[0]));
-                s2.push_back(ew_add_scaled(e.w, j.a2, b[3]));
-                s2.push_back(ew_add_scaled(e.v, j.a2, b[2]));
-                if (m >= 5) {
-                    s3.push_back(ew_add_scaled(e.w, j.a4, b[5]));
-                    s3.push_back(ew_add_scaled(e.v, j.a4, b[4]));
-                }
-                if (m >= 7) {
-                    s4.push_back(ew_add_scaled(e.w, j.a6, b[7]));
-                    s4.push_back(ew_add_scaled(e.v, j.a6, b[6]));
-                }
-            }
-        }
-        ew_batch(ctx, s1);
-        ew_batch(ctx, s2);
-        ew_batch(ctx, s3);
-        ew_batch(ctx, s4);
-        std::vector<EwDesc> s5;
-        for (auto& j : jobs)
-            if (j.degree == 9) {
-                size_t k = &j - jobs.data();
-                s5.push_back(ew_add_scaled(ev[k].w, j.a8, kPade9[9]));
-                s5.push_back(ew_add_scaled(ev[k].v, j.a8, kPade9[8]));
-            }
-        ew_batch(ctx, s5);
         // w += B6 inner; v += B6 inner_even (degree 13, beta = 1).
         std::vector<std::pair<const DMat*, const DMat*>> ab;
         std::vector<DMat*> c;

@@ -232,6 +232,16 @@ struct PanelDesc {  // Y := A X (or A^H X), X and Y n x t
     int ldy, t;
 };
 void ew_batch(Context& ctx, std::vector<EwDesc>& v);
+// The Pade numerator's polynomial parts of one matrix in one pass (see blas1.cu).
+struct PadeDesc {
+    const double *a, *a2, *a4, *a6, *a8;
+    double *b, *b6, *w, *v, *inner, *inner_even;
+    size_t count;  // doubles
+    int rows_p, n, cplx, degree;
+    double f, f2, f4, f6;  // 2^-s and its powers (degree 13)
+    double c[14];          // the Pade coefficients b_0..b_m
+};
+void pade_assemble_batch(Context& ctx, std::vector<PadeDesc>& v);
 EwDesc ew_scaled_copy(DMat& dst, const DMat& src, double f);
 EwDesc ew_add_scaled(DMat& t, const DMat& s, double f);
 EwDesc ew_identity(DMat& dst, double f);
