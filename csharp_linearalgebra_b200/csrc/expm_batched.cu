@@ -8,11 +8,17 @@
 // ell on the scaled matrix. What is batched is the work between decisions:
 // the powers A^2, A^4, A^6 are three grouped GEMM launches for the whole
 // batch; the norms, the ell chains and every normest1 product step are one
-// launch each for all matrices in that stage; the Pade evaluation is a few
-// elementwise launches and three grouped GEMMs; the LU of the denominators
+// launch each for all matrices in that stage; the Pade evaluation is one
+// fused elementwise launch and three grouped GEMMs; the LU of the denominators
 // advances all matrices block step by block step; the solve and each round
 // of squarings are grouped GEMMs over the matrices still squaring. A single
 // matrix is a batch of one.
+//
+// In the split form (Context::split_moduli > 0) every product runs on the
+// split product. d4 and d6 then carry intervals that hold the reference's
+// values (its FP64 rounding included), and a matrix whose next decision is
+// not settled on them has A^2, A^4, A^6 recomputed as the reference computes
+// them (powers / make_exact below), so the degree and s stay the reference's.
 
 #include "estimator.h"
 #include "pade.h"
