@@ -1,5 +1,5 @@
-"""Expm with its Pade-evaluation and squaring products in the split-precision
-form (8-bit residues modulo 20 moduli on the tensor cores, Chinese-remainder reconstruction).
+"""Expm with its products in the split-precision form (8-bit residues modulo
+18 or 20 moduli on the tensor cores, Chinese-remainder reconstruction).
 
 The degree and the squaring count are the reference's exactly: their inputs
 (norms, A^2, A^4, A^6, normest1) stay in plain FP64.
@@ -25,13 +25,17 @@ pytestmark = pytest.mark.gpu
 MODULI = 20
 
 
-@pytest.fixture
-def split_ws(ws):
+@pytest.fixture(params=[18, 20])
+def split_ws(ws, request):
+    """The split form at the benchmark's 18 moduli and at 20."""
+    global MODULI
+    MODULI = request.param
     ws.set_split_moduli(MODULI)
     try:
         yield ws
     finally:
         ws.set_split_moduli(0)
+        MODULI = 20
 
 
 def sweep_matrix(rng, n, w):
