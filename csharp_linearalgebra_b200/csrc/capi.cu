@@ -490,6 +490,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             wc.timing = ctx.timing;
             wc.split_moduli = ctx.split_moduli;
             wc.autotune = ctx.autotune;
+            wc.concurrent = true;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
                 run_group(wc, groups[w]);

@@ -916,7 +916,9 @@ bool launch_panel_coop(Context& ctx, const PanelFactorDesc& p) {
 
 void launch_panels(Context& ctx, bool cplx, std::vector<PanelFactorDesc>& v) {
     if (v.empty()) return;
-    if (v.size() == 1 && v[0].m - v[0].r0 >= kCoopPanelRows && v[0].w <= 64) {
+    // Not in a batch worker: two cooperative panels on concurrent streams
+    // could each hold part of the SMs while waiting for the rest.
+    if (!ctx.concurrent && v.size() == 1 && v[0].m - v[0].r0 >= kCoopPanelRows && v[0].w <= 64) {
         if (cplx ? launch_panel_coop<true>(ctx, v[0]) : launch_panel_coop<false>(ctx, v[0])) return;
     }
     Batch<PanelFactorDesc> b = make_batch(ctx, v);

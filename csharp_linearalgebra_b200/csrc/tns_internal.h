@@ -101,6 +101,10 @@ struct Context {
     // first launch (autotune.h) instead of the fixed rule.
     bool autotune = false;
     long long autotune_trials = 0;
+    // A batch worker: its kernels share the GPU with other workers' streams,
+    // so it launches nothing that needs the whole GPU at once (the
+    // cooperative LU panel).
+    bool concurrent = false;
     // Split form: matrices whose A^2, A^4, A^6 were recomputed in plain FP64
     // because a decision was not settled on the split values' intervals.
     long long exact_fallbacks = 0;
