@@ -58,8 +58,9 @@ def test_max_over_ranks_single_rank_is_identity():
 
 @pytest.mark.timeout(600)
 def test_reference_arm_under_torchrun_world_2():
-    """bench.py --impl reference launched as the driver launches it for N = 2:
-    both ranks join a gloo group, rank 0 alone prints one JSON line."""
+    """bench.py --impl reference under torchrun with two ranks, as a two-GPU
+    run launches it: both ranks join a gloo group, rank 0 alone prints one
+    JSON line."""
     env = dict(os.environ, OMP_NUM_THREADS="2")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
