@@ -45,11 +45,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "batched complex expm/s: split-prec vs plain FP64 GPU at ≤1e-12 rel err; vs CPU"
 # DRAM bytes of the GEMM launches per algorithmic byte, from one ncu capture of every GEMM launch of
-# the 16-matrix sweep (profiles/gemm_dmma_complex_sweep16.md): 109.1 MB measured / 153.4 MB.
+# the 16-matrix sweep (same generator, --count 16): 109.1 MB measured / 153.4 MB.
 GEMM_TRAFFIC_RATIO = 109.1 / 153.35
 # The same for the modular GEMM of the split form: every modular_gemm launch of the 16-matrix sweep
-# (110 launches) read and wrote 105.59 GB of DRAM against 101.09 GB of algorithmic bytes
-# (profiles/modular_gemm_sweep16.md).
+# (110 launches) read and wrote 105.59 GB of DRAM against 101.09 GB of algorithmic bytes.
 SPLIT_TRAFFIC_RATIO = 105.585 / 101.086
 WORKLOAD = ("frequency sweep of 256 complex128 matrices A_k = -(G + i w_k C), n_k ~ U{64..1024}, "
             "G ~ N(0,1)/sqrt(n), C = Q^T D Q (D log-uniform [1e-3,1]), w_k log-spaced 1e2..1e6; Expm of each")
@@ -72,16 +71,23 @@ def make_sweep(count: int, seed: int):
     return [int(n) for n in orders], mats
 
 
-def cpu_sample(orders, budget):
-    """Indices of a bounded, representative CPU sample: sweep order until the
-    summed n^3 reaches `budget`."""
-    idx, acc = [], 0.0
-    for i, n in enumerate(orders):
-        idx.append(i)
-        acc += float(n) ** 3
-        if acc >= budget:
-            break
-    return idx
+def cpu_sample(count, size):
+    """Indices of the bounded CPU sample: every ceil(count/size)-th matrix of
+    the sweep, starting half a stride in, so that the sample spans the whole
+    omega range (1e2..1e6, hence every squaring count) and the order range."""
+    stride = max(1, -(-count // size))
+    return list(range(stride // 2, count, stride))[:size]
+
+
+def sample_chunks(sample, chunks):
+    """The sample in `chunks` interleaved parts, each again spanning omega."""
+    return [sample[c::chunks] for c in range(chunks) if sample[c::chunks]]
+
+
+def expm_cost(n, s):
+    """The cost model of one Expm: n^3 (s + 8), about the product count of
+    degree 13 (six products, the Pade solve, s squarings) times n^3."""
+    return float(n) ** 3 * (s + 8)
 
 
 class ClockSampler:
@@ -160,34 +166,55 @@ def max_over_ranks_of(dist, value, device):
 
 
 def reference_arm(args, world, rank):
-    """The reference's algorithm on the host cores (the oracle restatement)."""
+    """The reference's algorithm on the host cores (the oracle restatement),
+    on the same stratified sample as the GPU arm's cpu_baseline. The sample's
+    matrices are split into interleaved chunks, each spanning omega; step j
+    runs chunk j mod chunks, so that a step stays bounded."""
     if rank != 0:
         return
     from oracle import oracle
     oracle.lib()
     threads = oracle.threads()
     orders, mats = make_sweep(args.count, args.seed)
-    sample = cpu_sample(orders, args.ref_budget)
-    def step():
-        for i in sample:
-            oracle.expm(mats[i])
-    for _ in range(args.warmup):
-        step()
+    sample = cpu_sample(len(orders), args.cpu_sample)
+    chunks = sample_chunks(sample, args.ref_chunks)
+    infos = {}
+
+    def step(j):
+        for i in chunks[j % len(chunks)]:
+            _, info = oracle.expm(mats[i])
+            infos[i] = info
+
+    for w in range(args.warmup):
+        step(w)
+    done = 0
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    dt = (time.perf_counter() - t0) / args.steps
-    value = len(sample) / dt
+    for j in range(args.steps):
+        step(j)
+        done += len(chunks[j % len(chunks)])
+    elapsed = time.perf_counter() - t0
+    value = done / elapsed
+    covered = sorted(set(i for j in range(args.steps) for i in chunks[j % len(chunks)]))
+    squarings = [infos[i]["squarings"] for i in covered]
+    desc = (f"stratified: every {sample[1] - sample[0] if len(sample) > 1 else 1}-th matrix of the sweep "
+            f"({len(sample)} matrices, omega {min(OMEGAS(args.count)[i] for i in sample):.3g}.."
+            f"{max(OMEGAS(args.count)[i] for i in sample):.3g}), in {len(chunks)} interleaved chunks; timed steps "
+            f"covered {len(covered)} of them, orders {[orders[i] for i in covered]}, squarings {squarings}")
     line = {"metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic, seeded",
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (complex128)", "data": "synthetic, seeded",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "count": args.count, "seed": args.seed,
-                       "sample": f"first {len(sample)} matrices of the sweep per step (sum n^3 >= {args.ref_budget:.1e})"},
-            "cpu_baseline": {"value": value, "unit": "expm/s", "cores": threads, "kind": "port",
-                             "sample": f"first {len(sample)} matrices of the sweep, orders {[orders[i] for i in sample]}"},
+            "config": {"workload": WORKLOAD, "count": args.count, "seed": args.seed, "sample": desc,
+                       "sample_cost_n3_s8": sum(expm_cost(orders[i], infos[i]["squarings"]) for i in covered),
+                       "sweep_sum_n3": sum(float(n) ** 3 for n in orders)},
+            "cpu_baseline": {"value": value, "unit": "expm/s", "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": "expm/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def OMEGAS(count):
+    """The sweep's frequencies, as make_sweep draws them."""
+    return np.logspace(2.0, 6.0, count)
 
 
 def measured_fp64_peak(torch):
@@ -352,19 +379,39 @@ def ours(args, world, rank, local, dist):
     ratios = [e / f if f > 0 else (0.0 if e == 0 else float("inf")) for e, f in zip(errs, floors)]
     del pert, pert_out
 
-    # CPU baseline (rank 0, N = 1 only): the oracle on a bounded sample
+    # CPU baseline (rank 0, N = 1 only): the oracle on a bounded, stratified
+    # sample. Its results are also the parity check of the plain form: the
+    # same bits as the reference's algorithm, matrix by matrix.
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle
         oracle.lib()
-        sample = cpu_sample(orders, args.cpu_budget)
+        sample = cpu_sample(count, args.cpu_sample)
         t0 = time.perf_counter()
-        for i in sample:
-            oracle.expm(mats[i])
+        refs = [oracle.expm(mats[i]) for i in sample]
         dt = time.perf_counter() - t0
+        equal, decisions, worst = 0, 0, 0.0
+        for i, (ref, info) in zip(sample, refs):
+            got = plain["outs"][i].cpu().numpy().T
+            equal += bool(np.array_equal(got, ref))
+            d = plain["diags"][i]
+            decisions += (d.degree, d.squarings) == (info["degree"], info["squarings"])
+            worst = max(worst, float(np.abs(got - ref).sum(axis=0).max() / np.abs(ref).sum(axis=0).max()))
+        omg = OMEGAS(count)
+        sample_cost = sum(expm_cost(orders[i], plain["diags"][i].squarings) for i in sample)
+        sweep_cost = sum(expm_cost(n, d.squarings) for n, d in zip(orders, plain["diags"]))
+        desc = (f"stratified: {len(sample)} matrices, every {sample[1] - sample[0] if len(sample) > 1 else 1}-th of "
+                f"this sweep (omega {omg[sample[0]]:.3g}..{omg[sample[-1]]:.3g}, orders "
+                f"{[orders[i] for i in sample]}, squarings {[plain['diags'][i].squarings for i in sample]}), "
+                f"{dt:.1f} s, C++ restatement of the reference, all host threads")
         cpu = {"value": len(sample) / dt, "unit": "expm/s", "cores": oracle.threads(), "kind": "port",
-               "sample": f"first {len(sample)} matrices of this sweep (orders {[orders[i] for i in sample]}), "
-                         f"{dt:.1f} s, C++ restatement of the reference, all host threads"}
+               "sample": desc, "sample_cost_n3_s8": sample_cost, "sweep_cost_n3_s8": sweep_cost,
+               "cost_weighted_value": (sample_cost / dt) / (sweep_cost / count),
+               "cost_weighted_note": "sample cost per second / mean sweep cost per matrix: the CPU rate had it "
+                                     "run the whole sweep's mix"}
+        parity = {"matrices_compared": len(sample), "bit_identical": equal, "decisions_equal": decisions,
+                  "max_rel_err_1norm": worst}
 
     def dmma_roofline(r):
         st = r["st"]
@@ -376,8 +423,7 @@ def ours(args, world, rank, local, dist):
                 "traffic": (GEMM_TRAFFIC_RATIO * st["gemm_bytes"] / st["gemm_launches"])
                            if st["gemm_launches"] else None,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every GEMM launch of "
-                                  "the 16-matrix sweep = 0.711 x its algorithmic bytes "
-                                  "(profiles/gemm_dmma_complex_sweep16.md), scaled to this sweep's "
+                                  "the 16-matrix sweep = 0.711 x its algorithmic bytes, scaled to this sweep's "
                                   "algorithmic bytes per launch",
                 "timing": "CUDA events around every GEMM launch of one extra sweep run as a single group",
                 "gemm_launches_per_sweep": int(st["gemm_launches"]),
@@ -417,9 +463,8 @@ def ours(args, world, rank, local, dist):
                          "traffic": (SPLIT_TRAFFIC_RATIO * sst["split_bytes"] / sst["split_launches"])
                          if sst["split_launches"] else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum over every modular_gemm "
-                                           "launch of the 16-matrix sweep = 1.044 x its algorithmic bytes "
-                                           "(profiles/modular_gemm_sweep16.md), scaled to this sweep's algorithmic "
-                                           "bytes per launch",
+                                           "launch of the 16-matrix sweep = 1.044 x its algorithmic bytes, scaled to "
+                                           "this sweep's algorithmic bytes per launch",
                          "timing": "CUDA events around every split-product launch of one extra sweep run as a "
                                    "single group; int8 operations counted on the padded residue extents",
                          "split_launches_per_sweep": int(sst["split_launches"]),
@@ -441,7 +486,7 @@ def ours(args, world, rank, local, dist):
                 "exact_fallbacks_per_sweep": int(split["st"]["exact_fallbacks"])},
             "plain_fp64": {"value": rate(plain["ms"]), "ms_per_step": plain["ms"],
                            "e2e": rate(plain["e2e_ms"]), "gpu_launches": int(plain["st_step"]["kernel_launches"]),
-                           "bit_identical_to_reference": True, "roofline": dmma_roofline(plain),
+                           "parity_vs_reference": parity, "roofline": dmma_roofline(plain),
                            "clocks": plain["clocks"]},
             "cpu_baseline": cpu,
             "clocks": split["clocks"],
@@ -460,8 +505,8 @@ def main():
     p.add_argument("--count", type=int, default=256)
     p.add_argument("--groups", type=int, default=4, help="cost-balanced groups run concurrently")
     p.add_argument("--seed", type=int, default=20260915)
-    p.add_argument("--cpu-budget", type=float, default=6e9, help="sum of n^3 in the CPU-baseline sample")
-    p.add_argument("--ref-budget", type=float, default=2e9, help="sum of n^3 per reference-arm step")
+    p.add_argument("--cpu-sample", type=int, default=16, help="matrices in the stratified CPU sample")
+    p.add_argument("--ref-chunks", type=int, default=4, help="reference arm: the sample in this many steps")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     p.add_argument("--no-peak", action="store_true", help="skip the measured FP64/INT8 peaks (profiling runs)")

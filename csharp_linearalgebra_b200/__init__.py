@@ -154,6 +154,18 @@ class Workspace:
         self._call("tns_get_stats", C.byref(s))
         return {k: getattr(s, k) for k, _ in N.Stats._fields_}
 
+    def set_lu_timing(self, enabled: bool):
+        """Collect the blocked LU's per-phase device times (LuPhaseTimings)."""
+        self._call("tns_set_lu_timing", int(bool(enabled)))
+
+    def lu_timings(self) -> dict:
+        """Summed per-phase times (ms) of the LUs timed since the last reset:
+        panel, swaps, triangular, gemm, total, unattributed; block steps and
+        factorizations."""
+        t = N.LuTimings()
+        self._call("tns_get_lu_timings", C.byref(t))
+        return {k: getattr(t, k) for k, _ in N.LuTimings._fields_}
+
     def reset_stats(self):
         self._call("tns_reset_stats")
 
@@ -262,6 +274,51 @@ class Workspace:
 
     def frobenius_norm(self, a) -> float:
         return self._norm(a, b"F")
+
+    # -- the kernel seam's primitives ------------------------------------------
+    _SOLVES = {
+        (False, "upper"): "tns_dsolve_upper", (False, "upper_transposed"): "tns_dsolve_upper_transposed",
+        (False, "lower"): "tns_dsolve_lower", (False, "lower_transposed"): "tns_dsolve_lower_transposed",
+        (False, "lower_unit"): "tns_dsolve_lower_unit",
+        (False, "lower_unit_transposed"): "tns_dsolve_lower_unit_transposed",
+        (True, "upper"): "tns_zsolve_upper", (True, "upper_transposed"): "tns_zsolve_upper_adjoint",
+        (True, "lower_unit"): "tns_zsolve_lower_unit", (True, "lower_unit_transposed"): "tns_zsolve_lower_unit_adjoint",
+    }
+
+    def solve_triangular(self, kind: str, a, b):
+        """X := T^-1 B (kind "upper", "lower", "lower_unit") or T^-T B
+        ("..._transposed"; complex: T^-H B) for the triangle T of square A
+        (KernelEntry.Solve* / Structures.cs's triangular structures). Returns X."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+        name = self._SOLVES.get((cplx, kind))
+        if name is None:
+            raise ValueError(f"no {'complex ' if cplx else ''}{kind} triangular solve")
+        a = _fortran(a, cplx)
+        x = _fortran(b, cplx).copy(order="F")
+        vec = x.ndim == 1
+        if vec:
+            x = x.reshape(-1, 1, order="F")
+        if a.ndim != 2 or a.shape[0] != a.shape[1]:
+            raise ValueError(f"The triangle must be square, got {a.shape}.")
+        if x.shape[0] != a.shape[0]:
+            raise ValueError(f"B has {x.shape[0]} rows, expected {a.shape[0]}.")
+        self._call(name, a.shape[0], x.shape[1], _p(a), _ld(a), _p(x), _ld(x))
+        return x[:, 0] if vec else x
+
+    def multiply_panel(self, a, x, transposed: bool = False):
+        """Y := A X, or A^T X (A^H X for complex) for a panel X
+        (KernelEntry.MultiplyPanel / MultiplyPanelTransposed; the complex dense
+        operator's Apply / ApplyAdjoint)."""
+        cplx = np.iscomplexobj(a) or np.iscomplexobj(x)
+        a, x = _fortran(a, cplx), _fortran(x, cplx)
+        if a.ndim != 2 or a.shape[0] != a.shape[1] or x.ndim != 2 or x.shape[0] != a.shape[0]:
+            raise ValueError("A must be square and X must have A's number of rows")
+        n, t = x.shape
+        y = np.zeros((n, t), dtype=x.dtype, order="F")
+        name = ("tns_zmultiply_panel_adjoint" if transposed else "tns_zmultiply_panel") if cplx else \
+            ("tns_dmultiply_panel_transposed" if transposed else "tns_dmultiply_panel")
+        self._call(name, n, t, _p(a), _ld(a), _p(x), _ld(x), _p(y), _ld(y))
+        return y
 
     # -- LU -----------------------------------------------------------------
     def factor_lu(self, a, block_size: int = 0) -> "LuDecomposition":
@@ -376,6 +433,50 @@ class Workspace:
             diagnostics.degree, diagnostics.scaling = info.degree, info.scaling
             diagnostics.applications, diagnostics.early_exits = info.applications, info.early_exits
         return out[:, 0] if vec else out
+
+    def expmv_batched(self, mats, panels, t: float = 1.0, diagnostics: list | None = None):
+        """exp(t A_k) B_k for every pair (the frequency-sweep form of Expmv):
+        every B_k with the same number of columns; the Taylor recurrences of
+        all matrices run in one device launch. Returns the results."""
+        cplx = any(np.iscomplexobj(m) for m in mats) or any(np.iscomplexobj(b) for b in panels)
+        arrs = [_fortran(m, cplx) for m in mats]
+        bs = [_fortran(b, cplx) for b in panels]
+        if len(arrs) != len(bs):
+            raise ValueError("one panel per matrix")
+        for m, b in zip(arrs, bs):
+            if m.ndim != 2 or m.shape[0] != m.shape[1]:
+                raise ValueError("every matrix must be square")
+            if b.ndim != 2 or b.shape[0] != m.shape[0]:
+                raise ValueError("every panel needs its operator's order of rows")
+        ncols = bs[0].shape[1] if bs else 0
+        if any(b.shape[1] != ncols for b in bs):
+            raise ValueError("every panel must have the same number of columns")
+        outs = [np.zeros_like(b, order="F") for b in bs]
+        cnt = len(arrs)
+        orders = (C.c_int * cnt)(*[m.shape[0] for m in arrs])
+        lda = (C.c_int * cnt)(*[_ld(m) for m in arrs])
+        ldb = (C.c_int * cnt)(*[_ld(b) for b in bs])
+        ldo = (C.c_int * cnt)(*[_ld(o) for o in outs])
+        ap = (C.c_void_p * cnt)(*[m.ctypes.data for m in arrs])
+        bp = (C.c_void_p * cnt)(*[b.ctypes.data for b in bs])
+        op = (C.c_void_p * cnt)(*[o.ctypes.data for o in outs])
+        infos = (N.ExpmvInfo * cnt)()
+        self._call("tns_zexpmv_batched" if cplx else "tns_dexpmv_batched", cnt, orders, ap, lda, ncols, bp, ldb,
+                   float(t), op, ldo, infos)
+        if diagnostics is not None:
+            diagnostics.clear()
+            diagnostics.extend(ExpmvDiagnostics(i.degree, i.scaling, i.applications, i.early_exits) for i in infos)
+        return outs
+
+    def expmv_batched_device(self, count, orders, a_ptrs, lds, ncols, b_ptrs, ldbs, t, out_ptrs, ldos):
+        """The batched complex Expmv over device-resident operands (raw device
+        pointers). Returns the diagnostics."""
+        ic = lambda v: (C.c_int * count)(*v)  # noqa: E731
+        pc = lambda v: (C.c_void_p * count)(*v)  # noqa: E731
+        infos = (N.ExpmvInfo * count)()
+        self._call("tns_zexpmv_batched_device", count, ic(orders), pc(a_ptrs), ic(lds), int(ncols), pc(b_ptrs),
+                   ic(ldbs), float(t), pc(out_ptrs), ic(ldos), infos)
+        return [ExpmvDiagnostics(i.degree, i.scaling, i.applications, i.early_exits) for i in infos]
 
     def expmv_operator(self, apply, n: int, b, t: float, one_norm_bound: float, complex_: bool = False,
                        diagnostics: ExpmvDiagnostics | None = None):

@@ -1,8 +1,9 @@
 """ctypes binding of libtensile_b200.so, the sm_100a CUDA library.
 
-This is the binding a caller of the C ABI (include/tensile_b200.h) writes; the
-C# one is in INTEGRATION.md. There is no fallback: if the library is missing or
-cannot load, importing the package's compute API raises.
+This is the binding a Python caller of the C ABI (include/tensile_b200.h)
+writes; a C# caller binds the same symbols through NativeLibrary and unmanaged
+function pointers. There is no fallback: if the library is missing or cannot
+load, importing the package's compute API raises.
 """
 from __future__ import annotations
 
@@ -56,6 +57,12 @@ class Stats(C.Structure):
                 ("exact_fallbacks", C.c_longlong)]
 
 
+class LuTimings(C.Structure):
+    _fields_ = [("panel_ms", C.c_double), ("swaps_ms", C.c_double), ("triangular_ms", C.c_double),
+                ("gemm_ms", C.c_double), ("total_ms", C.c_double), ("unattributed_ms", C.c_double),
+                ("block_steps", C.c_longlong), ("factorizations", C.c_longlong)]
+
+
 # y := A x on device panels: (user, ncols, x, y, ld, stream) -> status
 APPLY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
 
@@ -79,6 +86,12 @@ SIGNATURES = {
     "tns_zgetrf": (_I, [_P, _I, _I, _P, _I, _I, _P, C.POINTER(LuInfo)]),
     "tns_dgetrs": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
     "tns_zgetrs": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I, _I]),
+    **{name: (_I, [_P, _I, _I, _P, _I, _P, _I]) for name in (
+        "tns_dsolve_upper", "tns_dsolve_upper_transposed", "tns_dsolve_lower", "tns_dsolve_lower_transposed",
+        "tns_dsolve_lower_unit", "tns_dsolve_lower_unit_transposed", "tns_zsolve_upper", "tns_zsolve_upper_adjoint",
+        "tns_zsolve_lower_unit", "tns_zsolve_lower_unit_adjoint")},
+    **{name: (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I]) for name in (
+        "tns_dmultiply_panel", "tns_dmultiply_panel_transposed", "tns_zmultiply_panel", "tns_zmultiply_panel_adjoint")},
     "tns_dgecon": (_I, [_P, _I, _P, _I, _P, _I, _D, C.POINTER(_D)]),
     "tns_zgecon": (_I, [_P, _I, _P, _I, _P, _I, _D, C.POINTER(_D)]),
     "tns_dnormest1_power": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, C.POINTER(NormestResult)]),
@@ -89,6 +102,9 @@ SIGNATURES = {
     "tns_zexpm_batched_device": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "tns_dexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
     "tns_zexpmv": (_I, [_P, _I, _P, _I, _I, _P, _I, _D, _P, _I, C.POINTER(ExpmvInfo)]),
+    "tns_dexpmv_batched": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
+    "tns_zexpmv_batched": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
+    "tns_zexpmv_batched_device": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
     "tns_dexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
     "tns_zexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
     "tns_dexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,
@@ -109,6 +125,8 @@ SIGNATURES = {
     "tns_reset_stats": (_I, [_P]),
     "tns_set_timing": (_I, [_P, _I]),
     "tns_get_stream": (_I, [_P, C.POINTER(_P)]),
+    "tns_set_lu_timing": (_I, [_P, _I]),
+    "tns_get_lu_timings": (_I, [_P, C.POINTER(LuTimings)]),
 }
 
 _lib = None

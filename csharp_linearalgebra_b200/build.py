@@ -16,7 +16,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtensile_b200.so")
 OBJ = os.path.join(HERE, "_build")
 
-SOURCES = ["context.cu", "gemm.cu", "blas1.cu", "lu.cu", "algos.cu", "expm_batched.cu", "capi.cu", "noalloc.cu",
+SOURCES = ["context.cu", "gemm.cu", "blas1.cu", "lu.cu", "algos.cu", "expm_batched.cu", "expmv_batched.cu", "capi.cu",
+           "noalloc.cu",
            "ozaki.cu", "frechet.cu"]
 
 NVCC_FLAGS = [

@@ -253,7 +253,20 @@ void taylor_run(Context& ctx, const std::function<void(const double*, double*, i
 
 }  // namespace
 
-void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info) {
+void expmv_select_parameters(double scaled_norm, const std::function<double(int)>* alpha, double scale, int cols,
+                             int& m, int& s) {
+    select_parameters(scaled_norm, alpha, scale, cols, m, s);
+}
+
+void expmv_taylor_host(Context& ctx, const DMat& shifted, const DMat& b, double t, int m, int s, double eta_re,
+                       double eta_im, DMat& result, ExpmvInfo* info) {
+    const int cols_b = b.cols;
+    taylor_run(
+        ctx, [&](const double* x, double* y, int ld) { panel_product(ctx, shifted, x, ld, y, ld, cols_b, false); }, b,
+        t, m, s, eta_re, eta_im, info, result);
+}
+
+void expmv_host_loop(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info) {
     ExpmvInfo local;
     if (!info) info = &local;
     *info = ExpmvInfo{};

@@ -335,25 +335,6 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant_
     }
 }
 
-// Lane L (0..15) of a half-warp has accumulated the 16-lane partial sums of
-// .NET's ColumnOps.Dot with 256-bit Vector<double> (ColumnOps.cs:35-65):
-// partial L holds the terms i = L mod 16 below the last whole 16-block, in
-// index order, and partials 0..3 then take the remaining whole 4-blocks.
-// Combine them as the reference does: s[l] = (a0[l] + a1[l]) + (a2[l] + a3[l]),
-// total = (s0 + s1) + (s2 + s3).
-__device__ __forceinline__ double netdot_combine(double acc, int L, int base) {
-    const unsigned mask = 0xffffffffu;
-    double a0 = __shfl_sync(mask, acc, base + (L & 3));
-    double a1 = __shfl_sync(mask, acc, base + 4 + (L & 3));
-    double a2 = __shfl_sync(mask, acc, base + 8 + (L & 3));
-    double a3 = __shfl_sync(mask, acc, base + 12 + (L & 3));
-    double s = add_rn(add_rn(a0, a1), add_rn(a2, a3));
-    double s0 = __shfl_sync(mask, s, base + 0);
-    double s1 = __shfl_sync(mask, s, base + 1);
-    double s2 = __shfl_sync(mask, s, base + 2);
-    double s3 = __shfl_sync(mask, s, base + 3);
-    return add_rn(add_rn(s0, s1), add_rn(s2, s3));
-}
 
 // Y := A^T X (real) or A^H X (complex operator: pr = Ar^T xr, pi = Ar^T xi,
 // qr = Ai^T xr, qi = Ai^T xi, then (pr + qi, pi - qr)), PanelProduct.ApplyTranspose
@@ -702,6 +683,13 @@ void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, doub
     scale_kernel<<<blocks_for((long long)m * n), kThreads, 0, ctx.stream>>>(static_cast<double*>(c), m, n, ldc, cplx, br, bi);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
+}
+
+void scale_detached(cudaStream_t stream, double* c, int m, int n, int ldc, bool cplx, double br, double bi) {
+    if (br == 1.0 && bi == 0.0) return;
+    if ((long long)m * n == 0) return;
+    scale_kernel<<<blocks_for((long long)m * n), kThreads, 0, stream>>>(c, m, n, ldc, cplx, br, bi);
+    TNS_CUDA(cudaGetLastError());
 }
 
 void scaled_copy(Context& ctx, DMat& dst, const DMat& src, double f) {

@@ -288,6 +288,87 @@ int expmv_entry(tns_context* c, bool cplx, int n, const double* a, int lda, int 
     });
 }
 
+int expmv_batched_entry(tns_context* c, bool cplx, bool dev, int count, const int* orders, const double* const* a,
+                        const int* lda, int ncols, const double* const* b, const int* ldb, double t,
+                        double* const* out, const int* ldo, tns_expmv_info* infos) {
+    return guarded(c, [&](Context& ctx) {
+        require(count >= 0, TNS_E_ARGUMENT, "negative batch size");
+        require(ncols >= 0, TNS_E_ARGUMENT, "negative column count");
+        if (count == 0) return;
+        require(orders && a && lda && b && ldb && out && ldo, TNS_E_NULL, "a batch array is null");
+        for (int i = 0; i < count; ++i) {
+            check_operand(a[i], orders[i], orders[i], lda[i], "A[i]");
+            check_operand(b[i], orders[i], ncols, ldb[i], "B[i]");
+            check_operand(out[i], orders[i], ncols, ldo[i], "out[i]");
+        }
+        require(std::isfinite(t), TNS_E_OUT_OF_RANGE, "t must be finite");
+        if (infos)
+            for (int i = 0; i < count; ++i) infos[i] = tns_expmv_info{0, 0, 0, 0};
+        if (ncols == 0) return;
+        std::vector<int> live;
+        for (int i = 0; i < count; ++i)
+            if (orders[i] > 0) live.push_back(i);
+        if (live.empty()) return;
+        std::vector<DMat> A, B;
+        A.reserve(live.size());
+        B.reserve(live.size());
+        for (int i : live) {
+            A.push_back(upload(ctx, a[i], orders[i], orders[i], lda[i], cplx, dev, "an operator of the batch"));
+            B.push_back(upload(ctx, b[i], orders[i], ncols, ldb[i], cplx, dev, "a panel of the batch"));
+        }
+        std::vector<const DMat*> ap, bp;
+        for (size_t k = 0; k < live.size(); ++k) {
+            ap.push_back(&A[k]);
+            bp.push_back(&B[k]);
+        }
+        std::vector<DMat> R;
+        std::vector<tns::ExpmvInfo> ei;
+        tns::expmv_batch(ctx, ap, bp, t, R, ei);
+        check_device_flag(ctx);  // a wait that gave up leaves every destination untouched
+        for (size_t k = 0; k < live.size(); ++k) tns::copy_out(ctx, R[k], out[live[k]], ldo[live[k]], dev);
+        ctx.sync();
+        if (infos)
+            for (size_t k = 0; k < live.size(); ++k)
+                infos[live[k]] = tns_expmv_info{ei[k].degree, ei[k].scaling, ei[k].applications, ei[k].early_exits};
+    });
+}
+
+// KernelEntry.SolveUpper .. SolveLowerUnitTransposed (KernelEntry.cs:98-173):
+// RequireTriangular -- A square, B with A's rows -- then the solve in place.
+int trsolve_entry(tns_context* c, bool cplx, tns::TriangularKind kind, int m, int n, const double* a, int lda, double* b,
+                  int ldb) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, m, m, lda, "A");
+        check_operand(b, m, n, ldb, "B");
+        if (m == 0 || n == 0) return;
+        DMat A = upload(ctx, a, m, m, lda, cplx, false, "the triangle");
+        DMat B = upload(ctx, b, m, n, ldb, cplx, false, "the right-hand sides");
+        tns::solve_triangular(ctx, kind, A, B, n);
+        check_device_flag(ctx);
+        tns::copy_out(ctx, B, b, ldb, false);
+        ctx.sync();
+    });
+}
+
+// KernelEntry.MultiplyPanel / MultiplyPanelTransposed (KernelEntry.cs:176-201):
+// RequirePanel -- A square, X and Y n x t -- then Y := A X or A^T X (complex:
+// the dense operator's A X or A^H X, LinearOperators.cs:194-293).
+int panel_entry(tns_context* c, bool cplx, bool adjoint, int n, int t, const double* a, int lda, const double* x,
+                int ldx, double* y, int ldy) {
+    return guarded(c, [&](Context& ctx) {
+        check_operand(a, n, n, lda, "A");
+        check_operand(x, n, t, ldx, "X");
+        check_operand(y, n, t, ldy, "Y");
+        if (n == 0 || t == 0) return;
+        DMat A = upload(ctx, a, n, n, lda, cplx, false, "the operator");
+        DMat X = upload(ctx, x, n, t, ldx, cplx, false, "the panel");
+        DMat Y(ctx, n, t, cplx, "the product panel");
+        tns::panel_product(ctx, A, X.p, X.ld(), Y.p, Y.ld(), t, adjoint);
+        tns::copy_out(ctx, Y, y, ldy, false);
+        ctx.sync();
+    });
+}
+
 int frechet_entry(tns_context* c, bool cplx, int n, const double* a, int lda, const double* e, int lde, double* expa,
                   int ldx, double* l, int ldl, tns_expm_info* info) {
     return guarded(c, [&](Context& ctx) {
@@ -567,6 +648,8 @@ void reset_stats(Context& ctx) {
     ctx.split_flops = ctx.split_int8_ops = ctx.split_ms_done = ctx.split_bytes = 0.0;
     ctx.autotune_trials = 0;
     ctx.exact_fallbacks = 0;
+    ctx.lu_panel_ms = ctx.lu_swaps_ms = ctx.lu_triangular_ms = ctx.lu_gemm_ms = ctx.lu_total_ms = 0.0;
+    ctx.lu_block_steps = ctx.lu_factorizations = 0;
     for (auto& w : ctx.workers) {
         w->drain_events();
         w->kernel_launches = w->gemm_launches = 0;
@@ -709,6 +792,54 @@ int tns_zexpm_batched_device(tns_context* c, int count, const int* orders, const
                              double* const* out, const int* ldo, tns_expm_info* infos) {
     return zexpm_batched_entry(c, true, count, orders, a, lda, out, ldo, infos);
 }
+#define TNS_TRSOLVE(name, cplx, kind)                                                                  \
+    int name(tns_context* c, int m, int n, const double* a, int lda, double* b, int ldb) {                \
+        return trsolve_entry(c, cplx, tns::TriangularKind::kind, m, n, a, lda, b, ldb);                   \
+    }
+TNS_TRSOLVE(tns_dsolve_upper, false, kUpper)
+TNS_TRSOLVE(tns_dsolve_upper_transposed, false, kUpperTransposed)
+TNS_TRSOLVE(tns_dsolve_lower, false, kLower)
+TNS_TRSOLVE(tns_dsolve_lower_transposed, false, kLowerTransposed)
+TNS_TRSOLVE(tns_dsolve_lower_unit, false, kLowerUnit)
+TNS_TRSOLVE(tns_dsolve_lower_unit_transposed, false, kLowerUnitTransposed)
+TNS_TRSOLVE(tns_zsolve_upper, true, kUpper)
+TNS_TRSOLVE(tns_zsolve_upper_adjoint, true, kUpperTransposed)
+TNS_TRSOLVE(tns_zsolve_lower_unit, true, kLowerUnit)
+TNS_TRSOLVE(tns_zsolve_lower_unit_adjoint, true, kLowerUnitTransposed)
+#undef TNS_TRSOLVE
+
+int tns_dmultiply_panel(tns_context* c, int n, int t, const double* a, int lda, const double* x, int ldx, double* y,
+                        int ldy) {
+    return panel_entry(c, false, false, n, t, a, lda, x, ldx, y, ldy);
+}
+int tns_dmultiply_panel_transposed(tns_context* c, int n, int t, const double* a, int lda, const double* x, int ldx,
+                                   double* y, int ldy) {
+    return panel_entry(c, false, true, n, t, a, lda, x, ldx, y, ldy);
+}
+int tns_zmultiply_panel(tns_context* c, int n, int t, const double* a, int lda, const double* x, int ldx, double* y,
+                        int ldy) {
+    return panel_entry(c, true, false, n, t, a, lda, x, ldx, y, ldy);
+}
+int tns_zmultiply_panel_adjoint(tns_context* c, int n, int t, const double* a, int lda, const double* x, int ldx,
+                                double* y, int ldy) {
+    return panel_entry(c, true, true, n, t, a, lda, x, ldx, y, ldy);
+}
+
+int tns_dexpmv_batched(tns_context* c, int count, const int* orders, const double* const* a, const int* lda, int ncols,
+                       const double* const* b, const int* ldb, double t, double* const* out, const int* ldo,
+                       tns_expmv_info* infos) {
+    return expmv_batched_entry(c, false, false, count, orders, a, lda, ncols, b, ldb, t, out, ldo, infos);
+}
+int tns_zexpmv_batched(tns_context* c, int count, const int* orders, const double* const* a, const int* lda, int ncols,
+                       const double* const* b, const int* ldb, double t, double* const* out, const int* ldo,
+                       tns_expmv_info* infos) {
+    return expmv_batched_entry(c, true, false, count, orders, a, lda, ncols, b, ldb, t, out, ldo, infos);
+}
+int tns_zexpmv_batched_device(tns_context* c, int count, const int* orders, const double* const* a, const int* lda,
+                              int ncols, const double* const* b, const int* ldb, double t, double* const* out,
+                              const int* ldo, tns_expmv_info* infos) {
+    return expmv_batched_entry(c, true, true, count, orders, a, lda, ncols, b, ldb, t, out, ldo, infos);
+}
 int tns_dexpm_frechet(tns_context* c, int n, const double* a, int lda, const double* e, int lde, double* expa,
                       int ldx, double* l, int ldl, tns_expm_info* info) {
     return frechet_entry(c, false, n, a, lda, e, lde, expa, ldx, l, ldl, info);
@@ -782,6 +913,25 @@ int tns_set_workers(tns_context* c, int workers) {
 }
 int tns_set_timing(tns_context* c, int enabled) {
     return guarded(c, [&](Context& ctx) { ctx.timing = enabled != 0; });
+}
+int tns_set_lu_timing(tns_context* c, int enabled) {
+    return guarded(c, [&](Context& ctx) { ctx.lu_timing = enabled != 0; });
+}
+int tns_get_lu_timings(tns_context* c, tns_lu_timings* out) {
+    return guarded(c, [&](Context& ctx) {
+        require(out != nullptr, TNS_E_NULL, "out is null");
+        out->panel_ms = ctx.lu_panel_ms;
+        out->swaps_ms = ctx.lu_swaps_ms;
+        out->triangular_ms = ctx.lu_triangular_ms;
+        out->gemm_ms = ctx.lu_gemm_ms;
+        out->total_ms = ctx.lu_total_ms;
+        // The residue the phases do not account for, never negative
+        // (LuPhaseTimings.Unattributed).
+        out->unattributed_ms = std::max(0.0, ctx.lu_total_ms - (ctx.lu_panel_ms + ctx.lu_swaps_ms +
+                                                                  ctx.lu_triangular_ms + ctx.lu_gemm_ms));
+        out->block_steps = ctx.lu_block_steps;
+        out->factorizations = ctx.lu_factorizations;
+    });
 }
 int tns_get_stream(tns_context* c, void** stream) {
     return guarded(c, [&](Context& ctx) {

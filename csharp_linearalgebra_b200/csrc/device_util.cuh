@@ -148,6 +148,26 @@ __device__ __forceinline__ double cabs_net(double re, double im) {
     return __dmul_rn(large, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(ratio, ratio))));
 }
 
+// Lane L (0..15) of a half-warp has accumulated the 16-lane partial sums of
+// .NET's ColumnOps.Dot with 256-bit Vector<double> (ColumnOps.cs:35-65):
+// partial L holds the terms i = L mod 16 below the last whole 16-block, in
+// index order, and partials 0..3 then take the remaining whole 4-blocks.
+// Combine them as the reference does: s[l] = (a0[l] + a1[l]) + (a2[l] + a3[l]),
+// total = (s0 + s1) + (s2 + s3).
+__device__ __forceinline__ double netdot_combine(double acc, int L, int base) {
+    const unsigned mask = 0xffffffffu;
+    double a0 = __shfl_sync(mask, acc, base + (L & 3));
+    double a1 = __shfl_sync(mask, acc, base + 4 + (L & 3));
+    double a2 = __shfl_sync(mask, acc, base + 8 + (L & 3));
+    double a3 = __shfl_sync(mask, acc, base + 12 + (L & 3));
+    double s = add_rn(add_rn(a0, a1), add_rn(a2, a3));
+    double s0 = __shfl_sync(mask, s, base + 0);
+    double s1 = __shfl_sync(mask, s, base + 1);
+    double s2 = __shfl_sync(mask, s, base + 2);
+    double s3 = __shfl_sync(mask, s, base + 3);
+    return add_rn(add_rn(s0, s1), add_rn(s2, s3));
+}
+
 // Math.Max / Math.Min (.NET Core): NaN propagates, +0 beats -0.
 __device__ __forceinline__ double net_max(double a, double b) {
     if (a != b) {

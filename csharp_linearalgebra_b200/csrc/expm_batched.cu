@@ -183,6 +183,10 @@ void product_batch(Context& ctx, std::vector<std::pair<const DMat*, const DMat*>
 
 }  // namespace
 
+std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+    return power_norms(ctx, mats, power);
+}
+
 void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,
                 std::vector<ExpmInfo>& infos) {
     const size_t cnt = inputs.size();

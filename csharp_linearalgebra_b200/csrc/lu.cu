@@ -18,9 +18,11 @@
 // Solves: forward and backward substitution in the reference's order, blocked
 // into 32-row diagonal solves and register-tiled updates that continue each
 // element's chain of roundings in the reference's order, so A^-1 B -- the Pade
-// solve included -- matches the reference bit for bit. The adjoint solves use
-// 64-row diagonal blocks plus DMMA GEMM updates of the rows beyond them (a
-// blocked, GEMM-based TRSM).
+// solve included -- matches the reference bit for bit. The adjoint solves,
+// whose reference order is an inner product per row, run left-looking: ColumnOps.Dot's
+// vector order for real factors, sequential sums for complex ones (the forward
+// half of the complex adjoint, whose sums run in ascending k, right-looking
+// over the conjugate transpose), so they match bit for bit too.
 
 #include "batch.cuh"
 #include "device_util.cuh"
@@ -617,7 +619,7 @@ __device__ __forceinline__ Z subst_axpy(Z x, Z nxk, Z f) {
 // Step 1: the block's own triangle, one thread per right-hand side column,
 // the block's values in registers and its triangle in shared memory (every
 // thread reads the same entry at a time: a broadcast).
-template <bool CPLX, bool UPPER>
+template <bool CPLX, bool UPPER, bool LDIV = false>
 __global__ void __launch_bounds__(128) subst_diag_kernel(const __grid_constant__ Batch<SubstDiagDesc> b) {
     constexpr int B = kSubstBlock;
     constexpr int ES = CPLX ? 2 : 1;
@@ -646,9 +648,18 @@ __global__ void __launch_bounds__(128) subst_diag_kernel(const __grid_constant__
     }
     if (!UPPER) {
 #pragma unroll
-        for (int k = 0; k < B - 1; ++k) {
+        for (int k = 0; k < B; ++k) {
+            if (k >= w) continue;
+            if (LDIV) {
+                // An explicit diagonal (Triangular.SolveLower, Triangular.cs:131-150;
+                // the adjoint's U^H): x_k /= f_kk first, always for real, and for
+                // complex when x_k is not zero (BlockedLu's division rule).
+                const Z dg = t[k][k];
+                if (!CPLX) v[k].re = __ddiv_rn(v[k].re, dg.re);
+                else if (!(v[k].re == 0.0 && v[k].im == 0.0)) v[k] = zdiv(v[k], dg);
+            }
             const Z xk = v[k];
-            if (k >= w || (xk.re == 0.0 && xk.im == 0.0)) continue;
+            if (k == B - 1 || (xk.re == 0.0 && xk.im == 0.0)) continue;
             const Z nxk{-xk.re, -xk.im};
 #pragma unroll
             for (int i = k + 1; i < B; ++i)
@@ -981,13 +992,13 @@ void launch_trsm(Context& ctx, bool cplx, int kind, std::vector<TrsmDesc>& v) {
 
 // One block step of the substitution for every item of a batch: the
 // diagonal blocks in one launch, then the updates of all items' tiles in one.
-template <bool CPLX, bool UPPER>
+template <bool CPLX, bool UPPER, bool LDIV = false>
 void launch_subst_step_t(Context& ctx, std::vector<SubstDiagDesc>& diag, std::vector<SubstUpdateDesc>& upd) {
     if (!diag.empty()) {
         int mr = 0;
         for (auto& d : diag) mr = std::max(mr, d.nrhs);
         Batch<SubstDiagDesc> b = make_batch(ctx, diag);
-        subst_diag_kernel<CPLX, UPPER><<<dim3((mr + 127) / 128, b.count), 128, 0, ctx.stream>>>(b);
+        subst_diag_kernel<CPLX, UPPER, LDIV><<<dim3((mr + 127) / 128, b.count), 128, 0, ctx.stream>>>(b);
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches++;
     }
@@ -1006,14 +1017,141 @@ void launch_subst_step_t(Context& ctx, std::vector<SubstDiagDesc>& diag, std::ve
 }
 
 void launch_subst_step(Context& ctx, bool cplx, bool upper, std::vector<SubstDiagDesc>& diag,
-                       std::vector<SubstUpdateDesc>& upd) {
+                       std::vector<SubstUpdateDesc>& upd, bool lower_divides = false) {
     if (cplx) {
         if (upper) launch_subst_step_t<true, true>(ctx, diag, upd);
+        else if (lower_divides) launch_subst_step_t<true, false, true>(ctx, diag, upd);
         else launch_subst_step_t<true, false>(ctx, diag, upd);
     } else {
         if (upper) launch_subst_step_t<false, true>(ctx, diag, upd);
+        else if (lower_divides) launch_subst_step_t<false, false, true>(ctx, diag, upd);
         else launch_subst_step_t<false, false>(ctx, diag, upd);
     }
+}
+
+// Right-looking substitution of rows [0, n) of every item, in blocks of
+// kSubstBlock rows: lower (forward, unit diagonal unless lower_divides) or
+// upper (backward, explicit diagonal), the reference's column-oriented order
+// (Triangular.SolveLowerUnit / SolveLower / SolveUpper, BlockedLu.SolveLowerUnit /
+// SolveUpper). f: the factor (ld ldf), x: the right-hand sides (ld ldx).
+struct SubstItem {
+    const double* f;
+    int ldf;
+    double* x;
+    int ldx, n, nrhs;
+};
+void substitute(Context& ctx, bool cplx, bool upper, bool lower_divides, const std::vector<SubstItem>& items) {
+    constexpr int B = kSubstBlock;
+    int steps = 0;
+    for (auto& it : items)
+        if (it.n > 0 && it.nrhs > 0) steps = std::max(steps, (it.n + B - 1) / B);
+    for (int s = 0; s < steps; ++s) {
+        std::vector<SubstDiagDesc> diag;
+        std::vector<SubstUpdateDesc> upd;
+        for (auto& it : items) {
+            const int n = it.n;
+            if (n == 0 || it.nrhs == 0) continue;
+            const int blocks = (n + B - 1) / B;
+            if (s >= blocks) continue;
+            const int k0 = (upper ? blocks - 1 - s : s) * B, w = std::min(B, n - k0);
+            diag.push_back(SubstDiagDesc{it.f, it.ldf, it.x, it.ldx, it.nrhs, k0, w});
+            const int r0 = upper ? 0 : k0 + w, r1 = upper ? k0 : n;
+            if (r1 > r0)
+                upd.push_back(SubstUpdateDesc{it.f, it.ldf, it.x, it.ldx, it.nrhs, r0, r1, k0, k0 + w,
+                                              (r1 - r0 + 63) / 64, 0});
+        }
+        launch_subst_step(ctx, cplx, upper, diag, upd, lower_divides);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Left-looking substitution for the transposed (real) and adjoint (complex)
+// solves, whose reference order is an inner product per row: x[i] from the
+// x already solved, rows in sequence.
+//   FORWARD (U^T): i = 0 .. n-1, the product over rows [0, i) of column i of
+//     the factor; backward (L^T / L^H): i = n-1 .. 0, over rows (i, n).
+// Real (Triangular.SolveUpperTransposed / SolveLowerTransposed /
+// SolveLowerUnitTransposed, Triangular.cs:152-206): x[i] = (x[i] - Dot) / f_ii,
+// or x[i] -= Dot on a unit triangle, with ColumnOps.Dot's order: one half-warp
+// per right-hand side, lane L holding the 4-lane vector partials
+// (netdot_combine), then the scalar tail in order.
+// Complex, unit, backward (BlockedLu.SolveLowerUnitAdjoint, BlockedLu.cs:357-373):
+// sum = x[i]; sum -= conj(f_ki) x[k] for k ascending; one thread per
+// right-hand side.
+// ---------------------------------------------------------------------------
+template <bool FORWARD, bool UNIT>
+__global__ void __launch_bounds__(128) left_subst_real_kernel(const double* __restrict__ f, int ldf, double* x, int ldx,
+                                                             int n, int nrhs) {
+    const int half = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 4);
+    const int L = threadIdx.x & 15, base = threadIdx.x & 16;
+    // A half-warp past the last column reads column 0 and drops its results,
+    // so that every shuffle sees a converged warp.
+    const bool active = half < nrhs;
+    double* y = x + (size_t)(active ? half : 0) * ldx;
+    constexpr int W = 4;
+    for (int step = 0; step < n; ++step) {
+        const int i = FORWARD ? step : n - 1 - step;
+        const int off = FORWARD ? 0 : i + 1;
+        const int len = FORWARD ? i : n - i - 1;
+        const double* a = f + (size_t)i * ldf + off;
+        const double* yy = y + off;
+        const int n16 = (len / (4 * W)) * (4 * W);
+        const int n4 = len >= W ? n16 + ((len - n16) / W) * W : 0;
+        double total = 0.0;
+        if (len >= W) {
+            double acc = 0.0;
+            for (int p = L; p < n16; p += 16) acc = add_rn(acc, mul_rn(a[p], yy[p]));
+            if (L < W)
+                for (int p = n16 + L; p < n4; p += W) acc = add_rn(acc, mul_rn(a[p], yy[p]));
+            total = netdot_combine(acc, L, base);
+        }
+        if (L == 0) {
+            for (int p = n4; p < len; ++p) total = add_rn(total, mul_rn(a[p], yy[p]));
+            if (active) {
+                double v = sub_rn(y[i], total);
+                if (!UNIT) v = __ddiv_rn(v, f[(size_t)i * ldf + i]);
+                y[i] = v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(64) left_subst_cplx_unit_back_kernel(const double* __restrict__ f, int ldf, double* x,
+                                                                       int ldx, int n, int nrhs) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= nrhs) return;
+    double* y = x + (size_t)col * ldx * 2;
+    for (int i = n - 1; i >= 0; --i) {
+        const double* a = f + (size_t)i * ldf * 2;
+        Z sum = zload(y + (size_t)i * 2);
+        for (int k = i + 1; k < n; ++k) {
+            const Z fk = zload(a + (size_t)k * 2);
+            // conj(f) * x in .NET's product order, then sum - product
+            const Z p = zmul(Z{fk.re, -fk.im}, zload(y + (size_t)k * 2));
+            sum = Z{sub_rn(sum.re, p.re), sub_rn(sum.im, p.im)};
+        }
+        zstore(y + (size_t)i * 2, sum);
+    }
+}
+
+// One left-looking solve (see left_subst_real_kernel): real forward U^T
+// (unit = false) or backward L^T (unit or not); complex: backward L^H, unit.
+void left_substitute(Context& ctx, bool cplx, bool forward, bool unit, const double* f, int ldf, double* x, int ldx,
+                     int n, int nrhs) {
+    if (n == 0 || nrhs == 0) return;
+    if (!cplx) {
+        const unsigned grid = (unsigned)((nrhs * 16 + 127) / 128);
+        if (forward && !unit) left_subst_real_kernel<true, false><<<grid, 128, 0, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        else if (!forward && unit) left_subst_real_kernel<false, true><<<grid, 128, 0, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        else if (!forward && !unit) left_subst_real_kernel<false, false><<<grid, 128, 0, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        else fail(TNS_E_ARGUMENT, "internal: no unit forward transposed solve");
+    } else {
+        if (forward || !unit) fail(TNS_E_ARGUMENT, "internal: complex left-looking solves are backward and unit");
+        left_subst_cplx_unit_back_kernel<<<(unsigned)((nrhs + 63) / 64), 64, 0, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+    }
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
 }
 
 inline size_t off(const DMat& a, int i, int j) { return ((size_t)j * a.ld() + i) * (a.cplx ? 2 : 1); }
@@ -1039,6 +1177,24 @@ void getrf_batch(Context& ctx, std::vector<LuItem>& items) {
         // A whole-matrix panel (Lu.cs:244-249) when it fits one panel launch.
         int steps = (it.nb >= limit && it.n <= 64) ? 1 : (limit + it.nb - 1) / it.nb;
         max_steps = std::max(max_steps, steps);
+    }
+    // LuPhaseTimings (Lu.cs:92-164): CUDA events between the phases of every
+    // block step, when the context collects them; a whole-matrix panel is
+    // not a blocked loop and records nothing, as in the reference.
+    bool blocked = false;
+    for (auto& it : items)
+        if (std::min(it.m, it.n) > 0 && !(it.nb >= std::min(it.m, it.n) && it.n <= 64)) blocked = true;
+    const bool timed = ctx.lu_timing && blocked;
+    cudaEvent_t loop_start = nullptr;
+    std::vector<cudaEvent_t> marks;
+    auto mark = [&]() {
+        cudaEvent_t e = ctx.take_event();
+        TNS_CUDA(cudaEventRecord(e, ctx.stream));
+        marks.push_back(e);
+    };
+    if (timed) {
+        loop_start = ctx.take_event();
+        TNS_CUDA(cudaEventRecord(loop_start, ctx.stream));
     }
     for (int k = 0; k < max_steps; ++k) {
         std::vector<PanelFactorDesc> panels;
@@ -1076,62 +1232,62 @@ void getrf_batch(Context& ctx, std::vector<LuItem>& items) {
             p.work = (long long)(m - jb - w) * (n - jb - w) * w;
             gemms.push_back(p);
         }
+        if (timed) mark();
         launch_panels(ctx, cplx, panels);
+        if (timed) mark();
         launch_laswp(ctx, cplx, swaps);
+        if (timed) mark();
         launch_trsm(ctx, cplx, 0, trsms);
+        if (timed) mark();
         if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
+        if (timed) mark();
+    }
+    if (timed) {
+        cudaEvent_t loop_end = ctx.take_event();
+        TNS_CUDA(cudaEventRecord(loop_end, ctx.stream));
+        TNS_CUDA(cudaStreamSynchronize(ctx.stream));
+        auto ms = [](cudaEvent_t a, cudaEvent_t b) {
+            float v = 0.f;
+            TNS_CUDA(cudaEventElapsedTime(&v, a, b));
+            return (double)v;
+        };
+        for (size_t q = 0; q + 5 <= marks.size(); q += 5) {
+            ctx.lu_panel_ms += ms(marks[q], marks[q + 1]);
+            ctx.lu_swaps_ms += ms(marks[q + 1], marks[q + 2]);
+            ctx.lu_triangular_ms += ms(marks[q + 2], marks[q + 3]);
+            ctx.lu_gemm_ms += ms(marks[q + 3], marks[q + 4]);
+        }
+        ctx.lu_total_ms += ms(loop_start, loop_end);
+        ctx.lu_block_steps += max_steps;
+        ctx.lu_factorizations += (long long)items.size();
+        for (cudaEvent_t e : marks) ctx.event_pool.push_back(e);
+        ctx.event_pool.push_back(loop_start);
+        ctx.event_pool.push_back(loop_end);
     }
 }
 
 void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
     if (items.empty()) return;
     const bool cplx = items[0].lu->cplx;
-    const int bs = 64;
-    const size_t es = cplx ? 2 : 1;
-    int max_blocks = 0;
-    std::vector<DMat> herm;  // conjugate transposes for the adjoint solves
-    for (auto& it : items) {
-        int n = it.lu->rows;
-        if (n == 0 || it.nrhs == 0) continue;
-        max_blocks = std::max(max_blocks, (n + bs - 1) / bs);
-    }
-    if (adjoint) {
+    std::vector<DMat> herm;  // conjugate transposes for the complex adjoint solves
+    if (adjoint && cplx) {
         herm.reserve(items.size());
         for (auto& it : items) {
             herm.emplace_back(ctx, it.lu->cols, it.lu->rows, cplx, "the conjugate transpose of the factors");
             conj_transpose(ctx, herm.back(), *it.lu);
         }
     }
-    auto update = [&](std::vector<GemmProblem>& v, const double* A, int lda, const double* X, double* C, int ldb,
-                      int rows, int k, int nrhs) {
-        if (rows <= 0) return;
-        GemmProblem p{};
-        p.A = A;
-        p.B = X;
-        p.C = C;
-        p.lda = lda;
-        p.ldb = p.ldc = ldb;
-        p.M = round_up(rows, 2);
-        p.N = round_up(nrhs, 2);
-        p.K = round_up(k, 16);
-        p.alpha_re = -1.0;
-        p.beta_re = 1.0;
-        v.push_back(p);
-    };
     if (!adjoint) {
         // P B, then L (unit lower) forward and U backward by substitution in
         // the reference's order (Lu.Solve, Lu.cs:336-351; BlockedLu.Solve,
         // BlockedLu.cs:105-118): the result matches the reference bit for bit.
         std::vector<LaswpDesc> swaps;
         std::vector<SolveItem*> narrow;
-        constexpr int B = kSubstBlock;
-        int steps = 0;
         for (auto& it : items) {
             int n = it.lu->rows;
             if (n == 0 || it.nrhs == 0) continue;
             if (it.nrhs < kGatherMaxCols && n <= kGatherMaxRows) narrow.push_back(&it);
             else swaps.push_back(LaswpDesc{it.b->p, it.b->ld(), 0, it.nrhs, it.d_piv, 0, n, 0});
-            steps = std::max(steps, (n + B - 1) / B);
         }
         launch_laswp(ctx, cplx, swaps);
         if (!narrow.empty()) {
@@ -1178,70 +1334,33 @@ void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint) {
                                          (size_t)narrow[q]->b->ld() * narrow[q]->nrhs * narrow[q]->b->esz(),
                                          cudaMemcpyDeviceToDevice, ctx.stream));
         }
-        // Lower: blocks from the top; upper: each item's blocks from its last.
-        for (int upper = 0; upper < 2; ++upper)
-            for (int s = 0; s < steps; ++s) {
-                std::vector<SubstDiagDesc> diag;
-                std::vector<SubstUpdateDesc> upd;
-                for (auto& it : items) {
-                    const int n = it.lu->rows;
-                    if (n == 0 || it.nrhs == 0) continue;
-                    const int blocks = (n + B - 1) / B;
-                    if (s >= blocks) continue;
-                    const int k0 = (upper ? blocks - 1 - s : s) * B, w = std::min(B, n - k0);
-                    const int ldf = it.lu->ld(), ldx = it.b->ld();
-                    diag.push_back(SubstDiagDesc{it.lu->p, ldf, it.b->p, ldx, it.nrhs, k0, w});
-                    const int r0 = upper ? 0 : k0 + w, r1 = upper ? k0 : n;
-                    if (r1 > r0)
-                        upd.push_back(SubstUpdateDesc{it.lu->p, ldf, it.b->p, ldx, it.nrhs, r0, r1, k0, k0 + w,
-                                                      (r1 - r0 + 63) / 64, 0});
-                }
-                launch_subst_step(ctx, cplx, upper != 0, diag, upd);
-            }
+        std::vector<SubstItem> subst;
+        for (auto& it : items)
+            if (it.lu->rows > 0 && it.nrhs > 0)
+                subst.push_back(SubstItem{it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), it.lu->rows, it.nrhs});
+        substitute(ctx, cplx, false, false, subst);  // L, unit diagonal, forward
+        substitute(ctx, cplx, true, false, subst);   // U, backward
         return;
     }
-    // The adjoint: blocked, 64-row diagonal blocks plus DMMA GEMM updates.
-    // Pass 1: forward (U^H, non-unit).
-    for (int kb = 0; kb < max_blocks; ++kb) {
-        std::vector<TrsmDesc> diag;
-        std::vector<GemmProblem> gemms;
-        for (size_t q = 0; q < items.size(); ++q) {
-            auto& it = items[q];
-            const DMat& F = *it.lu;
-            int n = F.rows, ld = F.ld(), ldb = it.b->ld();
-            int k0 = kb * bs;
-            if (n == 0 || it.nrhs == 0 || k0 >= n) continue;
-            int w = std::min(bs, n - k0);
-            double* B = it.b->p;
-            diag.push_back(TrsmDesc{F.p + ((size_t)k0 * ld + k0) * es, ld, B + (size_t)k0 * es, ldb, w, it.nrhs, 1,
-                                    adjoint ? 0 : 1, adjoint ? 1 : 0});
-            const double* A = adjoint ? herm[q].p + ((size_t)k0 * herm[q].ld() + k0 + w) * es
-                                      : F.p + ((size_t)k0 * ld + k0 + w) * es;
-            update(gemms, A, adjoint ? herm[q].ld() : ld, B + (size_t)k0 * es, B + (size_t)(k0 + w) * es, ldb,
-                   n - k0 - w, w, it.nrhs);
+    // The adjoint in the reference's order (Lu.SolveTransposed, Lu.cs:364-378;
+    // BlockedLu.SolveAdjoint, BlockedLu.cs:130-141): U^H forward, then L^H
+    // backward, then the interchanges undone.
+    for (size_t q = 0; q < items.size(); ++q) {
+        auto& it = items[q];
+        const int n = it.lu->rows;
+        if (n == 0 || it.nrhs == 0) continue;
+        if (!cplx) {
+            // Both by inner products in ColumnOps.Dot's order.
+            left_substitute(ctx, false, true, false, it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs);
+            left_substitute(ctx, false, false, true, it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs);
+        } else {
+            // U^H: its sums run in ascending k, which a right-looking sweep over
+            // the conjugate transpose reproduces; L^H: ascending k inside a
+            // backward sweep, one inner product per row.
+            std::vector<SubstItem> fwd{SubstItem{herm[q].p, herm[q].ld(), it.b->p, it.b->ld(), n, it.nrhs}};
+            substitute(ctx, true, false, true, fwd);
+            left_substitute(ctx, true, false, true, it.lu->p, it.lu->ld(), it.b->p, it.b->ld(), n, it.nrhs);
         }
-        launch_trsm(ctx, cplx, 1, diag);
-        if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
-    }
-    // Pass 2: backward (U, non-unit; or L^H, unit, for the adjoint).
-    for (int kb = max_blocks - 1; kb >= 0; --kb) {
-        std::vector<TrsmDesc> diag;
-        std::vector<GemmProblem> gemms;
-        for (size_t q = 0; q < items.size(); ++q) {
-            auto& it = items[q];
-            const DMat& F = *it.lu;
-            int n = F.rows, ld = F.ld(), ldb = it.b->ld();
-            int k0 = kb * bs;
-            if (n == 0 || it.nrhs == 0 || k0 >= n) continue;
-            int w = std::min(bs, n - k0);
-            double* B = it.b->p;
-            diag.push_back(TrsmDesc{F.p + ((size_t)k0 * ld + k0) * es, ld, B + (size_t)k0 * es, ldb, w, it.nrhs, 0,
-                                    adjoint ? 1 : 0, adjoint ? 1 : 0});
-            const double* A = adjoint ? herm[q].p + ((size_t)k0 * herm[q].ld()) * es : F.p + ((size_t)k0 * ld) * es;
-            update(gemms, A, adjoint ? herm[q].ld() : ld, B + (size_t)k0 * es, B, ldb, k0, w, it.nrhs);
-        }
-        launch_trsm(ctx, cplx, 1, diag);
-        if (!gemms.empty()) gemm_grouped(ctx, gemms, cplx);
     }
     if (adjoint) {
         std::vector<LaswpDesc> swaps;
@@ -1283,6 +1402,38 @@ LuResult getrf(Context& ctx, DMat& a, int m, int n, int nb, int* d_piv) {
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint) {
     std::vector<SolveItem> items{SolveItem{&lu, d_piv, &b, nrhs}};
     getrs_batch(ctx, items, adjoint);
+}
+
+void solve_triangular(Context& ctx, TriangularKind kind, const DMat& f, DMat& b, int nrhs) {
+    const int n = f.rows;
+    if (n == 0 || nrhs == 0) return;
+    const bool cplx = f.cplx;
+    std::vector<SubstItem> it{SubstItem{f.p, f.ld(), b.p, b.ld(), n, nrhs}};
+    switch (kind) {
+        case TriangularKind::kUpper: substitute(ctx, cplx, true, false, it); break;
+        case TriangularKind::kLowerUnit: substitute(ctx, cplx, false, false, it); break;
+        case TriangularKind::kLower:
+            if (cplx) fail(TNS_E_ARGUMENT, "internal: no complex explicit-diagonal lower solve");
+            substitute(ctx, false, false, true, it);
+            break;
+        case TriangularKind::kUpperTransposed:
+            if (!cplx) {
+                left_substitute(ctx, false, true, false, f.p, f.ld(), b.p, b.ld(), n, nrhs);
+            } else {
+                DMat h(ctx, f.cols, f.rows, true, "the conjugate transpose of a triangle");
+                conj_transpose(ctx, h, f);
+                std::vector<SubstItem> fw{SubstItem{h.p, h.ld(), b.p, b.ld(), n, nrhs}};
+                substitute(ctx, true, false, true, fw);
+            }
+            break;
+        case TriangularKind::kLowerTransposed:
+            if (cplx) fail(TNS_E_ARGUMENT, "internal: no complex explicit-diagonal lower solve");
+            left_substitute(ctx, false, false, false, f.p, f.ld(), b.p, b.ld(), n, nrhs);
+            break;
+        case TriangularKind::kLowerUnitTransposed:
+            left_substitute(ctx, cplx, false, true, f.p, f.ld(), b.p, b.ld(), n, nrhs);
+            break;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -74,9 +74,17 @@ extern "C" int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const
         require((a || (long long)m * k == 0) && (b || (long long)k * n == 0) && (c || (long long)m * n == 0),
                 TNS_E_NULL, "an operand is null");
         if (m == 0 || n == 0) return TNS_OK;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (k == 0) {
+            // No product: C := beta*C, as tns_zgemm_device does; alpha is not
+            // read, so a non-finite alpha leaves C finite here too.
+            tns::scale_detached(s, c, m, n, ldc, true, beta[0], beta[1]);
+            TNS_CUDA(cudaStreamSynchronize(s));
+            return TNS_OK;
+        }
         // Padded extents: the kernel's tiles want M even and K a multiple of 16.
         const size_t mp = (size_t)tns::round_up(m, 2), np = (size_t)tns::round_up(n, 2);
-        const size_t kp = (size_t)tns::round_up(std::max(k, 1), 16);
+        const size_t kp = (size_t)tns::round_up(k, 16);
         const bool plain = alpha[0] == 1.0 && alpha[1] == 0.0 && beta[0] == 0.0 && beta[1] == 0.0;
         const size_t need = mp * kp + kp * np + mp * np + (plain ? 0 : mp * np);
         if (need > kNoAllocMaxElements)
@@ -88,7 +96,6 @@ extern "C" int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const
         int device = 0;
         TNS_CUDA(cudaGetDevice(&device));
         DeviceSlot& slot = device_slot(device);
-        cudaStream_t s = static_cast<cudaStream_t>(stream);
 
         double2* ap = slot.scratch;
         double2* bp = ap + mp * kp;
@@ -97,12 +104,10 @@ extern "C" int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const
         // The array keeps the previous call's contents: clear the operands'
         // padding (and everything else in them) before copying in.
         TNS_CUDA(cudaMemsetAsync(ap, 0, (mp * kp + kp * np) * sizeof(double2), s));
-        if (k > 0) {
-            TNS_CUDA(cudaMemcpy2DAsync(ap, mp * sizeof(double2), a, (size_t)lda * sizeof(double2), (size_t)m * sizeof(double2),
-                                       k, cudaMemcpyDeviceToDevice, s));
-            TNS_CUDA(cudaMemcpy2DAsync(bp, kp * sizeof(double2), b, (size_t)ldb * sizeof(double2), (size_t)k * sizeof(double2),
-                                       n, cudaMemcpyDeviceToDevice, s));
-        }
+        TNS_CUDA(cudaMemcpy2DAsync(ap, mp * sizeof(double2), a, (size_t)lda * sizeof(double2), (size_t)m * sizeof(double2),
+                                   k, cudaMemcpyDeviceToDevice, s));
+        TNS_CUDA(cudaMemcpy2DAsync(bp, kp * sizeof(double2), b, (size_t)ldb * sizeof(double2), (size_t)k * sizeof(double2),
+                                   n, cudaMemcpyDeviceToDevice, s));
         if (!(beta[0] == 0.0 && beta[1] == 0.0))
             TNS_CUDA(cudaMemcpy2DAsync(cp, mp * sizeof(double2), c, (size_t)ldc * sizeof(double2), (size_t)m * sizeof(double2),
                                        n, cudaMemcpyDeviceToDevice, s));
@@ -125,15 +130,19 @@ extern "C" int tns_zgemm_device_noalloc(void* stream, int m, int n, int k, const
         p.W = wp;
         p.ldw = (int)mp;
         tns::gemm_detached_complex(s, device, slot.error, p);
+        // The product stays in the array until the kernel's wait flag has been
+        // read: a wait that gave up leaves the caller's C untouched.
+        int flag = 0;
+        TNS_CUDA(cudaMemcpyAsync(&flag, slot.error, sizeof(int), cudaMemcpyDeviceToHost, s));
+        TNS_CUDA(cudaStreamSynchronize(s));
+        if (flag != 0) {
+            TNS_CUDA(cudaMemsetAsync(slot.error, 0, sizeof(int), s));
+            TNS_CUDA(cudaStreamSynchronize(s));
+            tns::fail(TNS_E_TIMEOUT, "a device-side wait gave up (code " + std::to_string(flag) + ")");
+        }
         TNS_CUDA(cudaMemcpy2DAsync(c, (size_t)ldc * sizeof(double2), cp, mp * sizeof(double2), (size_t)m * sizeof(double2), n,
                                    cudaMemcpyDeviceToDevice, s));
         TNS_CUDA(cudaStreamSynchronize(s));
-        int flag = 0;
-        TNS_CUDA(cudaMemcpy(&flag, slot.error, sizeof(int), cudaMemcpyDeviceToHost));
-        if (flag != 0) {
-            TNS_CUDA(cudaMemset(slot.error, 0, sizeof(int)));
-            tns::fail(TNS_E_TIMEOUT, "a device-side wait gave up (code " + std::to_string(flag) + ")");
-        }
         return TNS_OK;
     } catch (const tns::Error& e) {
         tns::set_detached_error(e.what());

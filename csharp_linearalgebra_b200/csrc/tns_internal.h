@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -120,6 +121,12 @@ struct Context {
     void* scratch(size_t bytes);
     cudaEvent_t take_event();
     void drain_events();        // sums finished event pairs into gemm_ms_done / split_ms_done
+
+    // LuPhaseTimings' device counterpart (tns_set_lu_timing): CUDA-event time
+    // of the blocked LU's phases, summed over the factorizations timed.
+    bool lu_timing = false;
+    double lu_panel_ms = 0.0, lu_swaps_ms = 0.0, lu_triangular_ms = 0.0, lu_gemm_ms = 0.0, lu_total_ms = 0.0;
+    long long lu_block_steps = 0, lu_factorizations = 0;
 
     // Batched work runs on worker contexts (one host thread and one stream
     // each), created on first use, so that independent matrices overlap on
@@ -257,6 +264,8 @@ void panel_product_batch(Context& ctx, std::vector<PanelDesc>& v, bool cplx, boo
 
 // ---- elementwise and reductions (blas1.cu) ---------------------------------
 void scale_inplace(Context& ctx, void* c, int m, int n, int ldc, bool cplx, double beta_re, double beta_im);
+// C := beta*C on a caller's stream without a context (nothing allocated).
+void scale_detached(cudaStream_t stream, double* c, int m, int n, int ldc, bool cplx, double beta_re, double beta_im);
 // dst := src * f (real factor, each part scaled on its own), whole padded extent.
 void scaled_copy(Context& ctx, DMat& dst, const DMat& src, double f);
 // t := t + s * f
@@ -309,6 +318,13 @@ struct SolveItem {
 void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint);
 // B := A^-1 B or A^-H B from factors (valid n x n), in place on the valid rows of b.
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
+// The triangular solves of the reference's kernel seam (KernelEntry.cs:98-173,
+// Triangular.cs) in its order of operations: B := T^-1 B or T^-T B in place
+// for the triangle of f named by kind (real); complex: the unit lower, upper
+// and their adjoints (BlockedLu.cs:283-373), "transposed" meaning the
+// conjugate transpose.
+enum class TriangularKind { kUpper, kUpperTransposed, kLower, kLowerTransposed, kLowerUnit, kLowerUnitTransposed };
+void solve_triangular(Context& ctx, TriangularKind kind, const DMat& f, DMat& b, int nrhs);
 
 // The precision form of the solve: LU whose trailing updates (depth 512) run
 // on the split-precision product with `moduli` moduli, panels of 512 columns
@@ -341,7 +357,26 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
 struct ExpmvInfo {
     int degree = 0, scaling = 0, applications = 0, early_exits = 0;
 };
+// exp(tA)B for dense A (MatrixExponentialAction.Dense + Run): the parameters
+// on the host, the Taylor recurrence in the fused device kernel (a batch of one).
 void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info);
+// The same for a batch of independent (A_k, B_k), every B_k with the same
+// column count; the Taylor recurrences of all matrices run in one cooperative
+// launch (expmv_batched.cu).
+void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::vector<const DMat*>& bs, double t,
+                 std::vector<DMat>& results, std::vector<ExpmvInfo>& infos);
+// The earlier host-driven form of the dense path: every application a panel
+// product launch, the norms read back to the host (kept as the reference
+// point for the fused kernel, and for panels wider than it takes).
+void expmv_host_loop(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, ExpmvInfo* info);
+void expmv_taylor_host(Context& ctx, const DMat& shifted, const DMat& b, double t, int m, int s, double eta_re,
+                       double eta_im, DMat& result, ExpmvInfo* info);
+// MatrixExponentialAction.SelectParameters (:347-398).
+void expmv_select_parameters(double scaled_norm, const std::function<double(int)>* alpha, double scale, int cols,
+                             int& m, int& s);
+// normest1 (t = 2, itmax = 5, the default seed) of A_k^power for a set of
+// matrices, every estimator's product step in one launch.
+std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power);
 // The matrix-free form: y := A x by a caller's function on device panels.
 using ApplyFn = int (*)(void* user, int ncols, const double* x, double* y, int ld, void* stream);
 void expmv_operator(Context& ctx, int n, ApplyFn apply, void* user, const DMat& b, double t, double bound,

@@ -154,6 +154,46 @@ int tns_dgetrs(tns_context* ctx, int n, int nrhs, const double* lu, int lda, con
 int tns_zgetrs(tns_context* ctx, int n, int nrhs, const double* lu, int lda, const int* pivots,
                int singular_column, double* b, int ldb, int adjoint);
 
+/* The triangular solves of the kernel seam, in place: B := T^-1 B (or
+ * T^-T B) for the m x m triangle T of A that the name gives (the other part of
+ * A is not read), B m x n, in the reference's order of operations (column
+ * axpys for the untransposed solves, ColumnOps.Dot inner products for the
+ * transposed ones), so the result is the reference's bit for bit. A zero on
+ * the diagonal divides by zero as the reference does (no error).
+ * KernelEntry.SolveUpper, SolveUpperTransposed, SolveLower,
+ * SolveLowerTransposed, SolveLowerUnit, SolveLowerUnitTransposed
+ * (src/Tensile.Kernels/KernelEntry.cs:98-173; src/Tensile.Kernels/Triangular.cs:26-206),
+ * as Structures.cs's UpperTriangular / LowerTriangular / UnitLowerTriangular
+ * call them (src/Tensile/Structures.cs:96-167). */
+int tns_dsolve_upper(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_dsolve_upper_transposed(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_dsolve_lower(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_dsolve_lower_transposed(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_dsolve_lower_unit(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_dsolve_lower_unit_transposed(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+/* The complex triangular solves the reference runs above its seam, in their
+ * order of operations: BlockedLu.SolveUpper, SolveUpperAdjoint (U^H),
+ * SolveLowerUnit, SolveLowerUnitAdjoint (L^H) (src/Tensile/BlockedLu.cs:283-373). */
+int tns_zsolve_upper(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_zsolve_upper_adjoint(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_zsolve_lower_unit(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+int tns_zsolve_lower_unit_adjoint(tns_context* ctx, int m, int n, const double* a, int lda, double* b, int ldb);
+
+/* Y := A X or Y := A^T X for square A (n x n) and panels X, Y (n x t).
+ * KernelEntry.MultiplyPanel / MultiplyPanelTransposed
+ * (src/Tensile.Kernels/KernelEntry.cs:176-201; PanelProduct.Apply /
+ * ApplyTranspose, src/Tensile.Kernels/PanelProduct.cs:25-55), in their order
+ * of operations. Complex: Y := A X or A^H X, ComplexDenseOperator.Apply /
+ * ApplyAdjoint (src/Tensile/LinearOperators.cs:194-293). */
+int tns_dmultiply_panel(tns_context* ctx, int n, int t, const double* a, int lda, const double* x, int ldx, double* y,
+                        int ldy);
+int tns_dmultiply_panel_transposed(tns_context* ctx, int n, int t, const double* a, int lda, const double* x, int ldx,
+                                   double* y, int ldy);
+int tns_zmultiply_panel(tns_context* ctx, int n, int t, const double* a, int lda, const double* x, int ldx, double* y,
+                        int ldy);
+int tns_zmultiply_panel_adjoint(tns_context* ctx, int n, int t, const double* a, int lda, const double* x, int ldx,
+                                double* y, int ldy);
+
 /* rcond = 1/(||A||_1 * est ||A^-1||_1), 0 when singular or ||A||_1 == 0.
  * Condition.ReciprocalOne (src/Tensile/NormEstimate.cs:432-466) over
  * LuInverseOperator (src/Tensile/LinearOperators.cs:303-350). */
@@ -224,6 +264,26 @@ int tns_dexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, con
                double t, double* out, int ldo, tns_expmv_info* info);
 int tns_zexpmv(tns_context* ctx, int n, const double* a, int lda, int ncols, const double* b, int ldb,
                double t, double* out, int ldo, tns_expmv_info* info);
+
+/* A batch of exponential actions out[i] = exp(t a[i]) b[i] of independent
+ * orders (every b[i] with ncols columns): the frequency-sweep form of
+ * tns_dexpmv / tns_zexpmv, each matrix with the reference's trace shift,
+ * sharp bounds, (m, s) and early exit. The parameters of all matrices are
+ * chosen together (their normest1 runs advanced in lockstep); the Taylor
+ * recurrences of all of them then run in one cooperative kernel launch, the
+ * early-exit test on the device. Each result is the reference's arithmetic
+ * (MatrixExponentialAction.Run, src/Tensile/MatrixExponentialAction.cs:239-320),
+ * so it equals tns_zexpmv on the same matrix bit for bit. Orders may be 0
+ * (nothing is written). infos may be NULL. _device: device pointers. */
+int tns_dexpmv_batched(tns_context* ctx, int count, const int* orders, const double* const* a, const int* lda,
+                       int ncols, const double* const* b, const int* ldb, double t, double* const* out,
+                       const int* ldo, tns_expmv_info* infos);
+int tns_zexpmv_batched(tns_context* ctx, int count, const int* orders, const double* const* a, const int* lda,
+                       int ncols, const double* const* b, const int* ldb, double t, double* const* out,
+                       const int* ldo, tns_expmv_info* infos);
+int tns_zexpmv_batched_device(tns_context* ctx, int count, const int* orders, const double* const* a,
+                              const int* lda, int ncols, const double* const* b, const int* ldb, double t,
+                              double* const* out, const int* ldo, tns_expmv_info* infos);
 
 /* ---- precision form of the solve ----------------------------------------- */
 
@@ -344,8 +404,11 @@ int tns_znormest1_operator(tns_context* ctx, int n, tns_apply_fn apply, tns_appl
  * (roughly m*k + k*n + 2*m*n complex elements, with m rounded up to even and k
  * to a multiple of 16) is refused with TNS_E_OUT_OF_RANGE; tns_last_error(NULL)
  * says why. There is no context: stream is the caller's cudaStream_t (NULL for
- * the default stream) on the current device, and the call returns when the
- * product is in C.
+ * the default stream) on the current device. Every call waits for that stream
+ * before it returns: it reads the product kernel's wait flag first and copies
+ * the product into C only when no device-side wait gave up (TNS_E_TIMEOUT
+ * leaves C untouched). k == 0 scales C by beta and reads neither alpha nor
+ * the working array, as tns_zgemm_device does.
  *
  * The first call on a device looks up the array's device address, with that
  * device current; make that first call before any stream capture. All calls
@@ -389,6 +452,23 @@ typedef struct {
 } tns_stats;
 
 int tns_get_stats(tns_context* ctx, tns_stats* out); /* waits for the stream */
+
+/* LuPhaseTimings (src/Tensile.Kernels/Lu.cs:92-164) on the device: with
+ * collection switched on, every blocked LU this context runs (tns_dgetrf,
+ * tns_zgetrf and the factorizations inside the solves and exponentials it
+ * runs itself) records CUDA events between its phases -- the panel
+ * factorization, the row interchanges, the triangular solve for U12, the
+ * trailing GEMM -- and around the whole blocked loop. A timed factorization
+ * waits for its stream once at the end. A factorization that is one
+ * whole-matrix panel has no blocked loop and records nothing, as in the
+ * reference. unattributed_ms is total_ms minus the phases, never negative
+ * (LuPhaseTimings.Unattributed). tns_reset_stats clears the sums. */
+typedef struct {
+    double panel_ms, swaps_ms, triangular_ms, gemm_ms, total_ms, unattributed_ms;
+    long long block_steps, factorizations;
+} tns_lu_timings;
+int tns_set_lu_timing(tns_context* ctx, int enabled);
+int tns_get_lu_timings(tns_context* ctx, tns_lu_timings* out);
 int tns_reset_stats(tns_context* ctx);
 int tns_set_timing(tns_context* ctx, int enabled);
 /* The CUDA stream (cudaStream_t) the context issues its work on. */

@@ -87,6 +87,10 @@ def lib():
             getattr(L, name).argtypes = [i, P, i, i, P, i, d, P, i, C.POINTER(ExpmvInfo)]
         for name in ("orc_dexpmv_bound", "orc_zexpmv_bound"):
             getattr(L, name).argtypes = [i, P, i, i, P, i, d, d, P, i, C.POINTER(ExpmvInfo)]
+        for name in ("orc_dtrsolve", "orc_ztrsolve"):
+            getattr(L, name).argtypes = [i, i, i, P, i, P, i]
+        for name in ("orc_dpanel", "orc_zpanel"):
+            getattr(L, name).argtypes = [i, i, i, P, i, P, i, P, i]
         _lib = L
     return _lib
 
@@ -282,3 +286,34 @@ def expmv(a, b, t=1.0):
     assert rc == 0
     res = out[:, 0] if squeeze else out
     return res, {k: getattr(info, k) for k, _ in ExpmvInfo._fields_}
+
+
+# Triangular solve kinds, in the kernel seam's order (KernelEntry.cs:98-173).
+TRI_KINDS = {"upper": 0, "upper_transposed": 1, "lower": 2, "lower_transposed": 3, "lower_unit": 4,
+             "lower_unit_transposed": 5}
+
+
+def trsolve(kind, a, b):
+    """B := T^-1 B (or T^-T B; complex: T^-H B) for the triangle of A named
+    by kind. Returns the solution (a new array)."""
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+    dt = np.complex128 if cplx else np.float64
+    a = _f(a, dt)
+    x = _f(b, dt).copy(order="F")
+    m, n = x.shape
+    fn = lib().orc_ztrsolve if cplx else lib().orc_dtrsolve
+    rc = fn(TRI_KINDS[kind], m, n, _p(a), _ld(a), _p(x), _ld(x))
+    assert rc == 0, f"no {'complex ' if cplx else ''}{kind} solve"
+    return x
+
+
+def panel(a, x, transposed=False):
+    """Y := A X, or A^T X (real) / A^H X (complex) for a panel X."""
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(x)
+    dt = np.complex128 if cplx else np.float64
+    a, x = _f(a, dt), _f(x, dt)
+    n, t = x.shape
+    y = np.zeros((n, t), dtype=dt, order="F")
+    fn = lib().orc_zpanel if cplx else lib().orc_dpanel
+    fn(int(transposed), n, t, _p(a), _ld(a), _p(x), _ld(x), _p(y), _ld(y))
+    return y

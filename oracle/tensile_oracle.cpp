@@ -613,6 +613,30 @@ void solve_upper_transposed(int m, int n, const double* u, int ldu, double* b, i
     }
 }
 
+// src/Tensile.Kernels/Triangular.cs:131-150: explicit diagonal, one column at a time.
+void solve_lower(int m, int n, const double* l, int ldl, double* b, int ldb) {
+    for (int j = 0; j < n; j++) {
+        double* col = b + (size_t)j * ldb;
+        for (int p = 0; p < m; p++) {
+            const double* lp = l + (size_t)p * ldl;
+            col[p] /= lp[p];
+            double v = col[p];
+            if (v != 0.0 && p + 1 < m) col_axpy(m - p - 1, -v, lp + p + 1, col + p + 1);
+        }
+    }
+}
+
+// src/Tensile.Kernels/Triangular.cs:157-168.
+void solve_lower_transposed(int m, int n, const double* l, int ldl, double* b, int ldb) {
+    for (int j = 0; j < n; j++) {
+        double* col = b + (size_t)j * ldb;
+        for (int i = m - 1; i >= 0; i--) {
+            const double* li = l + (size_t)i * ldl;
+            col[i] = (col[i] - col_dot(m - i - 1, li + i + 1, col + i + 1)) / li[i];
+        }
+    }
+}
+
 void solve_lower_unit_transposed(int m, int n, const double* l, int ldl, double* b, int ldb) {
     for (int j = 0; j < n; j++) {
         double* col = b + (size_t)j * ldb;
@@ -1757,6 +1781,56 @@ int orc_zgetrf(int m, int n, double* a, int lda, int nb, int* pivots, orc_lu_inf
     zgetrf_impl(m, n, (cplx*)a, lda, nb, pivots, info);
     return 0;
 }
+// KernelEntry.SolveUpper .. SolveLowerUnitTransposed (src/Tensile.Kernels/KernelEntry.cs:98-173).
+int orc_dtrsolve(int kind, int m, int n, const double* a, int lda, double* b, int ldb) {
+    if (m == 0 || n == 0) return 0;
+    switch (kind) {
+        case 0: solve_upper(m, n, a, lda, b, ldb); return 0;
+        case 1: solve_upper_transposed(m, n, a, lda, b, ldb); return 0;
+        case 2: solve_lower(m, n, a, lda, b, ldb); return 0;
+        case 3: solve_lower_transposed(m, n, a, lda, b, ldb); return 0;
+        case 4: solve_lower_unit(m, n, a, lda, b, ldb); return 0;
+        case 5: solve_lower_unit_transposed(m, n, a, lda, b, ldb); return 0;
+        default: return 1;
+    }
+}
+
+// BlockedLu's generic solves over Complex (src/Tensile/BlockedLu.cs:283-373).
+int orc_ztrsolve(int kind, int m, int n, const double* a, int lda, double* b, int ldb) {
+    if (m == 0 || n == 0) return 0;
+    const cplx* A = reinterpret_cast<const cplx*>(a);
+    cplx* B = reinterpret_cast<cplx*>(b);
+    switch (kind) {
+        case 0: zsolve_upper(m, n, A, lda, B, ldb); return 0;
+        case 1: zsolve_upper_adjoint(m, n, A, lda, B, ldb); return 0;
+        case 4: zsolve_lower_unit(m, n, A, lda, B, ldb); return 0;
+        case 5: zsolve_lower_unit_adjoint(m, n, A, lda, B, ldb); return 0;
+        default: return 1;
+    }
+}
+
+// KernelEntry.MultiplyPanel / MultiplyPanelTransposed (KernelEntry.cs:176-201,
+// PanelProduct.cs:25-55).
+int orc_dpanel(int transposed, int n, int t, const double* a, int lda, const double* x, int ldx, double* y, int ldy) {
+    if (n == 0 || t == 0) return 0;
+    (transposed ? panel_apply_transpose : panel_apply)(n, t, a, lda, x, ldx, y, ldy);
+    return 0;
+}
+
+// ComplexDenseOperator.Apply / ApplyAdjoint at power 1 (src/Tensile/LinearOperators.cs:194-293).
+int orc_zpanel(int adjoint, int n, int t, const double* a, int lda, const double* x, int ldx, double* y, int ldy) {
+    if (n == 0 || t == 0) return 0;
+    DenseComplexOperator op(n, reinterpret_cast<const cplx*>(a), lda, 1);
+    std::vector<cplx> xs((size_t)n * t), ys((size_t)n * t);
+    for (int j = 0; j < t; j++)
+        for (int i = 0; i < n; i++) xs[(size_t)j * n + i] = reinterpret_cast<const cplx*>(x)[(size_t)j * ldx + i];
+    if (adjoint) op.apply_adjoint(xs.data(), ys.data(), t);
+    else op.apply(xs.data(), ys.data(), t);
+    for (int j = 0; j < t; j++)
+        for (int i = 0; i < n; i++) reinterpret_cast<cplx*>(y)[(size_t)j * ldy + i] = ys[(size_t)j * n + i];
+    return 0;
+}
+
 int orc_dgetrs(int n, int nrhs, const double* lu, int lda, const int* pivots, int singular_column,
                double* b, int ldb, int adjoint) {
     if (singular_column >= 0) return 2;

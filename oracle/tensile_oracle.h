@@ -68,6 +68,16 @@ int orc_dgetrs(int n, int nrhs, const double* lu, int lda, const int* pivots, in
 int orc_zgetrs(int n, int nrhs, const double* lu, int lda, const int* pivots, int singular_column,
                double* b, int ldb, int adjoint);
 
+/* Triangular solves of the kernel seam, in place: kind 0 upper, 1 upper^T,
+ * 2 lower, 3 lower^T, 4 unit lower, 5 unit lower^T (Triangular.cs); complex
+ * (BlockedLu's generic solves): 0 upper, 1 upper^H, 4 unit lower, 5 unit
+ * lower^H. Returns 1 for an unknown kind. */
+int orc_dtrsolve(int kind, int m, int n, const double* a, int lda, double* b, int ldb);
+int orc_ztrsolve(int kind, int m, int n, const double* a, int lda, double* b, int ldb);
+/* Y := A X or A^T X (PanelProduct); complex: the dense operator's A X / A^H X. */
+int orc_dpanel(int transposed, int n, int t, const double* a, int lda, const double* x, int ldx, double* y, int ldy);
+int orc_zpanel(int adjoint, int n, int t, const double* a, int lda, const double* x, int ldx, double* y, int ldy);
+
 /* ---- Higham-Tisseur block 1-norm estimator ------------------------------ */
 typedef struct {
     double value;

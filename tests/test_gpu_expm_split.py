@@ -9,8 +9,8 @@ rounding) in the 1-norm. The bar is 1e-12, except where the problem itself
 cannot be computed that closely by any arithmetic that is not the
 reference's bit for bit. That level is measured per matrix as the floor: the
 change of the plain FP64 result when the input is perturbed by about one
-unit in the last place. The split result must lie within 4 x the floor, and
-within 1e-12 whenever 4 x the floor is below it. The floor grows with the
+unit in the last place. The split result must lie within SPLIT_FLOOR_FACTOR
+x the floor, and within 1e-12 whenever that is below it. The floor grows with the
 squarings (about 2^s u): under 1e-13 up to s = 10, above 1e-12 from s = 15.
 """
 import math
@@ -23,6 +23,11 @@ from conftest import rel1
 pytestmark = pytest.mark.gpu
 
 MODULI = 20
+# The bar against the oracle, in units of the matrix's FP64 floor. The split
+# form is as close to exp(A) itself as the reference is (within a factor 2,
+# tests/test_gpu_expm_truth.py), and the reference's own distance to exp(A)
+# is a few floors, so the two results can be several floors apart.
+SPLIT_FLOOR_FACTOR = 6.0
 
 
 @pytest.fixture(params=[18, 20])
@@ -36,6 +41,11 @@ def split_ws(ws, request):
     finally:
         ws.set_split_moduli(0)
         MODULI = 20
+# The bar against the oracle, in units of the matrix's FP64 floor. The split
+# form is as close to exp(A) itself as the reference is (within a factor 2,
+# tests/test_gpu_expm_truth.py), and the reference's own distance to exp(A)
+# is a few floors, so the two results can be several floors apart.
+SPLIT_FLOOR_FACTOR = 6.0
 
 
 def sweep_matrix(rng, n, w):
@@ -60,7 +70,7 @@ def floor_of(ws, a, ref):
 
 def check(ws, a, e, d, ref, info):
     assert (d.degree, d.squarings) == (info["degree"], info["squarings"])
-    bar = max(1e-12, 4.0 * floor_of(ws, a, ref))
+    bar = max(1e-12, SPLIT_FLOOR_FACTOR * floor_of(ws, a, ref))
     assert rel1(e, ref) <= bar, (rel1(e, ref), bar)
 
 

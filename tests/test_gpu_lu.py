@@ -82,6 +82,9 @@ def test_solves_match_oracle(ws, orc, n, nrhs):
     f, piv, info = orc.getrf(a)
     assert relfro(x, orc.getrs(f, piv, b)) < 1e-12
     assert relfro(xt, orc.getrs(f, piv, b, adjoint=True)) < 1e-12
+    # both solves keep the reference's order of operations: the same bits
+    assert np.array_equal(x, orc.getrs(f, piv, b))
+    assert np.array_equal(xt, orc.getrs(f, piv, b, adjoint=True))
     # backward error ||Ax - b||_inf / (||A||_inf ||x||_inf) (LuTests.cs:69-105)
     assert np.abs(a @ x - b).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max()) < 1e-12
 
@@ -95,6 +98,8 @@ def test_complex_solves_match_oracle(ws, orc, n, nrhs):
     f, piv, _ = orc.getrf(a)
     assert relfro(lu.solve(b), orc.getrs(f, piv, b)) < 1e-12
     assert relfro(lu.solve_adjoint(b), orc.getrs(f, piv, b, adjoint=True)) < 1e-12
+    assert np.array_equal(lu.solve(b), orc.getrs(f, piv, b))
+    assert np.array_equal(lu.solve_adjoint(b), orc.getrs(f, piv, b, adjoint=True))
     x = lu.solve(b)
     # complex solve backward error (ComplexLuTests.cs:126-133)
     assert np.abs(a @ x - b).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max()) < 1e-14 * n
@@ -111,7 +116,9 @@ def test_rcond_matches_oracle(ws, orc, n, cplx):
     f, piv, info = orc.getrf(a)
     r = lu.reciprocal_condition()
     ro = orc.gecon(f, piv, -1, orc.norm1(a))
-    assert r == pytest.approx(ro, rel=1e-10)
+    # every solve the estimator probes with is the reference's bit for bit
+    # (adjoint ones included), so the estimate is the oracle's exactly
+    assert r == ro
     exact = 1.0 / (np.linalg.norm(a, 1) * np.linalg.norm(np.linalg.inv(a), 1))
     assert exact * (1 - 1e-10) <= r <= 3 * exact
 
@@ -120,3 +127,31 @@ def test_determinant(ws):
     rng = np.random.default_rng(5)
     a = rng.standard_normal((12, 12))
     assert ws.factor_lu(a).determinant() == pytest.approx(np.linalg.det(a), rel=1e-12)
+
+
+def test_lu_phase_timings(ws, orc):
+    """LuPhaseTimings' counterpart: the four phases and the unattributed rest
+    add up to the loop's total, one block step per panel; a one-panel LU
+    records nothing; the factors are unchanged by the timing."""
+    rng = np.random.default_rng(77)
+    n = 512  # reference block size 32: 16 block steps
+    a = rng.uniform(-0.5, 0.5, (n, n))
+    ws.reset_stats()
+    ws.set_lu_timing(True)
+    try:
+        lu = ws.factor_lu(a)
+        t = ws.lu_timings()
+        small = ws.factor_lu(rng.uniform(-0.5, 0.5, (20, 20)))  # one whole-matrix panel
+        t2 = ws.lu_timings()
+    finally:
+        ws.set_lu_timing(False)
+    f, piv, _ = orc.getrf(a)
+    assert np.array_equal(lu.factors, f) and np.array_equal(lu.pivots, piv)
+    assert t["factorizations"] == 1 and t["block_steps"] == 16
+    phases = t["panel_ms"] + t["swaps_ms"] + t["triangular_ms"] + t["gemm_ms"]
+    assert all(t[k] > 0 for k in ("panel_ms", "swaps_ms", "triangular_ms", "gemm_ms"))
+    assert phases <= t["total_ms"] * 1.001 + 1e-3
+    assert t["unattributed_ms"] == pytest.approx(max(0.0, t["total_ms"] - phases), abs=1e-9)
+    assert t2 == t and small.rows == 20
+    ws.reset_stats()
+    assert ws.lu_timings()["total_ms"] == 0.0
