@@ -8,9 +8,12 @@ distributions of the batching configuration. Metric: expm/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU (torchrun, one process per GPU): every rank runs its own sweep
-(weak scaling, independent matrices, no collective on the data path); the
-time is the max over ranks.
+Multi-GPU (torchrun, one process per GPU): the job is one sweep of 256 x N
+matrices, partitioned over the N ranks by LPT on the estimated cost
+n^3 (log2 w + 8) (csharp_linearalgebra_b200.sweep); each rank builds and
+runs its own part (weak scaling: 256 matrices' worth per GPU, no collective
+on the data path) and the time is the max over ranks. --shard seeds gives
+every rank its own 256-matrix sweep instead.
 
 Two forms run on the same sweep. The split-precision form (`value`, `e2e`,
 `roofline`) computes the Pade-evaluation and squaring products from 8-bit
@@ -54,21 +57,31 @@ WORKLOAD = ("frequency sweep of 256 complex128 matrices A_k = -(G + i w_k C), n_
             "G ~ N(0,1)/sqrt(n), C = Q^T D Q (D log-uniform [1e-3,1]), w_k log-spaced 1e2..1e6; Expm of each")
 
 
-def make_sweep(count: int, seed: int):
-    """The seeded synthetic sweep: list of (n, complex128 Fortran array)."""
-    rng = np.random.default_rng(seed)
-    orders = rng.integers(64, 1025, size=count)
-    omegas = np.logspace(2.0, 6.0, count)
-    mats = []
-    for n, w in zip(orders, omegas):
-        n = int(n)
-        g = rng.standard_normal((n, n)) / math.sqrt(n)
-        q, _ = np.linalg.qr(rng.standard_normal((n, n)))
-        d = np.exp(rng.uniform(math.log(1e-3), 0.0, n))
-        c = (q.T * d) @ q
-        c = 0.5 * (c + c.T)
-        mats.append(np.asfortranarray(-(g + 1j * w * c)))
-    return [int(n) for n in orders], mats
+def sweep_spec(count: int, seed: int):
+    """Orders and frequencies of the seeded sweep: n_k ~ U{64..1024}, w_k
+    log-spaced 1e2..1e6."""
+    orders = np.random.default_rng(seed).integers(64, 1025, size=count)
+    return [int(n) for n in orders], np.logspace(2.0, 6.0, count)
+
+
+def sweep_matrix(k: int, n: int, w: float, seed: int):
+    """Matrix k of the sweep, A = -(G + i w C), from its own seeded stream, so
+    that any rank can build any subset of the sweep on its own."""
+    rng = np.random.default_rng([seed, k])
+    g = rng.standard_normal((n, n)) / math.sqrt(n)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    d = np.exp(rng.uniform(math.log(1e-3), 0.0, n))
+    c = (q.T * d) @ q
+    c = 0.5 * (c + c.T)
+    return np.asfortranarray(-(g + 1j * w * c))
+
+
+def make_sweep(count: int, seed: int, indices=None):
+    """The seeded synthetic sweep (or the listed matrices of it): orders and
+    complex128 Fortran arrays."""
+    orders, omegas = sweep_spec(count, seed)
+    idx = range(count) if indices is None else indices
+    return [orders[k] for k in idx], [sweep_matrix(k, orders[k], omegas[k], seed) for k in idx]
 
 
 def cpu_sample(count, size):
@@ -175,8 +188,9 @@ def reference_arm(args, world, rank):
     from oracle import oracle
     oracle.lib()
     threads = oracle.threads()
-    orders, mats = make_sweep(args.count, args.seed)
+    orders, _ = sweep_spec(args.count, args.seed)
     sample = cpu_sample(len(orders), args.cpu_sample)
+    mats = dict(zip(sample, make_sweep(args.count, args.seed, sample)[1]))
     chunks = sample_chunks(sample, args.ref_chunks)
     infos = {}
 
@@ -275,7 +289,16 @@ def ours(args, world, rank, local, dist):
 
     peak64 = None if args.no_peak else measured_fp64_peak(torch)
     peak8, peak8_src = (None, None) if args.no_peak else measured_int8_peak(torch)
-    orders, mats = make_sweep(args.count, args.seed + 1000 * rank)
+    if args.shard == "lpt" and world > 1:
+        from csharp_linearalgebra_b200.sweep import expm_cost_estimate, lpt_partition
+        g_orders, g_omegas = sweep_spec(args.count * world, args.seed)
+        parts, loads = lpt_partition([expm_cost_estimate(n, w) for n, w in zip(g_orders, g_omegas)], world)
+        orders, mats = make_sweep(args.count * world, args.seed, parts[rank])
+        shard_note = (f"one sweep of {args.count * world} matrices partitioned over {world} ranks by LPT on "
+                      f"n^3 (log2 w + 8); rank loads within {100 * (max(loads) / min(loads) - 1):.2f}%")
+    else:
+        orders, mats = make_sweep(args.count, args.seed + 1000 * rank)
+        shard_note = f"{world} rank(s), each its own {args.count}-matrix sweep"
     count = len(mats)
     # device-resident inputs and one set of outputs per form
     dev_in = [torch.from_numpy(m.T.copy()).to("cuda") for m in mats]  # row-major of A^T == column-major A
@@ -430,8 +453,10 @@ def ours(args, world, rank, local, dist):
                 "gemm_tflop_per_sweep": st["gemm_flops"] / 1e12,
                 "algorithmic_bytes_per_launch": st["gemm_bytes"] / st["gemm_launches"] if st["gemm_launches"] else None}
 
+    # matrices the whole job processed per step: every rank's share
+    jobs = args.count * world if (args.shard == "lpt" and world > 1) else count * world
     def rate(ms):
-        return world * count / (ms * 1e-3) if ms else None
+        return jobs / (ms * 1e-3) if ms else None
 
     sst = split["st"]
     int8_tops = sst["split_int8_ops"] / (sst["split_ms"] * 1e-3) / 1e12 if sst["split_ms"] > 0 else None
@@ -450,7 +475,7 @@ def ours(args, world, rank, local, dist):
                                "reference's degree and s, else recomputed in FP64); norms, normest1, LU and the Pade "
                                "solve in plain FP64",
                        "l2": f"inputs larger than L2: {in_bytes / 1e9:.2f} GB of matrices per step per GPU",
-                       "parallelism": f"independent matrices; {world} rank(s), each its own sweep",
+                       "parallelism": f"independent matrices; {shard_note}",
                        "squarings_range": [min(s for _, s in degrees), max(s for _, s in degrees)]},
             "e2e": {"value": rate(split["e2e_ms"]), "unit": "expm/s", "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": in_bytes},
@@ -515,6 +540,8 @@ def main():
     # 20 moduli (it is set by the FP64 steps' rounding), at 10% less conversion and product work.
     p.add_argument("--moduli", type=int, default=18, help="moduli of the split-precision form (8..22)")
     p.add_argument("--autotune", type=int, default=0, help="1: GEMM launch shapes chosen by timing (tns_set_autotune)")
+    p.add_argument("--shard", choices=["lpt", "seeds"], default="lpt",
+                   help="N > 1: one LPT-partitioned sweep (lpt) or a sweep per rank (seeds)")
     args = p.parse_args()
     world, rank, local, dist = dist_setup(args)
     try:
