@@ -126,6 +126,8 @@ SIGNATURES = {
     "tns_set_timing": (_I, [_P, _I]),
     "tns_get_stream": (_I, [_P, C.POINTER(_P)]),
     "tns_set_lu_timing": (_I, [_P, _I]),
+    "tns_inject_allocation_failure": (_I, [_P, _LL]),
+    "tns_selftest_wait": (_I, [_P, _LL]),
     "tns_get_lu_timings": (_I, [_P, C.POINTER(LuTimings)]),
 }
 

@@ -914,6 +914,18 @@ int tns_set_workers(tns_context* c, int workers) {
 int tns_set_timing(tns_context* c, int enabled) {
     return guarded(c, [&](Context& ctx) { ctx.timing = enabled != 0; });
 }
+int tns_inject_allocation_failure(tns_context* c, long long k) {
+    return guarded(c, [&](Context& ctx) {
+        require(k >= 0, TNS_E_OUT_OF_RANGE, "k must be >= 0");
+        ctx.fail_allocation_at = k > 0 ? ctx.allocations + k : 0;
+    });
+}
+int tns_selftest_wait(tns_context* c, long long limit_ns) {
+    return guarded(c, [&](Context& ctx) {
+        require(limit_ns > 0 && limit_ns <= 2000000000LL, TNS_E_OUT_OF_RANGE, "limit_ns must be in (0, 2e9]");
+        tns::selftest_wait(ctx, limit_ns);
+    });
+}
 int tns_set_lu_timing(tns_context* c, int enabled) {
     return guarded(c, [&](Context& ctx) { ctx.lu_timing = enabled != 0; });
 }

@@ -126,6 +126,7 @@ DMat::DMat(Context& c, int r, int k, bool complex_, const char* purpose)
       cplx(complex_) {
     if (r < 0 || k < 0) fail(TNS_E_ARGUMENT, "negative matrix dimension");
     c.check_limit((long long)r * k, purpose);
+    c.count_allocation();
     TNS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), bytes(), c.stream));
     TNS_CUDA(cudaMemsetAsync(p, 0, bytes(), c.stream));
 }
@@ -158,6 +159,7 @@ void* Context::scratch(size_t bytes) {
         split_scratch = nullptr;
         split_scratch_bytes = 0;
         const size_t grown = std::max(bytes, bytes + bytes / 4);  // headroom for the next, larger batch
+        count_allocation();
         TNS_CUDA(cudaMallocAsync(&split_scratch, grown, stream));
         split_scratch_bytes = grown;
     }
@@ -165,7 +167,37 @@ void* Context::scratch(size_t bytes) {
 }
 
 DBuf::DBuf(Context& c, size_t b) : ctx(&c), bytes(b) {
+    c.count_allocation();
     TNS_CUDA(cudaMallocAsync(&p, std::max<size_t>(b, 16), c.stream));
+}
+
+void Context::count_allocation() {
+    ++allocations;
+    if (fail_allocation_at > 0 && allocations >= fail_allocation_at) {
+        fail_allocation_at = 0;  // one injected failure, then allocations succeed again
+        fail(TNS_E_OUT_OF_MEMORY, "device allocation " + std::to_string(allocations) +
+                                      " refused (injected failure, tns_inject_allocation_failure)");
+    }
+}
+
+namespace {
+// A barrier that nothing ever arrives on: the bounded wait must give up after
+// limit_ns, record kDevTimeoutSelfTest and return. Nothing else is in flight.
+__global__ void wait_selftest_kernel(int* err, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    mbar_wait_bounded_ns(&bar, 0, err, kDevTimeoutSelfTest, limit_ns);
+}
+}  // namespace
+
+void selftest_wait(Context& ctx, long long limit_ns) {
+    wait_selftest_kernel<<<1, 32, 0, ctx.stream>>>(ctx.d_err, (unsigned long long)limit_ns);
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
 }
 DBuf& DBuf::operator=(DBuf&& o) noexcept {
     if (this != &o) {

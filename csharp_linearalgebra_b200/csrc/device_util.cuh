@@ -18,6 +18,7 @@ enum DeviceError : int {
     kDevTimeoutFull = 1,   // consumer waited for a stage that never landed
     kDevTimeoutEmpty = 2,  // producer waited for a stage that was never released
     kDevTimeoutDrain = 3,  // producer's final wait for its own copies
+    kDevTimeoutSelfTest = 5,  // tns_selftest_wait: a barrier nothing arrives on
 };
 
 __device__ __forceinline__ unsigned long long global_timer_ns() {
@@ -69,6 +70,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if ((it & 255u) == 0) {
             if (*reinterpret_cast<volatile int*>(err) != 0) return false;
             if (global_timer_ns() - start > kWaitTimeoutNs) {
+                atomicCAS(err, 0, code);
+                return false;
+            }
+        }
+    }
+}
+
+// The same with a caller's limit instead of kWaitTimeoutNs (the library's
+// self-test of its timeout path).
+__device__ __forceinline__ bool mbar_wait_bounded_ns(uint64_t* bar, uint32_t parity, int* err, int code,
+                                                     unsigned long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    unsigned long long start = global_timer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 255u) == 0) {
+            if (*reinterpret_cast<volatile int*>(err) != 0) return false;
+            if (global_timer_ns() - start > limit_ns) {
                 atomicCAS(err, 0, code);
                 return false;
             }

@@ -134,6 +134,12 @@ struct Context {
     int max_workers = 4;
     std::vector<std::unique_ptr<Context>> workers;
 
+    // Device allocations made through DMat, DBuf and the split scratch, and
+    // the test hook that fails one of them (tns_inject_allocation_failure).
+    long long allocations = 0;
+    long long fail_allocation_at = 0;  // 0: off; else the allocation number that fails
+    void count_allocation();
+
     explicit Context(int dev);
     ~Context();
     void sync();                       // stream sync + device error flag check
@@ -179,6 +185,10 @@ struct DBuf {
     template <class T>
     T* as() const { return static_cast<T*>(p); }
 };
+
+// Launch a kernel whose bounded wait on a barrier nothing arrives on gives up
+// after limit_ns and records the device error (the timeout path's self-test).
+void selftest_wait(Context& ctx, long long limit_ns);
 
 // ---- transfers -------------------------------------------------------------
 // Copy a rows x cols column-major operand (host or device pointer, ld in

@@ -471,6 +471,19 @@ int tns_set_lu_timing(tns_context* ctx, int enabled);
 int tns_get_lu_timings(tns_context* ctx, tns_lu_timings* out);
 int tns_reset_stats(tns_context* ctx);
 int tns_set_timing(tns_context* ctx, int enabled);
+/* Failure paths, exercised without a GPU fault. The k-th device allocation
+ * this context makes from now (counting the padded operand copies and work
+ * matrices of every call) fails as a cudaMalloc that ran out of memory would:
+ * the call returns TNS_E_OUT_OF_MEMORY with its destination untouched, and
+ * the next allocation succeeds again. k = 0 disarms it. No counterpart in the
+ * reference (its managed allocations throw OutOfMemoryException). */
+int tns_inject_allocation_failure(tns_context* ctx, long long k);
+/* Runs one kernel whose bounded wait, on a barrier that nothing arrives on,
+ * gives up after limit_ns nanoseconds (at most 2e9), as every device-side
+ * wait of the library does after its own limit: the call returns TNS_E_TIMEOUT
+ * and the context stays usable. */
+int tns_selftest_wait(tns_context* ctx, long long limit_ns);
+
 /* The CUDA stream (cudaStream_t) the context issues its work on. */
 int tns_get_stream(tns_context* ctx, void** stream);
 
