@@ -468,6 +468,25 @@ class Workspace:
             diagnostics.extend(ExpmvDiagnostics(i.degree, i.scaling, i.applications, i.early_exits) for i in infos)
         return outs
 
+    def expmv_select_batched(self, mats, ncols: int, t: float = 1.0, device: bool = False, orders=None, lds=None):
+        """(m, s) that the batched Expmv chooses for every complex matrix, for
+        panels of ncols columns, without running the recurrences. mats are
+        numpy arrays, or raw device pointers with device=True (orders and lds
+        given)."""
+        if device:
+            count = len(mats)
+            ptrs = (C.c_void_p * count)(*mats)
+        else:
+            arrs = [_fortran(m, True) for m in mats]
+            count = len(arrs)
+            orders = [m.shape[0] for m in arrs]
+            lds = [_ld(m) for m in arrs]
+            ptrs = (C.c_void_p * count)(*[m.ctypes.data for m in arrs])
+        infos = (N.ExpmvInfo * count)()
+        self._call("tns_zexpmv_select_batched_device" if device else "tns_zexpmv_select_batched", count,
+                   (C.c_int * count)(*orders), ptrs, (C.c_int * count)(*lds), int(ncols), float(t), infos)
+        return [(i.degree, i.scaling) for i in infos]
+
     def expmv_batched_device(self, count, orders, a_ptrs, lds, ncols, b_ptrs, ldbs, t, out_ptrs, ldos):
         """The batched complex Expmv over device-resident operands (raw device
         pointers). Returns the diagnostics."""

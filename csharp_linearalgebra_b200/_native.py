@@ -105,6 +105,8 @@ SIGNATURES = {
     "tns_dexpmv_batched": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
     "tns_zexpmv_batched": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
     "tns_zexpmv_batched_device": (_I, [_P, _I, _P, _P, _P, _I, _P, _P, _D, _P, _P, _P]),
+    "tns_zexpmv_select_batched": (_I, [_P, _I, _P, _P, _P, _I, _D, _P]),
+    "tns_zexpmv_select_batched_device": (_I, [_P, _I, _P, _P, _P, _I, _D, _P]),
     "tns_dexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
     "tns_zexpm_frechet": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, C.POINTER(ExpmInfo)]),
     "tns_dexpmv_gradient": (_I, [_P, _I, _I, _D, _P, _I, _P, _I, _P, _I, C.POINTER(_D), _P, _I, _P, _I,

@@ -369,6 +369,32 @@ int panel_entry(tns_context* c, bool cplx, bool adjoint, int n, int t, const dou
     });
 }
 
+int expmv_select_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
+                       int ncols, double t, tns_expmv_info* infos) {
+    return guarded(c, [&](Context& ctx) {
+        require(count >= 0, TNS_E_ARGUMENT, "negative batch size");
+        require(ncols >= 1, TNS_E_ARGUMENT, "the panel needs at least one column");
+        if (count == 0) return;
+        require(orders && a && lda && infos, TNS_E_NULL, "a batch array is null");
+        for (int i = 0; i < count; ++i) check_operand(a[i], orders[i], orders[i], lda[i], "A[i]");
+        require(std::isfinite(t), TNS_E_OUT_OF_RANGE, "t must be finite");
+        for (int i = 0; i < count; ++i) infos[i] = tns_expmv_info{0, 1, 0, 0};
+        std::vector<int> live;
+        for (int i = 0; i < count; ++i)
+            if (orders[i] > 0) live.push_back(i);
+        if (live.empty()) return;
+        std::vector<DMat> A;
+        A.reserve(live.size());
+        for (int i : live) A.push_back(upload(ctx, a[i], orders[i], orders[i], lda[i], true, dev, "an operator of the batch"));
+        std::vector<const DMat*> ap;
+        for (auto& m : A) ap.push_back(&m);
+        std::vector<DMat> R;
+        std::vector<tns::ExpmvInfo> ei;
+        tns::expmv_batch(ctx, ap, {}, t, R, ei, ncols);
+        for (size_t k = 0; k < live.size(); ++k) infos[live[k]] = tns_expmv_info{ei[k].degree, ei[k].scaling, 0, 0};
+    });
+}
+
 int frechet_entry(tns_context* c, bool cplx, int n, const double* a, int lda, const double* e, int lde, double* expa,
                   int ldx, double* l, int ldl, tns_expm_info* info) {
     return guarded(c, [&](Context& ctx) {
@@ -839,6 +865,14 @@ int tns_zexpmv_batched_device(tns_context* c, int count, const int* orders, cons
                               int ncols, const double* const* b, const int* ldb, double t, double* const* out,
                               const int* ldo, tns_expmv_info* infos) {
     return expmv_batched_entry(c, true, true, count, orders, a, lda, ncols, b, ldb, t, out, ldo, infos);
+}
+int tns_zexpmv_select_batched(tns_context* c, int count, const int* orders, const double* const* a, const int* lda,
+                              int ncols, double t, tns_expmv_info* infos) {
+    return expmv_select_entry(c, false, count, orders, a, lda, ncols, t, infos);
+}
+int tns_zexpmv_select_batched_device(tns_context* c, int count, const int* orders, const double* const* a,
+                                     const int* lda, int ncols, double t, tns_expmv_info* infos) {
+    return expmv_select_entry(c, true, count, orders, a, lda, ncols, t, infos);
 }
 int tns_dexpm_frechet(tns_context* c, int n, const double* a, int lda, const double* e, int lde, double* expa,
                       int ldx, double* l, int ldl, tns_expm_info* info) {

@@ -648,16 +648,18 @@ Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int n
 }  // namespace
 
 void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::vector<const DMat*>& bs, double t,
-                 std::vector<DMat>& results, std::vector<ExpmvInfo>& infos) {
+                 std::vector<DMat>& results, std::vector<ExpmvInfo>& infos, int select_only_cols) {
     const size_t cnt = as.size();
     results.clear();
     results.resize(cnt);
     infos.assign(cnt, ExpmvInfo{});
     if (cnt == 0) return;
     const bool cplx = as[0]->cplx;
-    const int ncols = bs[0]->cols;
+    const bool select_only = select_only_cols > 0;
+    const int ncols = select_only ? select_only_cols : bs[0]->cols;
     for (size_t k = 0; k < cnt; ++k)
-        if (as[k]->cplx != cplx || bs[k]->cols != ncols || bs[k]->rows != as[k]->rows || as[k]->rows < 1)
+        if (as[k]->cplx != cplx || as[k]->rows < 1 ||
+            (!select_only && (bs[k]->cols != ncols || bs[k]->rows != as[k]->rows)))
             fail(TNS_E_ARGUMENT, "internal: an exponential-action batch mixes element types or panel widths");
 
     // mu = trace / n (per part for complex), A - mu I, ||A - mu I||_1
@@ -724,6 +726,7 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
         for (int j = 0; j < m; ++j) coeffs.push_back(t / (s * (double)(j + 1)));
     }
 
+    if (select_only) return;
     if (ncols > kSlots * 4) {
         // Wider panels than the fused kernel holds: the host-driven loop.
         for (size_t k = 0; k < cnt; ++k)

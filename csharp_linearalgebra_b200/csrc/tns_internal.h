@@ -373,8 +373,10 @@ void expmv(Context& ctx, const DMat& a, const DMat& b, double t, DMat& result, E
 // The same for a batch of independent (A_k, B_k), every B_k with the same
 // column count; the Taylor recurrences of all matrices run in one cooperative
 // launch (expmv_batched.cu).
+// select_only_cols > 0: only (m, s) for panels of that many columns (bs is
+// not read, no results).
 void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::vector<const DMat*>& bs, double t,
-                 std::vector<DMat>& results, std::vector<ExpmvInfo>& infos);
+                 std::vector<DMat>& results, std::vector<ExpmvInfo>& infos, int select_only_cols = 0);
 // The earlier host-driven form of the dense path: every application a panel
 // product launch, the norms read back to the host (kept as the reference
 // point for the fused kernel, and for panels wider than it takes).

@@ -285,6 +285,18 @@ int tns_zexpmv_batched_device(tns_context* ctx, int count, const int* orders, co
                               const int* lda, int ncols, const double* const* b, const int* ldb, double t,
                               double* const* out, const int* ldo, tns_expmv_info* infos);
 
+/* Only the (m, s) that tns_zexpmv_batched would choose for each complex
+ * matrix, with panels of ncols columns and this t (trace shift, sharp
+ * bounds, the search of MatrixExponentialAction.SelectParameters,
+ * src/Tensile/MatrixExponentialAction.cs:347-398), without running the
+ * recurrences: infos[i].degree and .scaling; applications and early_exits
+ * stay 0. Lets a caller see the cost (m s applications) of a sweep before
+ * running it. _device: device pointers. */
+int tns_zexpmv_select_batched(tns_context* ctx, int count, const int* orders, const double* const* a, const int* lda,
+                              int ncols, double t, tns_expmv_info* infos);
+int tns_zexpmv_select_batched_device(tns_context* ctx, int count, const int* orders, const double* const* a,
+                                     const int* lda, int ncols, double t, tns_expmv_info* infos);
+
 /* ---- precision form of the solve ----------------------------------------- */
 
 typedef struct {

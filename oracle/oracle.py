@@ -87,6 +87,8 @@ def lib():
             getattr(L, name).argtypes = [i, P, i, i, P, i, d, P, i, C.POINTER(ExpmvInfo)]
         for name in ("orc_dexpmv_bound", "orc_zexpmv_bound"):
             getattr(L, name).argtypes = [i, P, i, i, P, i, d, d, P, i, C.POINTER(ExpmvInfo)]
+        for name in ("orc_dexpmv_params", "orc_zexpmv_params"):
+            getattr(L, name).argtypes = [i, P, i, i, d, C.POINTER(ExpmvInfo)]
         for name in ("orc_dtrsolve", "orc_ztrsolve"):
             getattr(L, name).argtypes = [i, i, i, P, i, P, i]
         for name in ("orc_dpanel", "orc_zpanel"):
@@ -317,3 +319,17 @@ def panel(a, x, transposed=False):
     fn = lib().orc_zpanel if cplx else lib().orc_dpanel
     fn(int(transposed), n, t, _p(a), _ld(a), _p(x), _ld(x), _p(y), _ld(y))
     return y
+
+
+def expmv_params(a, ncols, t=1.0):
+    """(m, s) that Expmv selects for A, an ncols-column panel and t, without
+    running the recurrence."""
+    cplx = np.iscomplexobj(a)
+    a = _f(a, np.complex128 if cplx else np.float64)
+    info = ExpmvInfo()
+    fn = lib().orc_zexpmv_params if cplx else lib().orc_dexpmv_params
+    rc = fn(a.shape[0], _p(a), _ld(a), int(ncols), float(t), C.byref(info))
+    if rc == 8:
+        raise OverflowError("||tA|| too large for the exponential action")
+    assert rc == 0
+    return info.degree, info.scaling

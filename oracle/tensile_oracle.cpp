@@ -1590,8 +1590,9 @@ int expmv_dense(int n, const typename K::T* a, int lda, int ncols, const typenam
     if (!info) info = &local;
     *info = orc_expmv_info{};
     if (n == 0 || ncols == 0) {
-        for (int j = 0; j < ncols; j++)
-            for (int i = 0; i < n; i++) out[(size_t)j * ldo + i] = b[(size_t)j * ldb + i];
+        if (b)
+            for (int j = 0; j < ncols; j++)
+                for (int i = 0; i < n; i++) out[(size_t)j * ldo + i] = b[(size_t)j * ldb + i];
         return 0;
     }
     // Trace shift (:138-139; complex :57-60).
@@ -1628,6 +1629,7 @@ int expmv_dense(int n, const typename K::T* a, int lda, int ncols, const typenam
     }
     info->degree = m;
     info->scaling = s;
+    if (!b) return 0;  // the parameters only (orc_{d,z}expmv_params)
 
     size_t ext = (size_t)n * ncols;
     std::vector<T> f(ext), work(ext), next(ext);
@@ -1925,6 +1927,15 @@ int orc_zexpmv(int n, const double* a, int lda, int ncols, const double* b, int 
                double* out, int ldo, orc_expmv_info* info) {
     return expmv_dense<ComplexK>(n, (const cplx*)a, lda, ncols, (const cplx*)b, ldb, t, (cplx*)out, ldo,
                                  info);
+}
+
+// The (m, s) that Expmv selects for A, a panel of ncols columns and t,
+// without running the recurrence.
+int orc_dexpmv_params(int n, const double* a, int lda, int ncols, double t, orc_expmv_info* info) {
+    return expmv_dense<RealK>(n, a, lda, ncols, nullptr, 0, t, nullptr, 0, info);
+}
+int orc_zexpmv_params(int n, const double* a, int lda, int ncols, double t, orc_expmv_info* info) {
+    return expmv_dense<ComplexK>(n, (const cplx*)a, lda, ncols, nullptr, 0, t, nullptr, 0, info);
 }
 
 }  // extern "C"

@@ -123,6 +123,10 @@ int orc_dexpmv(int n, const double* a, int lda, int ncols, const double* b, int 
                double* out, int ldo, orc_expmv_info* info);
 int orc_zexpmv(int n, const double* a, int lda, int ncols, const double* b, int ldb, double t,
                double* out, int ldo, orc_expmv_info* info);
+/* The (m, s) Expmv selects (trace shift, sharp bounds, the search) without
+ * running the Taylor recurrence; applications stay 0. */
+int orc_dexpmv_params(int n, const double* a, int lda, int ncols, double t, orc_expmv_info* info);
+int orc_zexpmv_params(int n, const double* a, int lda, int ncols, double t, orc_expmv_info* info);
 
 #ifdef __cplusplus
 }

@@ -102,3 +102,15 @@ def test_one_large_matrix_uses_the_whole_gpu(ws, orc):
     diags = []
     outs = ws.expmv_batched([a], [b], 0.5, diags)
     check_against_oracle(orc, [a], [b], 0.5, outs, diags)
+
+
+def test_parameter_selection_over_the_whole_frequency_range(ws, orc):
+    """(m, s) for sweep matrices up to w = 1e6, where the recurrence itself
+    (about 1.4 w applications) is out of reach for a test, from the
+    selection-only entry point: equal to the reference's choice."""
+    rng = np.random.default_rng(49)
+    mats = [sweep_matrix(rng, int(rng.integers(40, 120)), w) for w in np.logspace(2.0, 6.0, 9)]
+    got = ws.expmv_select_batched(mats, 8, 0.5)
+    for a, ms in zip(mats, got):
+        assert ms == orc.expmv_params(a, 8, 0.5)
+    assert max(s for _, s in got) > 1000
