@@ -314,6 +314,14 @@ def ours(args, world, rank, local, dist):
     ws.set_workers(args.groups)
     ws.set_autotune(bool(args.autotune))
     stream = torch.cuda.ExternalStream(ws.stream)
+    if args.configs_only:
+        # Only the other configurations' measurements (a profiling or a quick run).
+        del host_in, host_out
+        configs = other_configurations(args, ws, torch, peak64, peak8, (orders, mats, dev_in))
+        if rank == 0:
+            print(json.dumps({"configurations": configs}), flush=True)
+        ws.dispose()
+        return
 
     def barrier():
         if dist is not None:
@@ -458,6 +466,11 @@ def ours(args, world, rank, local, dist):
     def rate(ms):
         return jobs / (ms * 1e-3) if ms else None
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        del host_in, host_out
+        configs = other_configurations(args, ws, torch, peak64, peak8, (orders, mats, dev_in))
+
     sst = split["st"]
     int8_tops = sst["split_int8_ops"] / (sst["split_ms"] * 1e-3) / 1e12 if sst["split_ms"] > 0 else None
     degrees = sorted(set((d.degree, d.squarings) for d in split["diags"]))
@@ -514,11 +527,285 @@ def ours(args, world, rank, local, dist):
                            "parity_vs_reference": parity, "roofline": dmma_roofline(plain),
                            "clocks": plain["clocks"]},
             "cpu_baseline": cpu,
+            "configurations": configs,
             "clocks": split["clocks"],
             "gpu_launches": int(split["st_step"]["kernel_launches"]),
         }
         print(json.dumps(line), flush=True)
     ws.dispose()
+
+
+def measured_hbm_peak():
+    """The copy bandwidth (GB/s) MEASURED_PEAKS.json holds, else this pool's
+    earlier measurement (6650 GB/s), with where it came from."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        for k in ("hbm_gbs", "hbm_GBps", "hbm"):
+            if isinstance(d.get(k), (int, float)):
+                return float(d[k]), "MEASURED_PEAKS.json " + k
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback 6650 GB/s (earlier measurement on this pool)"
+
+
+def other_configurations(args, ws, torch, peak64, peak8, sweep):
+    """The other configurations of the workload, each measured once here, next
+    to the CPU restatement of the reference on the same inputs (the oracle,
+    all host threads) and its parity: the FP64 GEMM (1), the n = 512 dense
+    path (2), the precision form of the solve at n = 4096 (3), the batched
+    exponential action over the sweep (4, Expmv), and the differentiation
+    form (5). GPU times are CUDA events on the library's stream around the
+    public host-buffer call unless a field says otherwise, the median of a
+    few runs with L2 flushed (a 256 MB write) before each."""
+    from oracle import oracle
+    oracle.lib()
+    stream = torch.cuda.ExternalStream(ws.stream)
+    flush_buf = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device="cuda")  # 256 MB > L2
+
+    def gpu_ms(fn, reps=3):
+        times, out = [], None
+        for _ in range(reps):
+            flush_buf.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return statistics.median(times), out
+
+    def cpu_s(fn):
+        t0 = time.perf_counter()
+        out = fn()
+        return time.perf_counter() - t0, out
+
+    cores = oracle.threads()
+    res = {}
+
+    # (1) FP64 GEMM m = n = k = 1024, uniform [-1, 1), alpha 1, beta 0.
+    rng = np.random.default_rng(args.seed + 1)
+    n = 1024
+    a = np.asfortranarray(rng.uniform(-1.0, 1.0, (n, n)))
+    b = np.asfortranarray(rng.uniform(-1.0, 1.0, (n, n)))
+    da, db = torch.from_numpy(a.T.copy()).cuda(), torch.from_numpy(b.T.copy()).cuda()
+    dc = torch.empty_like(da)
+    dev_ms, _ = gpu_ms(lambda: ws._call("tns_dgemm_device", n, n, n, 1.0, da.data_ptr(), n, db.data_ptr(), n, 0.0,
+                                        dc.data_ptr(), n), reps=5)
+    e2e_ms, c = gpu_ms(lambda: ws.multiply(a, b), reps=5)
+    cs, cref = cpu_s(lambda: oracle.gemm(a, b))
+    flops = 2.0 * n ** 3
+    res["1_fp64_gemm_1024"] = {
+        "value": flops / (dev_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "ms": dev_ms,
+        "timing": "tns_dgemm_device (operands in HBM, padded copies inside the call)",
+        "e2e": {"value": flops / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "ms": e2e_ms,
+                "h2d_bytes": 2 * 8 * n * n, "d2h_bytes": 8 * n * n},
+        "roofline": {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA)", "peak": peak64, "unit": "TFLOP/s",
+                     "achieved": flops / (dev_ms * 1e-3) / 1e12,
+                     "frac": (flops / (dev_ms * 1e-3) / 1e12 / peak64) if peak64 else None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 in this process"},
+        "cpu_baseline": {"value": flops / cs / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                         "sample": "the same product, the reference's threaded blocking (KC 256)"},
+        "bit_identical_to_reference": bool(np.array_equal(c, cref))}
+    del da, db, dc
+
+    # (2) n = 512: LU + solve of 8 right-hand sides + rcond, real and complex;
+    # Expm over 32 draws with ||A||_1 log-uniform in [1e-2, 1e3].
+    n = 512
+    two = {}
+    for kind in ("real", "complex"):
+        rng = np.random.default_rng(args.seed + (2 if kind == "real" else 3))
+        if kind == "real":
+            a = rng.standard_normal((n, n)) / math.sqrt(n)
+            b = rng.standard_normal((n, 8))
+        else:
+            a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / math.sqrt(2 * n)
+            b = rng.standard_normal((n, 8)) + 1j * rng.standard_normal((n, 8))
+        a = np.asfortranarray(a)
+
+        def lu_path():
+            lu = ws.factor_lu(a)
+            return lu, lu.solve(b), lu.reciprocal_condition()
+
+        ms_lu, (lu, x, rc) = gpu_ms(lu_path)
+        cs_lu, (f, piv, _) = cpu_s(lambda: oracle.getrf(a))
+        cs_s, xo = cpu_s(lambda: oracle.getrs(f, piv, b))
+        cs_r, rco = cpu_s(lambda: oracle.gecon(f, piv, -1, oracle.norm1(a)))
+        norms = np.exp(rng.uniform(math.log(1e-2), math.log(1e3), 32))
+        draws = []
+        for v in norms:
+            g = rng.standard_normal((n, n)) / math.sqrt(n) if kind == "real" else \
+                (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / math.sqrt(2 * n)
+            draws.append(np.asfortranarray(g * (v / np.abs(g).sum(axis=0).max())))
+        from csharp_linearalgebra_b200 import ExpmDiagnostics
+        diags = [ExpmDiagnostics() for _ in draws]
+        outs = [None] * len(draws)
+
+        def ladder():
+            for q, d in enumerate(draws):
+                outs[q] = ws.expm(d, diags[q])
+
+        ms_ex, _ = gpu_ms(ladder, reps=1)
+        cs_ex, refs = cpu_s(lambda: [oracle.expm(d) for d in draws])
+        two[kind] = {
+            "lu_solve8_rcond_ms": ms_lu,
+            "lu_gflops": ((2.0 / 3.0) * n ** 3 * (4 if kind == "complex" else 1)) / (ms_lu * 1e-3) / 1e9,
+            "cpu_lu_solve8_rcond_ms": 1e3 * (cs_lu + cs_s + cs_r),
+            "pivots_equal": bool(np.array_equal(lu.pivots, piv)), "factors_equal": bool(np.array_equal(lu.factors, f)),
+            "solution_equal": bool(np.array_equal(x, xo)), "rcond_equal": bool(rc == rco),
+            "expm_ms_per_call": ms_ex / len(draws), "cpu_expm_ms_per_call": 1e3 * cs_ex / len(draws),
+            "expm_decisions_equal": sum((d.degree, d.squarings) == (i["degree"], i["squarings"])
+                                        for d, (_, i) in zip(diags, refs)),
+            "expm_bit_identical": sum(bool(np.array_equal(o, r)) for o, (r, _) in zip(outs, refs)),
+            "expm_draws": len(draws),
+            "degrees_seen": sorted(set(d.degree for d in diags)),
+            "squarings_range": [min(d.squarings for d in diags), max(d.squarings for d in diags)]}
+    two["timing"] = ("GPU: the host-buffer calls (factor, solve, rcond; one Expm per draw, in sequence); "
+                     "CPU: the oracle on all host threads, the same inputs")
+    res["2_dense_path_512"] = two
+
+    # (3) precision form: n = 4096, 64 right-hand sides, A = U diag(sigma) V^T.
+    n, nrhs = 4096, 64
+    rng = np.random.default_rng(args.seed + 4)
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    b = np.asfortranarray(rng.standard_normal((n, nrhs)))
+    three = {"kappa": {}}
+    for kappa in (1e2, 1e6, 1e10):
+        sig = np.logspace(0.0, -math.log10(kappa), n)
+        a = np.asfortranarray((u * sig) @ v.T)
+        ms_mx, (x, info) = gpu_ms(lambda: ws.solve_mixed(a, b), reps=1)
+
+        def fp64():
+            return ws.factor_lu(a).solve(b)
+
+        ms_64, x64 = gpu_ms(fp64, reps=1)
+        anorm = np.abs(a).sum(axis=1).max()
+
+        def backward(xx):
+            r = b - a @ xx
+            return float(max(np.abs(r[:, j]).max() / (anorm * np.abs(xx[:, j]).max() + np.abs(b[:, j]).max())
+                             for j in range(nrhs)))
+
+        entry = {"mixed_ms": ms_mx, "fp64_ms": ms_64, "moduli": info["moduli"],
+                 "factorizations": info["factorizations"], "refinement_steps": info["iterations"],
+                 "backward_error_mixed": backward(x), "backward_error_fp64": backward(x64),
+                 "rel_diff_mixed_vs_fp64": float(np.linalg.norm(x - x64) / np.linalg.norm(x64))}
+        if kappa == 1e2:
+            cs_f, (f, piv, _) = cpu_s(lambda: oracle.getrf(a))
+            cs_s, xo = cpu_s(lambda: oracle.getrs(f, piv, b))
+            entry["cpu_fp64_lu_solve_ms"] = 1e3 * (cs_f + cs_s)
+            entry["fp64_bit_identical_to_reference"] = bool(np.array_equal(x64, xo))
+        three["kappa"][f"{kappa:.0e}"] = entry
+    ws.reset_stats()
+    ws.set_timing(True)
+    g1 = rng.uniform(-1.0, 1.0, (n, n))
+    g2 = rng.uniform(-1.0, 1.0, (n, n))
+    ws.multiply_split(g1, g2, args.moduli)
+    ws.set_timing(False)
+    st = ws.stats()
+    three["split_gemm_4096"] = {
+        "moduli": args.moduli, "kernel_ms": st["split_ms"],
+        "fp64_equivalent_tflops": st["split_flops"] / (st["split_ms"] * 1e-3) / 1e12 if st["split_ms"] else None,
+        "int8_tops": st["split_int8_ops"] / (st["split_ms"] * 1e-3) / 1e12 if st["split_ms"] else None,
+        "int8_peak_tops": peak8,
+        "timing": "CUDA events around the modular GEMM launches of one real 4096^3 split product"}
+    three["timing"] = "GPU: the host-buffer calls, one run each (factorization included); CPU: the oracle"
+    res["3_precision_solve_4096"] = three
+    del u, v
+
+    # (4) the batched exponential action over the sweep: B n x 8, t = 0.5.
+    # the benchmark's own sweep, already on the device
+    orders, all_mats, dev_a = sweep
+    omegas = np.logspace(2.0, 6.0, len(orders))
+    ms_sel, sel = gpu_ms(lambda: ws.expmv_select_batched([t.data_ptr() for t in dev_a], 8, 0.5, device=True,
+                                                          orders=orders, lds=orders), reps=1)
+    sub = [k for k in range(len(orders)) if omegas[k] <= args.expmv_wmax]
+    rng = np.random.default_rng(args.seed + 5)
+    bs = [np.asfortranarray(rng.standard_normal((orders[k], 8)) + 1j * rng.standard_normal((orders[k], 8)))
+          for k in sub]
+    dev_b = [torch.from_numpy(x.T.copy()).cuda() for x in bs]
+    dev_o = [torch.empty_like(x) for x in dev_b]
+    so = [orders[k] for k in sub]
+    ms_dev, diags = gpu_ms(lambda: ws.expmv_batched_device(len(sub), so, [dev_a[k].data_ptr() for k in sub], so, 8,
+                                                           [x.data_ptr() for x in dev_b], so, 0.5,
+                                                           [x.data_ptr() for x in dev_o], so), reps=2)
+    ms_e2e, outs = gpu_ms(lambda: ws.expmv_batched([all_mats[k] for k in sub], bs, 0.5), reps=1)
+    apps = [d.applications for d in diags]
+    abytes = sum(ap * 16.0 * nn * nn for ap, nn in zip(apps, so))
+    fp64_instr = sum(ap * 64.0 * nn * nn for ap, nn in zip(apps, so))
+    hbm_peak, hbm_src = measured_hbm_peak()
+    cpu_pick = sub[:3]
+    cs_mv, refs = cpu_s(lambda: [oracle.expmv(all_mats[k], bs[sub.index(k)], 0.5) for k in cpu_pick])
+    res["4_batched_expmv"] = {
+        "value": len(sub) / (ms_dev * 1e-3), "unit": "expmv/s", "ms": ms_dev,
+        "matrices": len(sub), "omega_max": args.expmv_wmax,
+        "subset": f"the sweep's matrices with w <= {args.expmv_wmax:g} ({len(sub)} of {len(orders)}); "
+                  "above it the applications (about 1.4 w per matrix) grow past a benchmark step",
+        "applications": sum(apps), "early_exits": sum(d.early_exits for d in diags),
+        "e2e": {"value": len(sub) / (ms_e2e * 1e-3), "unit": "expmv/s", "ms": ms_e2e,
+                "h2d_bytes": sum(16 * nn * nn + 16 * nn * 8 for nn in so), "d2h_bytes": sum(16 * nn * 8 for nn in so)},
+        "roofline": {"bound": "fp64 pipe (exact-order products: a multiply and an add per term, no FMA)",
+                     "kernel": "taylor_kernel (one cooperative launch)",
+                     "achieved_a_bytes_gbs": abytes / (ms_dev * 1e-3) / 1e9, "hbm_peak_gbs": hbm_peak,
+                     "hbm_frac": abytes / (ms_dev * 1e-3) / 1e9 / hbm_peak, "hbm_peak_source": hbm_src,
+                     "achieved_fp64_tops": fp64_instr / (ms_dev * 1e-3) / 1e12,
+                     "fp64_peak_tops_nominal": 148 * 64 * 1.965e9 / 1e12,
+                     "fp64_frac": fp64_instr / (ms_dev * 1e-3) / (148 * 64 * 1.965e9),
+                     "algorithmic_work": "per application 16 n^2 bytes of A and 64 n^2 FP64 operations "
+                                         "(8 columns, 4 multiplies and 4 adds per complex term)"},
+        "selection_all_256": {"ms": ms_sel, "sum_m_s": int(sum(m * s_ for m, s_ in sel)),
+                              "sum_m_s_subset": int(sum(sel[k][0] * sel[k][1] for k in sub)),
+                              "max_s": int(max(s_ for _, s_ in sel))},
+        "cpu_baseline": {"value": len(cpu_pick) / cs_mv, "unit": "expmv/s", "cores": 1, "kind": "port",
+                         "sample": f"the {len(cpu_pick)} lowest-frequency matrices of the subset (orders "
+                                   f"{[orders[k] for k in cpu_pick]}), the oracle's sequential Expmv"},
+        "parity": {"compared": len(cpu_pick),
+                   "bit_identical": sum(bool(np.array_equal(outs[sub.index(k)], r)) for k, (r, _) in
+                                        zip(cpu_pick, refs)),
+                   "decisions_and_counts_equal": sum(
+                       (diags[sub.index(k)].degree, diags[sub.index(k)].scaling, diags[sub.index(k)].applications)
+                       == (i["degree"], i["scaling"], i["applications"]) for k, (_, i) in zip(cpu_pick, refs))}}
+    del dev_b, dev_o
+
+    # (5) differentiation: gradient of ||exp(tA)B - Y||_F^2 at n = 2048 (w = 1e4,
+    # B 2048 x 16, t = 1) and the Frechet derivative at n = 1024.
+    five = {}
+    n = 2048
+    a5 = sweep_matrix(10_000, n, 1e4, args.seed + 6)
+    rng = np.random.default_rng(args.seed + 7)
+    b5 = np.asfortranarray(rng.standard_normal((n, 16)) + 0j)
+    y5 = np.asfortranarray(rng.standard_normal((n, 16)) + 1j * rng.standard_normal((n, 16)))
+    ms_g, g = gpu_ms(lambda: ws.expmv_gradient(a5, b5, y5, 1.0), reps=1)
+    from csharp_linearalgebra_b200 import ExpmvDiagnostics
+    dv = ExpmvDiagnostics()
+    ms_v, fv = gpu_ms(lambda: ws.expmv(a5, b5, 1.0, dv), reps=1)
+    five["gradient_2048"] = {"ms": ms_g, "degree": g["degree"], "squarings": g["squarings"],
+                             "f_vs_expmv_rel": float(np.linalg.norm(g["f"] - fv) / np.linalg.norm(fv))}
+    five["expmv_2048x16"] = {"ms": ms_v, "degree": dv.degree, "scaling": dv.scaling,
+                             "applications": dv.applications,
+                             "a_bytes_gbs": dv.applications * 16.0 * n * n / (ms_v * 1e-3) / 1e9}
+    n = 1024
+    a6 = sweep_matrix(10_001, n, 1e4, args.seed + 8)
+    e6 = np.asfortranarray(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    ms_f, (x6, l6) = gpu_ms(lambda: ws.expm_frechet(a6, e6), reps=1)
+    block = np.zeros((2 * n, 2 * n), dtype=np.complex128, order="F")
+    block[:n, :n] = a6
+    block[:n, n:] = e6
+    block[n:, n:] = a6
+    ms_b, eb = gpu_ms(lambda: ws.expm(block), reps=1)
+    five["frechet_1024"] = {
+        "ms": ms_f, "block_expm_2048_ms": ms_b,
+        "rel_diff_vs_block_expm": float(np.abs(l6 - eb[:n, n:]).sum(axis=0).max() / np.abs(eb[:n, n:]).sum(axis=0).max()),
+        "block_expm": "the reference's route, Expm of [[A, E], [0, A]], in this library's plain form (the "
+                      "reference's arithmetic bit for bit)"}
+    five["cpu_baseline"] = None
+    five["cpu_baseline_note"] = ("not timed by default: the reference's route is Expm of the 2048-order block, "
+                                 "tens of seconds of the oracle")
+    res["5_differentiation"] = five
+    return res
 
 
 def main():
@@ -540,6 +827,10 @@ def main():
     # 20 moduli (it is set by the FP64 steps' rounding), at 10% less conversion and product work.
     p.add_argument("--moduli", type=int, default=18, help="moduli of the split-precision form (8..22)")
     p.add_argument("--autotune", type=int, default=0, help="1: GEMM launch shapes chosen by timing (tns_set_autotune)")
+    p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
+    p.add_argument("--configs-only", action="store_true", help="only the other configurations' measurements")
+    p.add_argument("--expmv-wmax", type=float, default=1e4,
+                   help="batched Expmv: time the sweep's matrices up to this frequency")
     p.add_argument("--shard", choices=["lpt", "seeds"], default="lpt",
                    help="N > 1: one LPT-partitioned sweep (lpt) or a sweep per rank (seeds)")
     args = p.parse_args()

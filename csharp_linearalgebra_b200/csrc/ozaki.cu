@@ -29,7 +29,7 @@
 // so that output columns 2j, 2j+1 are Re, Im of C[:, j]) -- four real
 // multiplications per complex multiply-add, as the 4M method (never 3M).
 //
-// Kernels. Residues: one thread per 16 bytes of a residue row, all moduli.
+// Kernels. Residues: one thread per 8 bytes of a residue row, all moduli.
 // Product: one CTA per 128 x 256 output tile and all moduli: a TMA producer
 // warp streams 128- and 256-row x 128-byte residue tiles (128-byte swizzle)
 // through a 4-stage mbarrier ring; one thread issues tcgen05.mma kind::i8
@@ -255,11 +255,12 @@ __device__ __forceinline__ uint32_t neg_bytes(uint32_t w) {
     return ((n & 0x7f7f7f7fu) + 0x01010101u) ^ (n & 0x80808080u);
 }
 
-// Sixteen entries of one residue row: their digits (in pairs), then for each
-// modulus the residue bytes, handed to store(q, words).
-template <int ND>
+// 2 NP consecutive entries of one residue row (8 or 16): their digits (in
+// pairs), then for each modulus the residue bytes, handed to store(q, words)
+// as NP / 2 words (uint2 or uint4).
+template <int ND, int NP>
 struct RowDigits {
-    float2 c[ND][8];
+    float2 c[ND][NP];
 
     template <class Load>
     __device__ __forceinline__ void take(Load load, int shift) {
@@ -267,7 +268,7 @@ struct RowDigits {
         const double f1 = pow2(h), f2 = pow2(shift - h);
         const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
+        for (int e = 0; e < NP; ++e) {
             float d0[ND], d1[ND];
             digits_of<ND>(load(2 * e), f1, f2, d0);
             digits_of<ND>(load(2 * e + 1), f1, f2, d1);
@@ -285,9 +286,9 @@ struct RowDigits {
         // constant-bank loads.
 #pragma unroll 1
         for (int q = 0; q < nm; ++q) {
-            uint32_t b[16];
+            uint32_t b[2 * NP];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
+            for (int e = 0; e < NP; ++e) {
                 float2 s = c[0][e];
 #pragma unroll
                 for (int i = 1; i < ND; ++i) s = __ffma2_rn(c[i][e], kResidueTable.w[q][i], s);
@@ -296,12 +297,19 @@ struct RowDigits {
                 b[2 * e] = __float_as_uint(r.x);
                 b[2 * e + 1] = __float_as_uint(r.y);
             }
-            uint4 words;
-            words.x = pack4(b[0], b[1], b[2], b[3]);
-            words.y = pack4(b[4], b[5], b[6], b[7]);
-            words.z = pack4(b[8], b[9], b[10], b[11]);
-            words.w = pack4(b[12], b[13], b[14], b[15]);
-            store(q, words);
+            if constexpr (NP == 8) {
+                uint4 words;
+                words.x = pack4(b[0], b[1], b[2], b[3]);
+                words.y = pack4(b[4], b[5], b[6], b[7]);
+                words.z = pack4(b[8], b[9], b[10], b[11]);
+                words.w = pack4(b[12], b[13], b[14], b[15]);
+                store(q, words);
+            } else {
+                uint2 words;
+                words.x = pack4(b[0], b[1], b[2], b[3]);
+                words.y = pack4(b[4], b[5], b[6], b[7]);
+                store(q, words);
+            }
         }
     }
 };
@@ -316,20 +324,24 @@ struct ResDesc {
 };
 
 // A' planes: row i holds [Re A(i,:), 0.., Im A(i,:), 0..] with the imaginary
-// half at kh (real: A(i,:)), zeros to kp; 16 bytes of one row per thread,
-// every modulus.
+// half at kh (real: A(i,:)), zeros to kp; every modulus. A thread converts 8
+// entries; the four lanes of a row's 32-byte segment are adjacent, so each
+// warp store writes eight whole 32-byte sectors (8 rows x 32 bytes), and the
+// small per-thread state (48 digit registers) leaves room for twice the
+// warps per SM of a 16-entry thread.
 template <bool CPLX, int ND>
 __global__ void __launch_bounds__(128) residue_a_kernel(const __grid_constant__ Batch<ResDesc> b,
                                                         const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.z);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c0 = blockIdx.y * 16;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + warp * 8 + (lane >> 2);
+    const int c0 = blockIdx.y * 32 + (lane & 3) * 8;
     if (i >= d.rows_p || c0 >= d.kp) return;
     const int shift = cp.t - (i < d.m ? d.e[i] : 0);
     const bool imag = CPLX && c0 >= d.kh;
     const int k0 = imag ? c0 - d.kh : c0;
     const bool rows_live = i < d.m && (!CPLX || c0 < 2 * d.kh);
-    RowDigits<ND> g;
+    RowDigits<ND, 4> g;
     g.take(
         [&](int u) {
             const int k = k0 + u;
@@ -339,23 +351,24 @@ __global__ void __launch_bounds__(128) residue_a_kernel(const __grid_constant__ 
         shift);
     int8_t* row = d.dst + (size_t)i * d.kp + c0;
     const size_t plane = (size_t)d.rows_p * d.kp;
-    g.residues(cp.nm, [&](int q, uint4 w) { *reinterpret_cast<uint4*>(row + q * plane) = w; });
+    g.residues(cp.nm, [&](int q, uint2 w) { *reinterpret_cast<uint2*>(row + q * plane) = w; });
 }
 
 // B' planes, K-major rows of the right factor. Complex: row 2j =
 // [Re B(:,j); -Im B(:,j)], row 2j+1 = [Im B(:,j); Re B(:,j)] (halves at 0 and
-// kh); real: row j = B(:,j); zeros to kp. One thread per 16 entries of one part
-// of one column: a real-part thread writes them to row 2j at 0 and to row 2j+1
-// at kh, an imaginary-part thread to row 2j+1 at 0 and, negated, to row 2j at
-// kh (the residues of -x are the negated residues of x). Threads past the last
-// chunk write the zero tail [2 kh, kp) of both rows.
+// kh); real: row j = B(:,j); zeros to kp. One thread per 8 entries of one part
+// of one column, consecutive threads on consecutive entries (whole sectors
+// per warp store): a real-part thread writes them to row 2j at 0 and to row
+// 2j+1 at kh, an imaginary-part thread to row 2j+1 at 0 and, negated, to row
+// 2j at kh (the residues of -x are the negated residues of x). Threads past
+// the last chunk write the zero tail [2 kh, kp) of both rows.
 template <bool CPLX, int ND>
 __global__ void __launch_bounds__(128) residue_b_kernel(const __grid_constant__ Batch<ResDesc> b,
                                                         const __grid_constant__ CrtParams cp) {
     const ResDesc& d = batch_item(b, blockIdx.y);
     constexpr int DPE = CPLX ? 2 : 1;
-    const int half = (CPLX ? d.kh : d.kp) / 16;  // data chunks of one part
-    const int items = CPLX ? 2 * half + (d.kp - 2 * d.kh) / 16 : half;
+    const int half = (CPLX ? d.kh : d.kp) / 8;  // data chunks of one part
+    const int items = CPLX ? 2 * half + (d.kp - 2 * d.kh) / 8 : half;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int jrows = d.rows_p / DPE;
     if (idx >= (long long)items * jrows) return;
@@ -364,17 +377,17 @@ __global__ void __launch_bounds__(128) residue_b_kernel(const __grid_constant__ 
     int8_t* row0 = d.dst + (size_t)(DPE * j) * d.kp;
     const size_t plane = (size_t)d.rows_p * d.kp;
     if (CPLX && it >= 2 * half) {  // zero tail of both rows
-        const int c0 = 2 * d.kh + (it - 2 * half) * 16;
+        const int c0 = 2 * d.kh + (it - 2 * half) * 8;
         for (int q = 0; q < cp.nm; ++q) {
-            *reinterpret_cast<int4*>(row0 + q * plane + c0) = make_int4(0, 0, 0, 0);
-            *reinterpret_cast<int4*>(row0 + q * plane + d.kp + c0) = make_int4(0, 0, 0, 0);
+            *reinterpret_cast<uint2*>(row0 + q * plane + c0) = make_uint2(0, 0);
+            *reinterpret_cast<uint2*>(row0 + q * plane + d.kp + c0) = make_uint2(0, 0);
         }
         return;
     }
     const bool imag = CPLX && it >= half;
-    const int k0 = (imag ? it - half : it) * 16;
+    const int k0 = (imag ? it - half : it) * 8;
     const int shift = cp.t - (live ? d.e[j] : 0);
-    RowDigits<ND> g;
+    RowDigits<ND, 4> g;
     g.take(
         [&](int u) {
             const int k = k0 + u;
@@ -383,17 +396,16 @@ __global__ void __launch_bounds__(128) residue_b_kernel(const __grid_constant__ 
         },
         shift);
     if (!CPLX) {
-        g.residues(cp.nm, [&](int q, uint4 w) { *reinterpret_cast<uint4*>(row0 + q * plane + k0) = w; });
+        g.residues(cp.nm, [&](int q, uint2 w) { *reinterpret_cast<uint2*>(row0 + q * plane + k0) = w; });
     } else if (!imag) {
-        g.residues(cp.nm, [&](int q, uint4 w) {
-            *reinterpret_cast<uint4*>(row0 + q * plane + k0) = w;
-            *reinterpret_cast<uint4*>(row0 + q * plane + d.kp + d.kh + k0) = w;
+        g.residues(cp.nm, [&](int q, uint2 w) {
+            *reinterpret_cast<uint2*>(row0 + q * plane + k0) = w;
+            *reinterpret_cast<uint2*>(row0 + q * plane + d.kp + d.kh + k0) = w;
         });
     } else {
-        g.residues(cp.nm, [&](int q, uint4 w) {
-            *reinterpret_cast<uint4*>(row0 + q * plane + d.kp + k0) = w;
-            const uint4 n = make_uint4(neg_bytes(w.x), neg_bytes(w.y), neg_bytes(w.z), neg_bytes(w.w));
-            *reinterpret_cast<uint4*>(row0 + q * plane + d.kh + k0) = n;
+        g.residues(cp.nm, [&](int q, uint2 w) {
+            *reinterpret_cast<uint2*>(row0 + q * plane + d.kp + k0) = w;
+            *reinterpret_cast<uint2*>(row0 + q * plane + d.kh + k0) = make_uint2(neg_bytes(w.x), neg_bytes(w.y));
         });
     }
 }
@@ -879,10 +891,10 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         max_m = std::max(max_m, s.m);
         max_cols = std::max(max_cols, s.n);
         max_rows_a = std::max(max_rows_a, s.mp);
-        max_chunks = std::max(max_chunks, s.kp / 16);
-        // residue_b: one thread per 16 entries of one part of a column of B
+        max_chunks = std::max(max_chunks, s.kp / 32);
+        // residue_b: one thread per 8 entries of one part of a column of B
         // plus the zero-tail chunks
-        const long long bchunks = CPLX ? 2 * (s.kh / 16) + (s.kp - 2 * s.kh) / 16 : s.kp / 16;
+        const long long bchunks = CPLX ? 2 * (s.kh / 8) + (s.kp - 2 * s.kh) / 8 : s.kp / 8;
         max_b_threads = std::max(max_b_threads, bchunks * (s.np / DPE));
         max_out_rows = std::max(max_out_rows, s.m);
         max_out_cols = std::max(max_out_cols, s.n);
@@ -896,7 +908,7 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         col_exponent_kernel<CPLX><<<dim3((max_cols + 7) / 8, bc.count), 256, 0, ctx.stream>>>(bc);
         TNS_CUDA(cudaGetLastError());
         Batch<ResDesc> bra = make_batch(ctx, ra);
-        const dim3 grid_a((max_rows_a + 127) / 128, max_chunks, bra.count);
+        const dim3 grid_a((max_rows_a + 31) / 32, max_chunks, bra.count);
         if (digits_for(cp.t) == 6) residue_a_kernel<CPLX, 6><<<grid_a, 128, 0, ctx.stream>>>(bra, cp);
         else residue_a_kernel<CPLX, 7><<<grid_a, 128, 0, ctx.stream>>>(bra, cp);
         TNS_CUDA(cudaGetLastError());
