@@ -64,15 +64,17 @@ struct LuInverseProbe : Probe<TE> {
     Context& ctx;
     const DMat& lu;
     const int* d_piv;
+    bool free_order;
     DMat panel;
-    LuInverseProbe(Context& c, const DMat& lu_, const int* piv, int t)
-        : ctx(c), lu(lu_), d_piv(piv), panel(c, lu_.rows, t, lu_.cplx, "an estimator probe panel") {}
+    LuInverseProbe(Context& c, const DMat& lu_, const int* piv, int t, bool free)
+        : ctx(c), lu(lu_), d_piv(piv), free_order(free), panel(c, lu_.rows, t, lu_.cplx, "an estimator probe panel") {}
     void apply(const typename TE::T* x, typename TE::T* y, int t, bool adjoint) override {
         int n = lu.rows;
         size_t esz = sizeof(double) * TE::kDoubles;
         TNS_CUDA(cudaMemcpy2DAsync(panel.p, (size_t)panel.ld() * esz, x, (size_t)n * esz, (size_t)n * esz, t,
                                    cudaMemcpyHostToDevice, ctx.stream));
-        getrs(ctx, lu, d_piv, panel, t, adjoint);
+        if (free_order) getrs_free_order(ctx, lu, d_piv, panel, t, adjoint);
+        else getrs(ctx, lu, d_piv, panel, t, adjoint);
         TNS_CUDA(cudaMemcpy2DAsync(y, (size_t)n * esz, panel.p, (size_t)panel.ld() * esz, (size_t)n * esz, t,
                                    cudaMemcpyDeviceToHost, ctx.stream));
         ctx.sync();
@@ -164,15 +166,16 @@ NormestResult normest_operator(Context& ctx, int n, bool cplx, ApplyFn apply, Ap
     return estimate<RealE>(op, n, t, itmax, seed);
 }
 
-NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed) {
+NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed,
+                                 bool free_order) {
     int n = lu.rows;
     if (n == 0) return {};
     int tt = std::clamp(t, 1, n);
     if (lu.cplx) {
-        LuInverseProbe<CplxE> op(ctx, lu, d_piv, tt);
+        LuInverseProbe<CplxE> op(ctx, lu, d_piv, tt, free_order);
         return estimate<CplxE>(op, n, t, itmax, seed);
     }
-    LuInverseProbe<RealE> op(ctx, lu, d_piv, tt);
+    LuInverseProbe<RealE> op(ctx, lu, d_piv, tt, free_order);
     return estimate<RealE>(op, n, t, itmax, seed);
 }
 

@@ -1404,6 +1404,63 @@ void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bo
     getrs_batch(ctx, items, adjoint);
 }
 
+void getrs_free_order(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint) {
+    const int n = lu.rows;
+    if (n == 0 || nrhs == 0) return;
+    const bool cplx = lu.cplx;
+    const size_t es = cplx ? 2 : 1;
+    constexpr int bs = 64;
+    const int blocks = (n + bs - 1) / bs;
+    const int ld = lu.ld(), ldb = b.ld();
+    DMat herm;  // the conjugate transpose, for the adjoint's GEMM updates
+    if (adjoint) {
+        herm = DMat(ctx, lu.cols, lu.rows, cplx, "the conjugate transpose of the factors");
+        conj_transpose(ctx, herm, lu);
+    }
+    const double* G = adjoint ? herm.p : lu.p;
+    const int ldg = adjoint ? herm.ld() : ld;
+    auto update = [&](const double* A, const double* X, double* C, int rows, int k) {
+        if (rows <= 0) return;
+        GemmProblem p{};
+        p.A = A;
+        p.B = X;
+        p.C = C;
+        p.lda = ldg;
+        p.ldb = p.ldc = ldb;
+        p.M = round_up(rows, 2);
+        p.N = round_up(nrhs, 2);
+        p.K = round_up(k, 16);
+        p.alpha_re = -1.0;
+        p.beta_re = 1.0;
+        std::vector<GemmProblem> g{p};
+        gemm_grouped(ctx, g, cplx);
+    };
+    if (!adjoint) {
+        std::vector<LaswpDesc> sw{LaswpDesc{b.p, ldb, 0, nrhs, d_piv, 0, n, 0}};
+        launch_laswp(ctx, cplx, sw);
+    }
+    // Forward: L (unit) or U^H (explicit diagonal), then the rows below.
+    for (int kb = 0; kb < blocks; ++kb) {
+        const int k0 = kb * bs, w = std::min(bs, n - k0);
+        std::vector<TrsmDesc> d{TrsmDesc{lu.p + ((size_t)k0 * ld + k0) * es, ld, b.p + (size_t)k0 * es, ldb, w, nrhs, 1,
+                                         adjoint ? 0 : 1, adjoint ? 1 : 0}};
+        launch_trsm(ctx, cplx, 1, d);
+        update(G + ((size_t)k0 * ldg + k0 + w) * es, b.p + (size_t)k0 * es, b.p + (size_t)(k0 + w) * es, n - k0 - w, w);
+    }
+    // Backward: U (explicit diagonal) or L^H (unit), then the rows above.
+    for (int kb = blocks - 1; kb >= 0; --kb) {
+        const int k0 = kb * bs, w = std::min(bs, n - k0);
+        std::vector<TrsmDesc> d{TrsmDesc{lu.p + ((size_t)k0 * ld + k0) * es, ld, b.p + (size_t)k0 * es, ldb, w, nrhs, 0,
+                                         adjoint ? 1 : 0, adjoint ? 1 : 0}};
+        launch_trsm(ctx, cplx, 1, d);
+        update(G + ((size_t)k0 * ldg) * es, b.p + (size_t)k0 * es, b.p, k0, w);
+    }
+    if (adjoint) {
+        std::vector<LaswpDesc> sw{LaswpDesc{b.p, ldb, 0, nrhs, d_piv, 0, n, 1}};
+        launch_laswp(ctx, cplx, sw);
+    }
+}
+
 void solve_triangular(Context& ctx, TriangularKind kind, const DMat& f, DMat& b, int nrhs) {
     const int n = f.rows;
     if (n == 0 || nrhs == 0) return;
@@ -1608,7 +1665,7 @@ void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli,
     };
     factor(moduli > 0 ? moduli : 8);
     const double anorm1 = norm1(ctx, a);
-    const NormestResult est = normest_lu_inverse(ctx, f, piv.as<int>(), 2, 5, 20260915);
+    const NormestResult est = normest_lu_inverse(ctx, f, piv.as<int>(), 2, 5, 20260915, true);
     info.rcond = (anorm1 > 0.0 && est.value > 0.0) ? 1.0 / (anorm1 * est.value) : 0.0;
     if (moduli == 0) {
         const double kappa = info.rcond > 0.0 ? 1.0 / info.rcond : 1e300;
@@ -1620,7 +1677,9 @@ void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli,
     }
     x = DMat(ctx, n, nrhs, cplx, "the solution");
     copy_dmat(ctx, x, b);
-    getrs(ctx, f, piv.as<int>(), x, nrhs, false);
+    // The precision form's solves have no reference order to keep: blocked
+    // triangular solves with DMMA updates.
+    getrs_free_order(ctx, f, piv.as<int>(), x, nrhs, false);
     const double ainf = norminf(ctx, a);
     const std::vector<double> bmax = col_absmax(ctx, b);
     DMat r(ctx, n, nrhs, cplx, "the refinement residual");
@@ -1638,7 +1697,7 @@ void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli,
         info.backward_error = berr;
         if (berr <= 4.0 * 1.1102230246251565e-16 || it >= max_iter || !(berr < 0.5 * prev)) break;
         prev = berr;
-        getrs(ctx, f, piv.as<int>(), r, nrhs, false);
+        getrs_free_order(ctx, f, piv.as<int>(), r, nrhs, false);
         std::vector<EwDesc> add{ew_add_scaled(x, r, 1.0)};
         ew_batch(ctx, add);
         info.iterations++;

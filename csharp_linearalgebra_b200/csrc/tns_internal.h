@@ -328,6 +328,10 @@ struct SolveItem {
 void getrs_batch(Context& ctx, std::vector<SolveItem>& items, bool adjoint);
 // B := A^-1 B or A^-H B from factors (valid n x n), in place on the valid rows of b.
 void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
+// The same solves in no particular order: 64-row triangular blocks and DMMA
+// GEMM updates of the rows beyond them (for the precision form, whose
+// refinement and condition estimate have no reference order to keep).
+void getrs_free_order(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
 // The triangular solves of the reference's kernel seam (KernelEntry.cs:98-173,
 // Triangular.cs) in its order of operations: B := T^-1 B or T^-T B in place
 // for the triangle of f named by kind (real); complex: the unit lower, upper
@@ -353,7 +357,10 @@ struct NormestResult {
     int iterations = 0, products = 0;
 };
 NormestResult normest_power(Context& ctx, const DMat& a, int power, int t, int itmax, int seed);
-NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed);
+// free_order: the probes' solves by getrs_free_order (no reference order to
+// keep: the precision form's condition estimate).
+NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed,
+                                 bool free_order = false);
 
 struct ExpmInfo {
     int degree = 0, squarings = 0;
