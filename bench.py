@@ -415,6 +415,7 @@ def ours(args, world, rank, local, dist):
     # same bits as the reference's algorithm, matrix by matrix.
     cpu = None
     parity = None
+    truth_check = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle
         oracle.lib()
@@ -443,6 +444,22 @@ def ours(args, world, rank, local, dist):
                                      "run the whole sweep's mix"}
         parity = {"matrices_compared": len(sample), "bit_identical": equal, "decisions_equal": decisions,
                   "max_rel_err_1norm": worst}
+        # Both forms against exp(A) itself (the extended-precision exponential),
+        # on the sweep's smallest matrices, one per frequency band.
+        from oracle.extended import expm_extended, has_extended_precision, rel1_extended
+        if has_extended_precision():
+            bands = np.array_split(np.arange(count), args.truth_sample)
+            picks = [int(b[np.argmin([orders[i] for i in b])]) for b in bands if len(b)]
+            rows = []
+            for i in picks:
+                truth = expm_extended(mats[i])
+                rows.append({"n": orders[i], "squarings": plain["diags"][i].squarings,
+                             "plain_vs_exact": rel1_extended(plain["outs"][i].cpu().numpy().T, truth),
+                             "split_vs_exact": rel1_extended(split["outs"][i].cpu().numpy().T, truth)})
+            truth_check = {"matrices": rows,
+                           "max_split_over_plain": max(r["split_vs_exact"] / r["plain_vs_exact"] for r in rows),
+                           "exact": "exp(A) by Taylor scaling and squaring in 80-bit long double (about 2^-9 of "
+                                    "an FP64 computation's rounding on these matrices)"}
 
     def dmma_roofline(r):
         st = r["st"]
@@ -521,7 +538,8 @@ def ours(args, world, rank, local, dist):
                 "decisions": "degree and s equal the plain form's (the reference's) for every matrix (asserted); "
                              "A^2, A^4, A^6 from the split product with bounds holding the reference's d4, d6; "
                              "matrices whose decision was not settled on the bounds recomputed them in FP64",
-                "exact_fallbacks_per_sweep": int(split["st"]["exact_fallbacks"])},
+                "exact_fallbacks_per_sweep": int(split["st"]["exact_fallbacks"]),
+                "vs_exact": truth_check},
             "plain_fp64": {"value": rate(plain["ms"]), "ms_per_step": plain["ms"],
                            "e2e": rate(plain["e2e_ms"]), "gpu_launches": int(plain["st_step"]["kernel_launches"]),
                            "parity_vs_reference": parity, "roofline": dmma_roofline(plain),
@@ -585,7 +603,25 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
     cores = oracle.threads()
     res = {}
 
+    def wanted(k):
+        return args.only_config in (0, k)
+
     # (1) FP64 GEMM m = n = k = 1024, uniform [-1, 1), alpha 1, beta 0.
+    if wanted(1):
+        config_gemm(args, ws, torch, oracle, res, gpu_ms, cpu_s, cores, peak64)
+    if wanted(2):
+        config_dense(args, ws, oracle, res, gpu_ms, cpu_s)
+    if wanted(3):
+        config_precision(args, ws, oracle, res, gpu_ms, cpu_s, peak8)
+    if wanted(4):
+        config_expmv(args, ws, torch, oracle, res, gpu_ms, cpu_s, sweep)
+    if wanted(5):
+        config_differentiation(args, ws, res, gpu_ms)
+    return res
+
+
+def config_gemm(args, ws, torch, oracle, res, gpu_ms, cpu_s, cores, peak64):
+    """(1) FP64 GEMM m = n = k = 1024."""
     rng = np.random.default_rng(args.seed + 1)
     n = 1024
     a = np.asfortranarray(rng.uniform(-1.0, 1.0, (n, n)))
@@ -611,8 +647,10 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
         "bit_identical_to_reference": bool(np.array_equal(c, cref))}
     del da, db, dc
 
-    # (2) n = 512: LU + solve of 8 right-hand sides + rcond, real and complex;
-    # Expm over 32 draws with ||A||_1 log-uniform in [1e-2, 1e3].
+
+def config_dense(args, ws, oracle, res, gpu_ms, cpu_s):
+    """(2) n = 512: LU + solve of 8 right-hand sides + rcond, real and complex;
+    Expm over 32 draws with ||A||_1 log-uniform in [1e-2, 1e3]."""
     n = 512
     two = {}
     for kind in ("real", "complex"):
@@ -666,7 +704,9 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
                      "CPU: the oracle on all host threads, the same inputs")
     res["2_dense_path_512"] = two
 
-    # (3) precision form: n = 4096, 64 right-hand sides, A = U diag(sigma) V^T.
+
+def config_precision(args, ws, oracle, res, gpu_ms, cpu_s, peak8):
+    """(3) precision form: n = 4096, 64 right-hand sides, A = U diag(sigma) V^T."""
     n, nrhs = 4096, 64
     rng = np.random.default_rng(args.seed + 4)
     u, _ = np.linalg.qr(rng.standard_normal((n, n)))
@@ -714,10 +754,11 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
         "timing": "CUDA events around the modular GEMM launches of one real 4096^3 split product"}
     three["timing"] = "GPU: the host-buffer calls, one run each (factorization included); CPU: the oracle"
     res["3_precision_solve_4096"] = three
-    del u, v
 
-    # (4) the batched exponential action over the sweep: B n x 8, t = 0.5.
-    # the benchmark's own sweep, already on the device
+
+def config_expmv(args, ws, torch, oracle, res, gpu_ms, cpu_s, sweep):
+    """(4) the batched exponential action over the benchmark's own sweep (on
+    the device already): B n x 8, t = 0.5."""
     orders, all_mats, dev_a = sweep
     omegas = np.logspace(2.0, 6.0, len(orders))
     ms_sel, sel = gpu_ms(lambda: ws.expmv_select_batched([t.data_ptr() for t in dev_a], 8, 0.5, device=True,
@@ -770,8 +811,10 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
                        == (i["degree"], i["scaling"], i["applications"]) for k, (_, i) in zip(cpu_pick, refs))}}
     del dev_b, dev_o
 
-    # (5) differentiation: gradient of ||exp(tA)B - Y||_F^2 at n = 2048 (w = 1e4,
-    # B 2048 x 16, t = 1) and the Frechet derivative at n = 1024.
+
+def config_differentiation(args, ws, res, gpu_ms):
+    """(5) differentiation: gradient of ||exp(tA)B - Y||_F^2 at n = 2048
+    (w = 1e4, B 2048 x 16, t = 1) and the Frechet derivative at n = 1024."""
     five = {}
     n = 2048
     a5 = sweep_matrix(10_000, n, 1e4, args.seed + 6)
@@ -805,7 +848,6 @@ def other_configurations(args, ws, torch, peak64, peak8, sweep):
     five["cpu_baseline_note"] = ("not timed by default: the reference's route is Expm of the 2048-order block, "
                                  "tens of seconds of the oracle")
     res["5_differentiation"] = five
-    return res
 
 
 def main():
@@ -819,6 +861,7 @@ def main():
     p.add_argument("--seed", type=int, default=20260915)
     p.add_argument("--cpu-sample", type=int, default=16, help="matrices in the stratified CPU sample")
     p.add_argument("--ref-chunks", type=int, default=4, help="reference arm: the sample in this many steps")
+    p.add_argument("--truth-sample", type=int, default=8, help="matrices checked against the extended-precision exp")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     p.add_argument("--no-peak", action="store_true", help="skip the measured FP64/INT8 peaks (profiling runs)")
@@ -829,6 +872,7 @@ def main():
     p.add_argument("--autotune", type=int, default=0, help="1: GEMM launch shapes chosen by timing (tns_set_autotune)")
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' measurements")
     p.add_argument("--configs-only", action="store_true", help="only the other configurations' measurements")
+    p.add_argument("--only-config", type=int, default=0, help="with --configs-only: just this one (1..5)")
     p.add_argument("--expmv-wmax", type=float, default=1e4,
                    help="batched Expmv: time the sweep's matrices up to this frequency")
     p.add_argument("--shard", choices=["lpt", "seeds"], default="lpt",

@@ -9,7 +9,8 @@ grows about twofold per squaring on these matrices, so the scaling is kept
 close to the one Al-Mohy and Higham's algorithm takes (||A/2^s|| near 5.4):
 at most two squarings more. Every step is in long double, so the result
 carries about 2^-11 x 4 = 2^-9 of the rounding error of an FP64 computation
-of the same matrix. This is test infrastructure, run on the host only.
+of the same matrix. This is test infrastructure, run on the host only: the
+tests and the benchmark's accuracy check measure the GPU forms against it.
 """
 from __future__ import annotations
 

@@ -1,4 +1,4 @@
-"""The extended-precision exponential (tests/extended_expm.py) that the GPU
+"""The extended-precision exponential (oracle/extended.py) that the GPU
 forms' accuracy is measured against: it must be far more accurate than FP64
 before it can tell two FP64 results apart."""
 import math
@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 import scipy.linalg
 
-from extended_expm import expm_extended, has_extended_precision, rel1_extended
+from oracle.extended import expm_extended, has_extended_precision, rel1_extended
 
 pytestmark = pytest.mark.skipif(not has_extended_precision(), reason="long double is not the 80-bit format")
 

@@ -1,6 +1,6 @@
 """Both GPU forms of Expm against exp(A) itself.
 
-The truth is the extended-precision exponential of tests/extended_expm.py
+The truth is the extended-precision exponential of oracle/extended.py
 (long double, about 2^-9 of an FP64 computation's rounding on these
 matrices). The plain form is the reference's arithmetic bit for bit, so its
 distance to the truth is the reference's own error; the split form's must be
@@ -14,7 +14,7 @@ import math
 import numpy as np
 import pytest
 
-from extended_expm import expm_extended, has_extended_precision, rel1_extended
+from oracle.extended import expm_extended, has_extended_precision, rel1_extended
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not has_extended_precision(), reason="long double is not the 80-bit format")]
