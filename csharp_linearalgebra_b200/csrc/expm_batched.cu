@@ -95,10 +95,12 @@ std::vector<int> ell_batch(Context& ctx, const std::vector<const DMat*>& mats, i
     return out;
 }
 
-// normest1 of A^p (t = 2, itmax = 5, the default seed) for a set of matrices:
-// every estimator's products of one round run in one launch per power step.
+// normest1 of A_k^p_k (t = 2, itmax = 5, the default seed) for a set of
+// (matrix, power) items: every estimator's products of one round run in one
+// launch per power step (items of a lower power drop out of the later steps).
 template <class TE>
-std::vector<double> power_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+std::vector<double> power_estimates(Context& ctx, const std::vector<const DMat*>& mats,
+                                    const std::vector<int>& powers) {
     using Est = Estimator<TE>;
     const size_t cnt = mats.size();
     std::vector<double> out(cnt, 0.0);
@@ -127,22 +129,28 @@ std::vector<double> power_estimates(Context& ctx, const std::vector<const DMat*>
                 std::copy(src, src + (size_t)mats[k]->rows * est[k]->t() * TE::kDoubles, host.data() + offs[k]);
             }
             TNS_CUDA(cudaMemcpyAsync(d0.p, host.data(), sizeof(double) * total, cudaMemcpyHostToDevice, ctx.stream));
-            double* src = d0.as<double>();
-            double* dst = d1.as<double>();
-            for (int step = 0; step < power; ++step) {
+            // Each item ping-pongs between its slots of the two buffers; after
+            // an odd number of steps its result is in d1.
+            int maxp = 0;
+            for (size_t k : live) maxp = std::max(maxp, powers[k]);
+            for (int step = 0; step < maxp; ++step) {
+                double* src = (step % 2 == 0) ? d0.as<double>() : d1.as<double>();
+                double* dst = (step % 2 == 0) ? d1.as<double>() : d0.as<double>();
                 std::vector<PanelDesc> v;
                 for (size_t k : live) {
+                    if (powers[k] <= step) continue;
                     int n = mats[k]->rows;
                     v.push_back(PanelDesc{mats[k]->p, n, mats[k]->ld(), src + offs[k], n, dst + offs[k], n, est[k]->t()});
                 }
                 panel_product_batch(ctx, v, cplx, adjoint);
-                std::swap(src, dst);
             }
-            TNS_CUDA(cudaMemcpyAsync(host.data(), src, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
+            TNS_CUDA(cudaMemcpyAsync(host.data(), d0.p, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
+            std::vector<double> odd(total);
+            TNS_CUDA(cudaMemcpyAsync(odd.data(), d1.p, sizeof(double) * total, cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
             for (size_t k : live) {
                 double* dstp = reinterpret_cast<double*>(adjoint ? est[k]->z() : est[k]->y());
-                const double* from = host.data() + offs[k];
+                const double* from = (powers[k] % 2 == 0 ? host.data() : odd.data()) + offs[k];
                 std::copy(from, from + (size_t)mats[k]->rows * est[k]->t() * TE::kDoubles, dstp);
                 if (adjoint) est[k]->adjointed();
                 else est[k]->applied();
@@ -157,9 +165,13 @@ std::vector<double> power_estimates(Context& ctx, const std::vector<const DMat*>
     return out;
 }
 
-std::vector<double> power_norms(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+std::vector<double> power_norms(Context& ctx, const std::vector<const DMat*>& mats, const std::vector<int>& powers) {
     if (mats.empty()) return {};
-    return mats[0]->cplx ? power_estimates<CplxE>(ctx, mats, power) : power_estimates<RealE>(ctx, mats, power);
+    return mats[0]->cplx ? power_estimates<CplxE>(ctx, mats, powers) : power_estimates<RealE>(ctx, mats, powers);
+}
+
+std::vector<double> power_norms(Context& ctx, const std::vector<const DMat*>& mats, int power) {
+    return power_norms(ctx, mats, std::vector<int>(mats.size(), power));
 }
 
 // Whether a product may take the split-precision form when the context asks
@@ -183,8 +195,9 @@ void product_batch(Context& ctx, std::vector<std::pair<const DMat*, const DMat*>
 
 }  // namespace
 
-std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power) {
-    return power_norms(ctx, mats, power);
+std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats,
+                                         const std::vector<int>& powers) {
+    return power_norms(ctx, mats, powers);
 }
 
 void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,

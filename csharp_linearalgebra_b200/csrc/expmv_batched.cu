@@ -694,9 +694,19 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
         }
     }
     std::vector<std::vector<double>> dp(cnt, std::vector<double>(kMaxPower + 2, std::numeric_limits<double>::quiet_NaN()));
-    for (int p = 2; p <= kMaxPower + 1 && !sharp.empty(); ++p) {
-        std::vector<double> v = power_norm_estimates(ctx, sharp_mats, p);
-        for (size_t q = 0; q < sharp.size(); ++q) dp[sharp[q]][p] = std::pow(v[q], 1.0 / p);
+    if (!sharp.empty()) {
+        // Every (matrix, power) estimator of the batch advances together.
+        std::vector<const DMat*> items;
+        std::vector<int> powers;
+        for (int p = 2; p <= kMaxPower + 1; ++p)
+            for (const DMat* m : sharp_mats) {
+                items.push_back(m);
+                powers.push_back(p);
+            }
+        std::vector<double> v = power_norm_estimates(ctx, items, powers);
+        size_t q = 0;
+        for (int p = 2; p <= kMaxPower + 1; ++p)
+            for (size_t k = 0; k < sharp.size(); ++k) dp[sharp[k]][p] = std::pow(v[q++], 1.0 / p);
     }
 
     // (m, s), eta and the coefficients, per matrix (Run, :258-283).

@@ -393,9 +393,10 @@ void expmv_taylor_host(Context& ctx, const DMat& shifted, const DMat& b, double 
 // MatrixExponentialAction.SelectParameters (:347-398).
 void expmv_select_parameters(double scaled_norm, const std::function<double(int)>* alpha, double scale, int cols,
                              int& m, int& s);
-// normest1 (t = 2, itmax = 5, the default seed) of A_k^power for a set of
-// matrices, every estimator's product step in one launch.
-std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats, int power);
+// normest1 (t = 2, itmax = 5, the default seed) of A_k^p_k for a set of
+// (matrix, power) items, every estimator's product step in one launch.
+std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const DMat*>& mats,
+                                         const std::vector<int>& powers);
 // The matrix-free form: y := A x by a caller's function on device panels.
 using ApplyFn = int (*)(void* user, int ncols, const double* x, double* y, int ld, void* stream);
 void expmv_operator(Context& ctx, int n, ApplyFn apply, void* user, const DMat& b, double t, double bound,
