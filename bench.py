@@ -633,15 +633,25 @@ def config_gemm(args, ws, torch, oracle, res, gpu_ms, cpu_s, cores, peak64):
     e2e_ms, c = gpu_ms(lambda: ws.multiply(a, b), reps=5)
     cs, cref = cpu_s(lambda: oracle.gemm(a, b))
     flops = 2.0 * n ** 3
+    kernel_ms = []
+    for _ in range(5):
+        ws.reset_stats()
+        ws.set_timing(True)
+        ws._call("tns_dgemm_device", n, n, n, 1.0, da.data_ptr(), n, db.data_ptr(), n, 0.0, dc.data_ptr(), n)
+        ws.set_timing(False)
+        kernel_ms.append(ws.stats()["gemm_ms"])
+    kms = statistics.median(kernel_ms)
     res["1_fp64_gemm_1024"] = {
         "value": flops / (dev_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "ms": dev_ms,
         "timing": "tns_dgemm_device (operands in HBM, padded copies inside the call)",
         "e2e": {"value": flops / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "ms": e2e_ms,
                 "h2d_bytes": 2 * 8 * n * n, "d2h_bytes": 8 * n * n},
         "roofline": {"bound": "tensor", "kernel": "gemm_dmma_kernel (FP64 DMMA)", "peak": peak64, "unit": "TFLOP/s",
-                     "achieved": flops / (dev_ms * 1e-3) / 1e12,
-                     "frac": (flops / (dev_ms * 1e-3) / 1e12 / peak64) if peak64 else None,
-                     "peak_source": "cuBLAS DGEMM 8192^3 in this process"},
+                     "achieved": flops / (kms * 1e-3) / 1e12, "kernel_ms": kms,
+                     "frac": (flops / (kms * 1e-3) / 1e12 / peak64) if peak64 else None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 in this process",
+                     "timing": "CUDA events around the GEMM kernel alone (the call's padded copies leave the "
+                               "operands in L2)"},
         "cpu_baseline": {"value": flops / cs / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
                          "sample": "the same product, the reference's threaded blocking (KC 256)"},
         "bit_identical_to_reference": bool(np.array_equal(c, cref))}

@@ -15,8 +15,12 @@
 // all of X, staged through shared memory by cp.async in 32-deep k tiles (a
 // 4-stage ring); one thread owns one (row, column) pair and sums in k order
 // with the reference's rounding (PanelProduct.Apply's axpy order, a product
-// and a sum per term, zero x skipped; the complex operator's four real sums
-// then (pr - qi, pi + qr), LinearOperators.cs:262-282). The epilogue scales
+// and a sum per term; the complex operator's four real sums then
+// (pr - qi, pi + qr), LinearOperators.cs:262-282). The reference skips a term
+// whose x is zero; forming it instead adds +-0 to a sum that is never -0,
+// which changes nothing as long as A is finite -- and an operator with a
+// non-finite entry has a non-finite ||A - mu I||_1, which the parameter
+// search refuses (TNS_E_OUT_OF_RANGE) before any recurrence runs. The epilogue scales
 // the sums by t/(s(j+1)) into the next work panel, adds them into F and forms
 // both row sums of moduli in column order (InfinityNorm). Every CTA writes
 // its largest row sums to its slot, the group meets at a barrier, and every
@@ -52,9 +56,15 @@ namespace tns {
 
 namespace {
 
-constexpr int kRows = 64;                  // rows per chunk of a CTA's row range
-constexpr int kSlots = 8;                  // column slots per row
-constexpr int kThreadsT = kRows * kSlots;  // 512 threads: (row, column slot)
+constexpr int kThreadsT = 512;  // threads per CTA: (row, column slot) pairs
+
+// The thread layout, per launch: SLOTS column slots per row (8 for panels of
+// up to 8 columns, else 16), CPT columns per slot (c + SLOTS q), ROWS =
+// 512 / SLOTS rows per chunk of a CTA's row range.
+template <int SLOTS_, int CPT_>
+struct Shape {
+    static constexpr int SLOTS = SLOTS_, CPT = CPT_, ROWS = kThreadsT / SLOTS_;
+};
 constexpr int kKT = 32;                    // k per staged tile
 constexpr int kStagesT = 4;                // cp.async ring depth
 constexpr double kU = 1.1102230246251565e-16;
@@ -240,53 +250,54 @@ __device__ __forceinline__ double modulus(double re, double im) {
 
 // Row sums of moduli over the columns in column order (InfinityNorm,
 // ComplexKernels.cs:164-180 / Norms.cs:50-66): the 8 lanes of a row hold its
-// columns c + 8q; every lane ends with its row's sum.
-template <int CPT>
-__device__ __forceinline__ double row_sum(const double (&v)[CPT], int ncols) {
-    const int base = threadIdx.x & 24;  // first lane of this row in the warp
+// columns c + SLOTS q; every lane ends with its row's sum.
+template <class S>
+__device__ __forceinline__ double row_sum(const double (&v)[S::CPT], int ncols) {
+    const int base = threadIdx.x & (32 - S::SLOTS);  // first lane of this row in the warp
     double sum = 0.0;
 #pragma unroll
-    for (int q = 0; q < CPT; ++q)
+    for (int q = 0; q < S::CPT; ++q)
 #pragma unroll
-        for (int c = 0; c < kSlots; ++c) {
+        for (int c = 0; c < S::SLOTS; ++c) {
             const double x = __shfl_sync(0xffffffffu, v[q], base + c);
-            if (q * kSlots + c < ncols) sum = add_rn(sum, x);
+            if (q * S::SLOTS + c < ncols) sum = add_rn(sum, x);
         }
     return sum;
 }
 
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 struct Tiles {
     static constexpr int ES = CPLX ? 2 : 1;                 // doubles per element
     static constexpr int XS = CPLX ? kKT + 1 : kKT + 2;     // elements per staged X column
-    static constexpr int A_DOUBLES = kKT * kRows * ES;
-    static constexpr int X_DOUBLES = kSlots * CPT * XS * ES;
+    static constexpr int A_DOUBLES = kKT * S::ROWS * ES;
+    static constexpr int X_DOUBLES = S::SLOTS * S::CPT * XS * ES;
     static constexpr int STAGE = A_DOUBLES + X_DOUBLES;
     static constexpr size_t SMEM = sizeof(double) * (size_t)STAGE * kStagesT;
 };
 
 // Stage k tile [k0, k0 + kKT) of the CTA's rows [r0, r0 + rows) of A and of
 // the work panel x (all columns) into stage buffer `buf`.
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 __device__ __forceinline__ void stage_tile(double* buf, const TaylorDesc& d, const double* x, int ncols, int r0,
                                            int rows, int k0) {
-    using T = Tiles<CPLX, CPT>;
+    using T = Tiles<CPLX, S>;
+    constexpr int R = S::ROWS;
     double* sA = buf;
     double* sX = buf + T::A_DOUBLES;
     const int tid = threadIdx.x;
     if constexpr (CPLX) {
-        for (int e = tid; e < kKT * kRows; e += kThreadsT) {
-            const int k = e >> 6, r = e & 63;
-            if (r < rows) cp16(sA + (k * kRows + r) * 2, d.a + ((size_t)(k0 + k) * d.lda + r0 + r) * 2);
+        for (int e = tid; e < kKT * R; e += kThreadsT) {
+            const int k = e / R, r = e % R;
+            if (r < rows) cp16(sA + (k * R + r) * 2, d.a + ((size_t)(k0 + k) * d.lda + r0 + r) * 2);
         }
         for (int e = tid; e < ncols * kKT; e += kThreadsT) {
             const int col = e >> 5, k = e & 31;
             cp16(sX + (col * T::XS + k) * 2, x + ((size_t)col * d.ldp + k0 + k) * 2);
         }
     } else {
-        for (int e = tid; e < kKT * (kRows / 2); e += kThreadsT) {
-            const int k = e >> 5, rp = (e & 31) * 2;
-            if (rp < rows) cp16(sA + k * kRows + rp, d.a + (size_t)(k0 + k) * d.lda + r0 + rp);
+        for (int e = tid; e < kKT * (R / 2); e += kThreadsT) {
+            const int k = e / (R / 2), rp = (e % (R / 2)) * 2;
+            if (rp < rows) cp16(sA + k * R + rp, d.a + (size_t)(k0 + k) * d.lda + r0 + rp);
         }
         for (int e = tid; e < ncols * (kKT / 2); e += kThreadsT) {
             const int col = e >> 4, kp = (e & 15) * 2;
@@ -296,30 +307,31 @@ __device__ __forceinline__ void stage_tile(double* buf, const TaylorDesc& d, con
 }
 
 // acc := (rows r0.. of A) * x for this thread's (row, columns), in k order.
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d, const double* x, int ncols, int r0,
-                                              int rows, double (&acc)[CPT][CPLX ? 4 : 1]) {
-    using T = Tiles<CPLX, CPT>;
-    const int rr = threadIdx.x >> 3, c = threadIdx.x & 7;
+                                              int rows, double (&acc)[S::CPT][CPLX ? 4 : 1]) {
+    using T = Tiles<CPLX, S>;
+    constexpr int R = S::ROWS;
+    const int rr = threadIdx.x / S::SLOTS, c = threadIdx.x % S::SLOTS;
 #pragma unroll
-    for (int q = 0; q < CPT; ++q)
+    for (int q = 0; q < S::CPT; ++q)
 #pragma unroll
         for (int z = 0; z < (CPLX ? 4 : 1); ++z) acc[q][z] = 0.0;
     const int n = d.n;
     const int ktiles = (n + kKT - 1) / kKT;
 #pragma unroll
     for (int st = 0; st < kStagesT - 1; ++st) {
-        if (st < ktiles) stage_tile<CPLX, CPT>(smem + st * T::STAGE, d, x, ncols, r0, rows, st * kKT);
+        if (st < ktiles) stage_tile<CPLX, S>(smem + st * T::STAGE, d, x, ncols, r0, rows, st * kKT);
         cp_commit();
     }
-    bool col_ok[CPT];
+    bool col_ok[S::CPT];
 #pragma unroll
-    for (int q = 0; q < CPT; ++q) col_ok[q] = c + q * kSlots < ncols;
+    for (int q = 0; q < S::CPT; ++q) col_ok[q] = c + q * S::SLOTS < ncols;
     for (int kt = 0; kt < ktiles; ++kt) {
         cp_wait<kStagesT - 2>();
         __syncthreads();
         const int nxt = kt + kStagesT - 1;
-        if (nxt < ktiles) stage_tile<CPLX, CPT>(smem + (nxt % kStagesT) * T::STAGE, d, x, ncols, r0, rows, nxt * kKT);
+        if (nxt < ktiles) stage_tile<CPLX, S>(smem + (nxt % kStagesT) * T::STAGE, d, x, ncols, r0, rows, nxt * kKT);
         cp_commit();
         const double* sA = smem + (kt % kStagesT) * T::STAGE;
         const double* sX = sA + T::A_DOUBLES;
@@ -330,16 +342,15 @@ __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d,
                 const double2* x2 = reinterpret_cast<const double2*>(sX) + c * T::XS;
 #pragma unroll 4
                 for (int kk = 0; kk < klen; ++kk) {
-                    const double2 av = a2[kk * kRows];
+                    const double2 av = a2[kk * R];
 #pragma unroll
-                    for (int q = 0; q < CPT; ++q) {
+                    for (int q = 0; q < S::CPT; ++q) {
                         if (!col_ok[q]) continue;
-                        const double2 xv = x2[q * kSlots * T::XS + kk];
-                        const bool nr = xv.x != 0.0, ni = xv.y != 0.0;
-                        acc[q][0] = add_rn(acc[q][0], nr ? mul_rn(xv.x, av.x) : 0.0);  // pr
-                        acc[q][2] = add_rn(acc[q][2], nr ? mul_rn(xv.x, av.y) : 0.0);  // qr
-                        acc[q][1] = add_rn(acc[q][1], ni ? mul_rn(xv.y, av.x) : 0.0);  // pi
-                        acc[q][3] = add_rn(acc[q][3], ni ? mul_rn(xv.y, av.y) : 0.0);  // qi
+                        const double2 xv = x2[q * S::SLOTS * T::XS + kk];
+                        acc[q][0] = add_rn(acc[q][0], mul_rn(xv.x, av.x));  // pr
+                        acc[q][2] = add_rn(acc[q][2], mul_rn(xv.x, av.y));  // qr
+                        acc[q][1] = add_rn(acc[q][1], mul_rn(xv.y, av.x));  // pi
+                        acc[q][3] = add_rn(acc[q][3], mul_rn(xv.y, av.y));  // qi
                     }
                 }
             } else {
@@ -347,12 +358,12 @@ __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d,
                 const double* x1 = sX + c * T::XS;
 #pragma unroll 4
                 for (int kk = 0; kk < klen; ++kk) {
-                    const double av = a1[kk * kRows];
+                    const double av = a1[kk * R];
 #pragma unroll
-                    for (int q = 0; q < CPT; ++q) {
+                    for (int q = 0; q < S::CPT; ++q) {
                         if (!col_ok[q]) continue;
-                        const double xv = x1[q * kSlots * T::XS + kk];
-                        acc[q][0] = add_rn(acc[q][0], xv != 0.0 ? mul_rn(xv, av) : 0.0);
+                        const double xv = x1[q * S::SLOTS * T::XS + kk];
+                        acc[q][0] = add_rn(acc[q][0], mul_rn(xv, av));
                     }
                 }
             }
@@ -362,8 +373,9 @@ __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d,
     __syncthreads();
 }
 
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_constant__ TaylorLaunch L) {
+    constexpr int CPT = S::CPT, R = S::ROWS;
     extern __shared__ __align__(128) double smem[];
     __shared__ double s_red[64];
     __shared__ int s_nan[64];
@@ -371,7 +383,7 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
     __shared__ double s_norm[2];
     __shared__ int s_flag;
     const int ncols = L.ncols;
-    const int rr = threadIdx.x >> 3, cs = threadIdx.x & 7;
+    const int rr = threadIdx.x / S::SLOTS, cs = threadIdx.x % S::SLOTS;
     for (int e = L.plan_off[blockIdx.x]; e < L.plan_off[blockIdx.x + 1]; ++e) {
         const TaylorPlan pl = L.plan[e];
         const TaylorDesc d = L.descs[pl.matrix];
@@ -382,13 +394,13 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
 
         // F := B, work := B, c1 = ||B||_inf (Run, :274-276, :285).
         NormAcc n0, n1;
-        for (int r0 = rbeg; r0 < rend; r0 += kRows) {
+        for (int r0 = rbeg; r0 < rend; r0 += R) {
             const int i = r0 + rr;
             const bool row_ok = i < rend;
             double v[CPT];
 #pragma unroll
             for (int q = 0; q < CPT; ++q) {
-                const int col = cs + q * kSlots;
+                const int col = cs + q * S::SLOTS;
                 v[q] = 0.0;
                 if (row_ok && col < ncols) {
                     const size_t bi = ((size_t)col * d.ldb + i) * es, pi = ((size_t)col * d.ldp + i) * es;
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
                     v[q] = modulus<CPLX>(re, im);
                 }
             }
-            const double rs = row_sum<CPT>(v, ncols);
+            const double rs = row_sum<S>(v, ncols);
             if (row_ok) n0.add(rs);
         }
         if (!group_norms(d, rank, phase, L, n0, n1, s_red, s_nan, s_part, s_norm, &s_flag)) return;
@@ -415,16 +427,16 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
             for (int j = 0; j < d.m; ++j) {
                 const double coeff = d.coeff[j];
                 NormAcc nw, nf;
-                for (int r0 = rbeg; r0 < rend; r0 += kRows) {
-                    const int rows = min(kRows, rend - r0);
+                for (int r0 = rbeg; r0 < rend; r0 += R) {
+                    const int rows = min(R, rend - r0);
                     double acc[CPT][CPLX ? 4 : 1];
-                    product_chunk<CPLX, CPT>(smem, d, win, ncols, r0, rows, acc);
+                    product_chunk<CPLX, S>(smem, d, win, ncols, r0, rows, acc);
                     const int i = r0 + rr;
                     const bool row_ok = rr < rows;
                     double vw[CPT], vf[CPT];
 #pragma unroll
                     for (int q = 0; q < CPT; ++q) {
-                        const int col = cs + q * kSlots;
+                        const int col = cs + q * S::SLOTS;
                         vw[q] = 0.0;
                         vf[q] = 0.0;
                         if (row_ok && col < ncols) {
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
                             }
                         }
                     }
-                    const double sw = row_sum<CPT>(vw, ncols), sf = row_sum<CPT>(vf, ncols);
+                    const double sw = row_sum<S>(vw, ncols), sf = row_sum<S>(vf, ncols);
                     if (row_ok) {
                         nw.add(sw);
                         nf.add(sf);
@@ -472,13 +484,13 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
             }
             // F *= eta (ScaleInPlace, :455-464); work := F (CopyInto); c1 = ||work||_inf.
             NormAcc ne, unused;
-            for (int r0 = rbeg; r0 < rend; r0 += kRows) {
+            for (int r0 = rbeg; r0 < rend; r0 += R) {
                 const int i = r0 + rr;
                 const bool row_ok = i < rend;
                 double v[CPT];
 #pragma unroll
                 for (int q = 0; q < CPT; ++q) {
-                    const int col = cs + q * kSlots;
+                    const int col = cs + q * S::SLOTS;
                     v[q] = 0.0;
                     if (row_ok && col < ncols) {
                         const size_t pi = ((size_t)col * d.ldp + i) * es;
@@ -501,7 +513,7 @@ __global__ void __launch_bounds__(kThreadsT, 1) taylor_kernel(const __grid_const
                         v[q] = modulus<CPLX>(re, im);
                     }
                 }
-                const double rs = row_sum<CPT>(v, ncols);
+                const double rs = row_sum<S>(v, ncols);
                 if (row_ok) ne.add(rs);
             }
             if (!group_norms(d, rank, phase, L, ne, unused, s_red, s_nan, s_part, s_norm, &s_flag)) return;
@@ -552,29 +564,43 @@ std::vector<double> traces(Context& ctx, const std::vector<const DMat*>& as) {
 
 const int kEll = 2, kMaxPower = 8;
 
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 void launch_taylor(Context& ctx, const TaylorLaunch& L, int grid) {
-    using T = Tiles<CPLX, CPT>;
-    TNS_CUDA(cudaFuncSetAttribute(taylor_kernel<CPLX, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    using T = Tiles<CPLX, S>;
+    TNS_CUDA(cudaFuncSetAttribute(taylor_kernel<CPLX, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
     void* args[] = {const_cast<TaylorLaunch*>(&L)};
-    TNS_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(taylor_kernel<CPLX, CPT>), dim3(grid),
+    TNS_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(taylor_kernel<CPLX, S>), dim3(grid),
                                          dim3(kThreadsT), args, T::SMEM, ctx.stream));
     ctx.kernel_launches++;
 }
 
-template <bool CPLX, int CPT>
+template <bool CPLX, class S>
 int resident_ctas(Context& ctx) {
-    using T = Tiles<CPLX, CPT>;
-    TNS_CUDA(cudaFuncSetAttribute(taylor_kernel<CPLX, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    using T = Tiles<CPLX, S>;
+    TNS_CUDA(cudaFuncSetAttribute(taylor_kernel<CPLX, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
     int per_sm = 0;
-    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, taylor_kernel<CPLX, CPT>, kThreadsT, T::SMEM));
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, taylor_kernel<CPLX, S>, kThreadsT, T::SMEM));
     if (per_sm < 1) fail(TNS_E_DEVICE, "the Taylor kernel cannot be resident on this device");
     return per_sm * ctx.num_sms;
 }
 
-int ctas_for(Context& ctx, bool cplx, int cpt) {
-    if (cplx) return cpt == 1 ? resident_ctas<true, 1>(ctx) : cpt == 2 ? resident_ctas<true, 2>(ctx) : resident_ctas<true, 4>(ctx);
-    return cpt == 1 ? resident_ctas<false, 1>(ctx) : cpt == 2 ? resident_ctas<false, 2>(ctx) : resident_ctas<false, 4>(ctx);
+// One kernel instance per (element type, layout); L null: only the count of
+// resident CTAs.
+template <bool CPLX>
+int taylor_dispatch(Context& ctx, int layout, const TaylorLaunch* L, int grid) {
+    using S8 = Shape<8, 1>;
+    using S16 = Shape<16, 1>;
+    using S16x2 = Shape<16, 2>;
+    if (!L) return layout == 0 ? resident_ctas<CPLX, S8>(ctx) : layout == 1 ? resident_ctas<CPLX, S16>(ctx)
+                                                                              : resident_ctas<CPLX, S16x2>(ctx);
+    if (layout == 0) launch_taylor<CPLX, S8>(ctx, *L, grid);
+    else if (layout == 1) launch_taylor<CPLX, S16>(ctx, *L, grid);
+    else launch_taylor<CPLX, S16x2>(ctx, *L, grid);
+    return grid;
+}
+
+int taylor(Context& ctx, bool cplx, int layout, const TaylorLaunch* L, int grid) {
+    return cplx ? taylor_dispatch<true>(ctx, layout, L, grid) : taylor_dispatch<false>(ctx, layout, L, grid);
 }
 
 // The list schedule: each matrix's width from its share of the work, then,
@@ -737,14 +763,16 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
     }
 
     if (select_only) return;
-    if (ncols > kSlots * 4) {
+    if (ncols > 32) {
         // Wider panels than the fused kernel holds: the host-driven loop.
         for (size_t k = 0; k < cnt; ++k)
             expmv_taylor_host(ctx, sh[k], *bs[k], t, ms[k], ss[k], eta_re[k], eta_im[k], results[k], &infos[k]);
         return;
     }
-    const int cpt = ncols <= kSlots ? 1 : ncols <= 2 * kSlots ? 2 : 4;
-    const int lanes = ctas_for(ctx, cplx, cpt);
+    // Layout: 8 slots x 64 rows for up to 8 columns, 16 x 32 for up to 16,
+    // 16 x 32 with two columns per slot for up to 32.
+    const int layout = ncols <= 8 ? 0 : ncols <= 16 ? 1 : 2;
+    const int lanes = taylor(ctx, cplx, layout, nullptr, 0);
 
     std::vector<int> orders(cnt);
     std::vector<double> apps(cnt);
@@ -804,8 +832,7 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
     L.ncols = ncols;
     L.err = ctx.d_err;
     L.progress = bars + cnt;
-    if (cplx) cpt == 1 ? launch_taylor<true, 1>(ctx, L, lanes) : cpt == 2 ? launch_taylor<true, 2>(ctx, L, lanes) : launch_taylor<true, 4>(ctx, L, lanes);
-    else cpt == 1 ? launch_taylor<false, 1>(ctx, L, lanes) : cpt == 2 ? launch_taylor<false, 2>(ctx, L, lanes) : launch_taylor<false, 4>(ctx, L, lanes);
+    taylor(ctx, cplx, layout, &L, lanes);
     std::vector<int> h(2 * cnt);
     TNS_CUDA(cudaMemcpyAsync(h.data(), outs, sizeof(int) * 2 * cnt, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();

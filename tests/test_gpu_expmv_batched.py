@@ -114,3 +114,29 @@ def test_parameter_selection_over_the_whole_frequency_range(ws, orc):
     for a, ms in zip(mats, got):
         assert ms == orc.expmv_params(a, 8, 0.5)
     assert max(s for _, s in got) > 1000
+
+
+def test_zero_entries_in_the_panel(ws, orc):
+    """The reference skips a term whose x is zero; the kernel forms it, which
+    adds +-0 to a sum that is never -0: the same bits."""
+    rng = np.random.default_rng(50)
+    mats = [sweep_matrix(rng, n, 150.0) for n in (40, 97)]
+    panels = []
+    for a in mats:
+        b = panel(rng, a.shape[0], 6)
+        b[rng.uniform(size=b.shape) < 0.5] = 0.0
+        b[:, 2] = 0.0  # a whole zero column
+        panels.append(np.asfortranarray(b))
+    diags = []
+    outs = ws.expmv_batched(mats, panels, 0.5, diags)
+    check_against_oracle(orc, mats, panels, 0.5, outs, diags)
+
+
+def test_non_finite_operator_is_refused(ws):
+    """A non-finite entry makes ||A - mu I||_1 non-finite and the cost
+    uncountable: ArgumentOutOfRangeException in the reference, before any
+    recurrence runs."""
+    a = np.eye(5, dtype=complex)
+    a[1, 3] = np.inf
+    with pytest.raises(OverflowError):
+        ws.expmv_batched([a], [np.ones((5, 2), dtype=complex)], 0.5)
