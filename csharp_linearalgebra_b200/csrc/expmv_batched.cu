@@ -18,9 +18,8 @@
 // and a sum per term; the complex operator's four real sums then
 // (pr - qi, pi + qr), LinearOperators.cs:262-282). The reference skips a term
 // whose x is zero; forming it instead adds +-0 to a sum that is never -0,
-// which changes nothing as long as A is finite -- and an operator with a
-// non-finite entry has a non-finite ||A - mu I||_1, which the parameter
-// search refuses (TNS_E_OUT_OF_RANGE) before any recurrence runs. The epilogue scales
+// which changes nothing as long as A is finite, so the skip is kept (as a
+// compare and a select) only in launches with a non-finite operator. The epilogue scales
 // the sums by t/(s(j+1)) into the next work panel, adds them into F and forms
 // both row sums of moduli in column order (InfinityNorm). Every CTA writes
 // its largest row sums to its slot, the group meets at a barrier, and every
@@ -58,12 +57,18 @@ namespace {
 
 constexpr int kThreadsT = 512;  // threads per CTA: (row, column slot) pairs
 
-// The thread layout, per launch: SLOTS column slots per row (8 for panels of
-// up to 8 columns, else 16), CPT columns per slot (c + SLOTS q), ROWS =
-// 512 / SLOTS rows per chunk of a CTA's row range.
-template <int SLOTS_, int CPT_>
+// The thread layout and the inner loop's form, per launch: SLOTS column slots
+// per row (8 for panels of up to 8 columns, else 16), CPT columns per slot
+// (c + SLOTS q), ROWS = 512 / SLOTS rows per chunk of a CTA's row range.
+// SKIP keeps the reference's skip of a zero x term explicitly (a compare and
+// a select per term). Without it the term is always formed: that adds +-0 to
+// a sum that is never -0, the same bits whenever A is finite; the host takes
+// that form only when every ||A - mu I||_1 of the launch is finite (0 * inf
+// would otherwise differ from a skip).
+template <int SLOTS_, int CPT_, bool SKIP_>
 struct Shape {
     static constexpr int SLOTS = SLOTS_, CPT = CPT_, ROWS = kThreadsT / SLOTS_;
+    static constexpr bool SKIP = SKIP_;
 };
 constexpr int kKT = 32;                    // k per staged tile
 constexpr int kStagesT = 4;                // cp.async ring depth
@@ -347,10 +352,18 @@ __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d,
                     for (int q = 0; q < S::CPT; ++q) {
                         if (!col_ok[q]) continue;
                         const double2 xv = x2[q * S::SLOTS * T::XS + kk];
-                        acc[q][0] = add_rn(acc[q][0], mul_rn(xv.x, av.x));  // pr
-                        acc[q][2] = add_rn(acc[q][2], mul_rn(xv.x, av.y));  // qr
-                        acc[q][1] = add_rn(acc[q][1], mul_rn(xv.y, av.x));  // pi
-                        acc[q][3] = add_rn(acc[q][3], mul_rn(xv.y, av.y));  // qi
+                        if constexpr (S::SKIP) {
+                            const bool nr = xv.x != 0.0, ni = xv.y != 0.0;
+                            acc[q][0] = add_rn(acc[q][0], nr ? mul_rn(xv.x, av.x) : 0.0);  // pr
+                            acc[q][2] = add_rn(acc[q][2], nr ? mul_rn(xv.x, av.y) : 0.0);  // qr
+                            acc[q][1] = add_rn(acc[q][1], ni ? mul_rn(xv.y, av.x) : 0.0);  // pi
+                            acc[q][3] = add_rn(acc[q][3], ni ? mul_rn(xv.y, av.y) : 0.0);  // qi
+                        } else {
+                            acc[q][0] = add_rn(acc[q][0], mul_rn(xv.x, av.x));
+                            acc[q][2] = add_rn(acc[q][2], mul_rn(xv.x, av.y));
+                            acc[q][1] = add_rn(acc[q][1], mul_rn(xv.y, av.x));
+                            acc[q][3] = add_rn(acc[q][3], mul_rn(xv.y, av.y));
+                        }
                     }
                 }
             } else {
@@ -363,7 +376,8 @@ __device__ __forceinline__ void product_chunk(double* smem, const TaylorDesc& d,
                     for (int q = 0; q < S::CPT; ++q) {
                         if (!col_ok[q]) continue;
                         const double xv = x1[q * S::SLOTS * T::XS + kk];
-                        acc[q][0] = add_rn(acc[q][0], mul_rn(xv, av));
+                        if constexpr (S::SKIP) acc[q][0] = add_rn(acc[q][0], xv != 0.0 ? mul_rn(xv, av) : 0.0);
+                        else acc[q][0] = add_rn(acc[q][0], mul_rn(xv, av));
                     }
                 }
             }
@@ -584,13 +598,13 @@ int resident_ctas(Context& ctx) {
     return per_sm * ctx.num_sms;
 }
 
-// One kernel instance per (element type, layout); L null: only the count of
-// resident CTAs.
-template <bool CPLX>
+// One kernel instance per (element type, layout, skip form); L null: only the
+// count of resident CTAs.
+template <bool CPLX, bool SKIP>
 int taylor_dispatch(Context& ctx, int layout, const TaylorLaunch* L, int grid) {
-    using S8 = Shape<8, 1>;
-    using S16 = Shape<16, 1>;
-    using S16x2 = Shape<16, 2>;
+    using S8 = Shape<8, 1, SKIP>;
+    using S16 = Shape<16, 1, SKIP>;
+    using S16x2 = Shape<16, 2, SKIP>;
     if (!L) return layout == 0 ? resident_ctas<CPLX, S8>(ctx) : layout == 1 ? resident_ctas<CPLX, S16>(ctx)
                                                                               : resident_ctas<CPLX, S16x2>(ctx);
     if (layout == 0) launch_taylor<CPLX, S8>(ctx, *L, grid);
@@ -599,8 +613,9 @@ int taylor_dispatch(Context& ctx, int layout, const TaylorLaunch* L, int grid) {
     return grid;
 }
 
-int taylor(Context& ctx, bool cplx, int layout, const TaylorLaunch* L, int grid) {
-    return cplx ? taylor_dispatch<true>(ctx, layout, L, grid) : taylor_dispatch<false>(ctx, layout, L, grid);
+int taylor(Context& ctx, bool cplx, bool skip, int layout, const TaylorLaunch* L, int grid) {
+    if (cplx) return skip ? taylor_dispatch<true, true>(ctx, layout, L, grid) : taylor_dispatch<true, false>(ctx, layout, L, grid);
+    return skip ? taylor_dispatch<false, true>(ctx, layout, L, grid) : taylor_dispatch<false, false>(ctx, layout, L, grid);
 }
 
 // The list schedule: each matrix's width from its share of the work, then,
@@ -612,14 +627,20 @@ struct Sched {
     std::vector<TaylorPlan> plan;
 };
 
-Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int ncols, int lanes) {
+Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int ncols, int lanes, int chunk_rows) {
     const size_t cnt = n.size();
     Sched sc;
     sc.width.assign(cnt, 1);
     sc.rows_per.assign(cnt, 8);
-    // Time model per application: n x (rows per CTA) x ncols element steps
-    // at `rate` per CTA, plus a barrier overhead for groups wider than one.
+    // Time model per application: a chunk of chunk_rows rows costs about the
+    // same however many of its rows are live (each thread's k chain is the
+    // critical path), so a CTA's time is its chunks x n x chunk_rows x ncols
+    // element steps at `rate`, plus a barrier overhead for groups wider than
+    // one. In a batch a CTA takes at least half a chunk of rows (narrower
+    // slices would hold lanes that other matrices could use); a CTA's rows
+    // beyond one chunk come in whole chunks.
     const double rate = 1.0e10, bar_wide = 2.0e-6, bar_one = 0.5e-6;
+    const int min_rows = cnt > 1 ? chunk_rows / 2 : 8;
     std::vector<double> work(cnt);
     double total = 0.0;
     for (size_t k = 0; k < cnt; ++k) {
@@ -631,11 +652,13 @@ Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int n
         const int max_w = std::max(1, std::min(lanes, (n[k] + 7) / 8));
         int w = total > 0.0 ? (int)std::lround(lanes * work[k] / total) : 1;
         w = std::clamp(w, 1, max_w);
-        int rp = round_up((n[k] + w - 1) / w, 8);
+        int rp = std::max(round_up((n[k] + w - 1) / w, 8), std::min(min_rows, round_up(n[k], 8)));
+        if (rp > chunk_rows) rp = round_up(rp, chunk_rows);
         w = (n[k] + rp - 1) / rp;  // no rank without rows
         sc.width[k] = w;
         sc.rows_per[k] = rp;
-        dur[k] = apps[k] * ((double)n[k] * rp * ncols / rate + (w > 1 ? bar_wide : bar_one));
+        const int chunks = (rp + chunk_rows - 1) / chunk_rows;
+        dur[k] = apps[k] * ((double)n[k] * chunks * chunk_rows * ncols / rate + (w > 1 ? bar_wide : bar_one));
     }
     std::vector<int> order(cnt);
     std::iota(order.begin(), order.end(), 0);
@@ -772,7 +795,13 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
     // Layout: 8 slots x 64 rows for up to 8 columns, 16 x 32 for up to 16,
     // 16 x 32 with two columns per slot for up to 32.
     const int layout = ncols <= 8 ? 0 : ncols <= 16 ? 1 : 2;
-    const int lanes = taylor(ctx, cplx, layout, nullptr, 0);
+    // The explicit zero skip only when some operator has a non-finite entry
+    // (its parameters can still be finite: a nilpotent shifted operator has
+    // d(p) = 0 for p >= 2).
+    bool skip = false;
+    for (size_t k = 0; k < cnt; ++k)
+        if (!std::isfinite(one_norm[k])) skip = true;
+    const int lanes = taylor(ctx, cplx, skip, layout, nullptr, 0);
 
     std::vector<int> orders(cnt);
     std::vector<double> apps(cnt);
@@ -780,7 +809,7 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
         orders[k] = as[k]->rows;
         apps[k] = std::max(1.0, (double)ms[k] * ss[k]);
     }
-    Sched sc = schedule(orders, apps, ncols, lanes);
+    Sched sc = schedule(orders, apps, ncols, lanes, layout == 0 ? 64 : 32);
 
     std::vector<DMat> w0(cnt), w1(cnt);
     size_t partial_doubles = 0;
@@ -832,7 +861,7 @@ void expmv_batch(Context& ctx, const std::vector<const DMat*>& as, const std::ve
     L.ncols = ncols;
     L.err = ctx.d_err;
     L.progress = bars + cnt;
-    taylor(ctx, cplx, layout, &L, lanes);
+    taylor(ctx, cplx, skip, layout, &L, lanes);
     std::vector<int> h(2 * cnt);
     TNS_CUDA(cudaMemcpyAsync(h.data(), outs, sizeof(int) * 2 * cnt, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
