@@ -256,23 +256,28 @@ __global__ void abs_power_step_kernel(const __grid_constant__ Batch<ChainDesc> b
 // sum that is never -0.0, which changes nothing, and it keeps 0 * inf out.
 // Complex operator (LinearOperators.cs:262-282): four real sums per column,
 // pr = Ar xr, pi = Ar xi, qr = Ai xr, qi = Ai xi, then (pr - qi, pi + qr).
-// One thread per row covers all t <= TMAX columns, so A is read once per
-// product; x is staged through shared memory.
-template <int TMAX, bool CPLX>
+// TPR threads share a row, thread `sub` covering columns sub, sub + TPR, ...
+// (each (row, column) sum stays one thread's chain); the row's A entries are
+// one load for all of them, so A is read once per product. x is staged
+// through shared memory.
+template <int TMAX, bool CPLX, int TPR>
 __global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant__ Batch<PanelDesc> b) {
+    constexpr int RPB = 128 / TPR;       // rows per block
+    constexpr int CPT = TMAX / TPR;      // columns per thread
     const PanelDesc& d = batch_item(b, blockIdx.y);
     const int n = d.n, t = d.t;
-    if ((int)(blockIdx.x * blockDim.x) >= n) return;  // whole block past this item
-    constexpr int CH = 64;                              // rows of x staged per chunk
+    if ((int)(blockIdx.x * RPB) >= n) return;  // whole block past this item
+    constexpr int CH = 64;                     // rows of x staged per chunk
     constexpr int ES = CPLX ? 2 : 1;
     __shared__ double sx[CH * TMAX * ES];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * RPB + threadIdx.x / TPR;
+    const int sub = threadIdx.x % TPR;
     const bool row_ok = i < n;
-    double acc[TMAX][CPLX ? 4 : 1];
+    double acc[CPT][CPLX ? 4 : 1];
 #pragma unroll
-    for (int c = 0; c < TMAX; ++c)
+    for (int q = 0; q < CPT; ++q)
 #pragma unroll
-        for (int q = 0; q < (CPLX ? 4 : 1); ++q) acc[c][q] = 0.0;
+        for (int z = 0; z < (CPLX ? 4 : 1); ++z) acc[q][z] = 0.0;
     for (int j0 = 0; j0 < n; j0 += CH) {
         const int len = min(CH, n - j0);
         __syncthreads();
@@ -296,27 +301,22 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant_
             for (int u = 0; u < U; ++u) {
                 if (jb + u >= len) break;
                 const int jj = jb + u;
-                if constexpr (!CPLX) {
 #pragma unroll
-                    for (int c = 0; c < TMAX; ++c) {
-                        if (c < t) {
-                            double s = sx[c * CH + jj];
-                            double term = s != 0.0 ? mul_rn(s, av[u]) : 0.0;
-                            acc[c][0] = add_rn(acc[c][0], term);
-                        }
-                    }
-                } else {
-                    const double2 aij = av[u];
-#pragma unroll
-                    for (int c = 0; c < TMAX; ++c) {
-                        if (c < t) {
-                            double sr = sx[(c * CH + jj) * 2], si = sx[(c * CH + jj) * 2 + 1];
-                            bool nr = sr != 0.0, ni = si != 0.0;
-                            acc[c][0] = add_rn(acc[c][0], nr ? mul_rn(sr, aij.x) : 0.0);  // pr
-                            acc[c][2] = add_rn(acc[c][2], nr ? mul_rn(sr, aij.y) : 0.0);  // qr
-                            acc[c][1] = add_rn(acc[c][1], ni ? mul_rn(si, aij.x) : 0.0);  // pi
-                            acc[c][3] = add_rn(acc[c][3], ni ? mul_rn(si, aij.y) : 0.0);  // qi
-                        }
+                for (int q = 0; q < CPT; ++q) {
+                    const int c = sub + q * TPR;
+                    if (c >= t) continue;
+                    if constexpr (!CPLX) {
+                        double sv = sx[c * CH + jj];
+                        double term = sv != 0.0 ? mul_rn(sv, av[u]) : 0.0;
+                        acc[q][0] = add_rn(acc[q][0], term);
+                    } else {
+                        const double2 aij = av[u];
+                        double sr = sx[(c * CH + jj) * 2], si = sx[(c * CH + jj) * 2 + 1];
+                        bool nr = sr != 0.0, ni = si != 0.0;
+                        acc[q][0] = add_rn(acc[q][0], nr ? mul_rn(sr, aij.x) : 0.0);  // pr
+                        acc[q][2] = add_rn(acc[q][2], nr ? mul_rn(sr, aij.y) : 0.0);  // qr
+                        acc[q][1] = add_rn(acc[q][1], ni ? mul_rn(si, aij.x) : 0.0);  // pi
+                        acc[q][3] = add_rn(acc[q][3], ni ? mul_rn(si, aij.y) : 0.0);  // qi
                     }
                 }
             }
@@ -324,17 +324,17 @@ __global__ void __launch_bounds__(128) panel_apply_kernel(const __grid_constant_
     }
     if (!row_ok) return;
 #pragma unroll
-    for (int c = 0; c < TMAX; ++c) {
+    for (int q = 0; q < CPT; ++q) {
+        const int c = sub + q * TPR;
         if (c >= t) continue;
         if (!CPLX) {
-            d.y[(size_t)c * d.ldy + i] = acc[c][0];
+            d.y[(size_t)c * d.ldy + i] = acc[q][0];
         } else {
             reinterpret_cast<double2*>(d.y)[(size_t)c * d.ldy + i] =
-                make_double2(sub_rn(acc[c][0], acc[c][3]), add_rn(acc[c][1], acc[c][2]));
+                make_double2(sub_rn(acc[q][0], acc[q][3]), add_rn(acc[q][1], acc[q][2]));
         }
     }
 }
-
 
 // Y := A^T X (real) or A^H X (complex operator: pr = Ar^T xr, pi = Ar^T xi,
 // qr = Ai^T xr, qi = Ai^T xi, then (pr + qi, pi - qr)), PanelProduct.ApplyTranspose
@@ -450,8 +450,11 @@ void launch_panel(Context& ctx, std::vector<PanelDesc>& v, bool adjoint) {
     if (nmax == 0) return;
     Batch<PanelDesc> b = make_batch(ctx, v);
     if (!adjoint) {
-        dim3 grid((nmax + 127) / 128, b.count);
-        panel_apply_kernel<TMAX, CPLX><<<grid, 128, 0, ctx.stream>>>(b);
+        // Narrow panels (the estimator's two or four columns): one thread per
+        // (row, column), twice or four times the threads of one per row.
+        constexpr int TPR = TMAX <= 4 ? TMAX : 1;
+        dim3 grid((nmax + 128 / TPR - 1) / (128 / TPR), b.count);
+        panel_apply_kernel<TMAX, CPLX, TPR><<<grid, 128, 0, ctx.stream>>>(b);
     } else {
         long long threads = (long long)nmax * 16;
         dim3 grid((unsigned)((threads + 255) / 256), b.count);

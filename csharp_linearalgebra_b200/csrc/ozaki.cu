@@ -267,11 +267,15 @@ struct RowDigits {
         const int h = shift >> 1;
         const double f1 = pow2(h), f2 = pow2(shift - h);
         const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
+        // All the entries' loads first, so that they are in flight together.
+        double v[2 * NP];
+#pragma unroll
+        for (int e = 0; e < 2 * NP; ++e) v[e] = load(e);
 #pragma unroll
         for (int e = 0; e < NP; ++e) {
             float d0[ND], d1[ND];
-            digits_of<ND>(load(2 * e), f1, f2, d0);
-            digits_of<ND>(load(2 * e + 1), f1, f2, d1);
+            digits_of<ND>(v[2 * e], f1, f2, d0);
+            digits_of<ND>(v[2 * e + 1], f1, f2, d1);
 #pragma unroll
             for (int i = 0; i < ND; ++i) c[i][e] = __fadd2_rn(make_float2(d0[i], d1[i]), neg_magic);
         }
@@ -688,13 +692,15 @@ __global__ void __launch_bounds__(256) crt_kernel(const __grid_constant__ Batch<
         const int sc = sc4[u];
         double a1 = 0.0, a2 = 0.0, a3 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
         for (int q = 0; q < nm; ++q) {
+            // Bytes to doubles exactly without a conversion instruction: the
+            // byte as the low word of 2^52 + byte, minus 2^52.
             double ur, ui = 0.0;
             if (CPLX) {
-                const uint16_t v = *reinterpret_cast<const uint16_t*>(&su[q][lane][2 * jj]);
-                ur = (double)(v & 0xFF);
-                ui = (double)(v >> 8);
+                const uint32_t v = *reinterpret_cast<const uint16_t*>(&su[q][lane][2 * jj]);
+                ur = __hiloint2double(0x43300000, (int)(v & 0xFF)) - 4503599627370496.0;
+                ui = __hiloint2double(0x43300000, (int)(v >> 8)) - 4503599627370496.0;
             } else {
-                ur = (double)su[q][lane][jj];
+                ur = __hiloint2double(0x43300000, (int)su[q][lane][jj]) - 4503599627370496.0;
             }
             a1 = fma(ur, cp.d1[q], a1);
             a2 = fma(ur, cp.d2[q], a2);
