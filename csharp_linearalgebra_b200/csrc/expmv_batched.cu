@@ -296,7 +296,7 @@ __device__ __forceinline__ void stage_tile(double* buf, const TaylorDesc& d, con
             if (r < rows) cp16(sA + (k * R + r) * 2, d.a + ((size_t)(k0 + k) * d.lda + r0 + r) * 2);
         }
         for (int e = tid; e < ncols * kKT; e += kThreadsT) {
-            const int col = e >> 5, k = e & 31;
+            const int col = e / kKT, k = e % kKT;
             cp16(sX + (col * T::XS + k) * 2, x + ((size_t)col * d.ldp + k0 + k) * 2);
         }
     } else {
@@ -305,7 +305,7 @@ __device__ __forceinline__ void stage_tile(double* buf, const TaylorDesc& d, con
             if (rp < rows) cp16(sA + k * R + rp, d.a + (size_t)(k0 + k) * d.lda + r0 + rp);
         }
         for (int e = tid; e < ncols * (kKT / 2); e += kThreadsT) {
-            const int col = e >> 4, kp = (e & 15) * 2;
+            const int col = e / (kKT / 2), kp = (e % (kKT / 2)) * 2;
             cp16(sX + col * T::XS + kp, x + (size_t)col * d.ldp + k0 + kp);
         }
     }
@@ -632,15 +632,12 @@ Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int n
     Sched sc;
     sc.width.assign(cnt, 1);
     sc.rows_per.assign(cnt, 8);
-    // Time model per application: a chunk of chunk_rows rows costs about the
-    // same however many of its rows are live (each thread's k chain is the
-    // critical path), so a CTA's time is its chunks x n x chunk_rows x ncols
-    // element steps at `rate`, plus a barrier overhead for groups wider than
-    // one. In a batch a CTA takes at least half a chunk of rows (narrower
-    // slices would hold lanes that other matrices could use); a CTA's rows
-    // beyond one chunk come in whole chunks.
+    // Time model per application: n x (rows per CTA) x ncols element steps
+    // at `rate` per CTA, plus a barrier overhead for groups wider than one.
+    // (Measured on the sweep: widths in proportion to the work share beat
+    // rounding the rows per CTA up to whole chunks.)
     const double rate = 1.0e10, bar_wide = 2.0e-6, bar_one = 0.5e-6;
-    const int min_rows = cnt > 1 ? chunk_rows / 2 : 8;
+    (void)chunk_rows;
     std::vector<double> work(cnt);
     double total = 0.0;
     for (size_t k = 0; k < cnt; ++k) {
@@ -652,13 +649,11 @@ Sched schedule(const std::vector<int>& n, const std::vector<double>& apps, int n
         const int max_w = std::max(1, std::min(lanes, (n[k] + 7) / 8));
         int w = total > 0.0 ? (int)std::lround(lanes * work[k] / total) : 1;
         w = std::clamp(w, 1, max_w);
-        int rp = std::max(round_up((n[k] + w - 1) / w, 8), std::min(min_rows, round_up(n[k], 8)));
-        if (rp > chunk_rows) rp = round_up(rp, chunk_rows);
+        int rp = round_up((n[k] + w - 1) / w, 8);
         w = (n[k] + rp - 1) / rp;  // no rank without rows
         sc.width[k] = w;
         sc.rows_per[k] = rp;
-        const int chunks = (rp + chunk_rows - 1) / chunk_rows;
-        dur[k] = apps[k] * ((double)n[k] * chunks * chunk_rows * ncols / rate + (w > 1 ? bar_wide : bar_one));
+        dur[k] = apps[k] * ((double)n[k] * rp * ncols / rate + (w > 1 ? bar_wide : bar_one));
     }
     std::vector<int> order(cnt);
     std::iota(order.begin(), order.end(), 0);
