@@ -733,6 +733,11 @@ def config_precision(args, ws, oracle, res, gpu_ms, cpu_s, peak8):
     v, _ = np.linalg.qr(rng.standard_normal((n, n)))
     b = np.asfortranarray(rng.standard_normal((n, nrhs)))
     three = {"kappa": {}}
+    # one untimed call of each route first (module loading, memory pool)
+    a0 = np.asfortranarray((u * np.logspace(0.0, -2.0, n)) @ v.T)
+    ws.solve_mixed(a0, b)
+    ws.factor_lu(a0).solve(b)
+    del a0
     for kappa in (1e2, 1e6, 1e10):
         sig = np.logspace(0.0, -math.log10(kappa), n)
         a = np.asfortranarray((u * sig) @ v.T)
@@ -751,6 +756,8 @@ def config_precision(args, ws, oracle, res, gpu_ms, cpu_s, peak8):
 
         entry = {"mixed_ms": ms_mx, "fp64_ms": ms_64, "moduli": info["moduli"],
                  "factorizations": info["factorizations"], "refinement_steps": info["iterations"],
+                 "route": "partial pivoting" if info["pivoting"] else "butterfly transforms, no pivoting",
+                 "rcond_estimate": info["rcond"],
                  "backward_error_mixed": backward(x), "backward_error_fp64": backward(x64),
                  "rel_diff_mixed_vs_fp64": float(np.linalg.norm(x - x64) / np.linalg.norm(x64))}
         if kappa == 1e2:

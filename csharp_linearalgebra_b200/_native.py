@@ -46,7 +46,7 @@ class ExpmvInfo(C.Structure):
 
 class MixedInfo(C.Structure):
     _fields_ = [("moduli", C.c_int), ("factorizations", C.c_int), ("iterations", C.c_int),
-                ("backward_error", C.c_double), ("rcond", C.c_double)]
+                ("backward_error", C.c_double), ("rcond", C.c_double), ("pivoting", C.c_int)]
 
 
 class Stats(C.Structure):

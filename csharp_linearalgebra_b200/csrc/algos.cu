@@ -81,6 +81,28 @@ struct LuInverseProbe : Probe<TE> {
     }
 };
 
+// An operator given as an in-place device solve on a panel of `rows` rows
+// (the probe's n rows, zeros below).
+template <class TE>
+struct SolveProbe : Probe<TE> {
+    Context& ctx;
+    int n;
+    const std::function<void(DMat&, int, bool)>& solve;
+    DMat panel;
+    SolveProbe(Context& c, int n_, int rows, bool cplx, const std::function<void(DMat&, int, bool)>& s, int t)
+        : ctx(c), n(n_), solve(s), panel(c, rows, t, cplx, "an estimator probe panel") {}
+    void apply(const typename TE::T* x, typename TE::T* y, int t, bool adjoint) override {
+        const size_t esz = sizeof(double) * TE::kDoubles;
+        panel.zero();
+        TNS_CUDA(cudaMemcpy2DAsync(panel.p, (size_t)panel.ld() * esz, x, (size_t)n * esz, (size_t)n * esz, t,
+                                   cudaMemcpyHostToDevice, ctx.stream));
+        solve(panel, t, adjoint);
+        TNS_CUDA(cudaMemcpy2DAsync(y, (size_t)n * esz, panel.p, (size_t)panel.ld() * esz, (size_t)n * esz, t,
+                                   cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+    }
+};
+
 // A caller's operator (IAdjointOperator<T>, src/Tensile/LinearOperators.cs:37-75):
 // the probe panel goes to the device, the caller's apply or adjoint callback
 // writes the result there on the context's stream, and it comes back.
@@ -151,6 +173,18 @@ NormestResult normest_power(Context& ctx, const DMat& a, int power, int t, int i
         return estimate<CplxE>(op, n, t, itmax, seed);
     }
     PowerProbe<RealE> op(ctx, a, power, tt);
+    return estimate<RealE>(op, n, t, itmax, seed);
+}
+
+NormestResult normest_solve(Context& ctx, int n, int rows, bool cplx,
+                            const std::function<void(DMat&, int, bool)>& solve, int t, int itmax, int seed) {
+    if (n == 0) return {};
+    int tt = std::clamp(t, 1, n);
+    if (cplx) {
+        SolveProbe<CplxE> op(ctx, n, rows, true, solve, tt);
+        return estimate<CplxE>(op, n, t, itmax, seed);
+    }
+    SolveProbe<RealE> op(ctx, n, rows, false, solve, tt);
     return estimate<RealE>(op, n, t, itmax, seed);
 }
 

@@ -469,7 +469,7 @@ int gesv_mixed_entry(tns_context* c, bool cplx, int n, int nrhs, const double* a
         require(max_iter >= 0, TNS_E_OUT_OF_RANGE, "max_iter must not be negative");
         tns_mixed_info local{};
         tns_mixed_info* inf = info ? info : &local;
-        *inf = tns_mixed_info{0, 0, 0, 0.0, 0.0};
+        *inf = tns_mixed_info{0, 0, 0, 0.0, 0.0, 0};
         if (n == 0 || nrhs == 0) return;
         DMat A = upload(ctx, a, n, n, lda, cplx, false, "the matrix");
         DMat B = upload(ctx, b, n, nrhs, ldb, cplx, false, "the right-hand sides");
@@ -478,7 +478,7 @@ int gesv_mixed_entry(tns_context* c, bool cplx, int n, int nrhs, const double* a
         tns::gesv_mixed(ctx, A, B, X, moduli, max_iter, mi);
         tns::copy_out(ctx, X, x, ldx, false);
         ctx.sync();
-        *inf = tns_mixed_info{mi.moduli, mi.factorizations, mi.iterations, mi.backward_error, mi.rcond};
+        *inf = tns_mixed_info{mi.moduli, mi.factorizations, mi.iterations, mi.backward_error, mi.rcond, mi.pivoting};
     });
 }
 

@@ -19,6 +19,7 @@ enum DeviceError : int {
     kDevTimeoutEmpty = 2,  // producer waited for a stage that was never released
     kDevTimeoutDrain = 3,  // producer's final wait for its own copies
     kDevTimeoutSelfTest = 5,  // tns_selftest_wait: a barrier nothing arrives on
+    kDevTimeoutChain = 6,     // a chained triangular solve waited for a block that never completed
 };
 
 __device__ __forceinline__ unsigned long long global_timer_ns() {

@@ -507,12 +507,29 @@ __global__ void trsm_kernel(const __grid_constant__ Batch<TrsmDesc> bt) {
     extern __shared__ double sT[];  // effective operator, w x w, ld w: op(i, p)
     const int w = d.w;
     if (d.ncols <= 0 || (int)(blockIdx.x * (blockDim.x >> 5)) >= d.ncols) return;  // nothing for this block
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-        int i = e % w, p = e / w;
-        int si = d.conj ? p : i, sp = d.conj ? i : p;
-        const double* src = d.t + ((size_t)sp * d.ldt + si) * ES;
-        sT[(size_t)e * ES] = src[0];
-        if (CPLX) sT[(size_t)e * ES + 1] = d.conj ? -src[1] : src[1];
+    // Eight loads in flight per thread before their stores.
+    for (int e0 = threadIdx.x; e0 < w * w; e0 += 8 * blockDim.x) {
+        double re[8], im[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            re[u] = im[u] = 0.0;
+            if (e < w * w) {
+                const int i = e % w, p = e / w;
+                const int si = d.conj ? p : i, sp = d.conj ? i : p;
+                const double* src = d.t + ((size_t)sp * d.ldt + si) * ES;
+                re[u] = src[0];
+                if (CPLX) im[u] = src[1];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < w * w) {
+                sT[(size_t)e * ES] = re[u];
+                if (CPLX) sT[(size_t)e * ES + 1] = d.conj ? -im[u] : im[u];
+            }
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -1435,7 +1452,7 @@ void getrs_free_order(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, i
         std::vector<GemmProblem> g{p};
         gemm_grouped(ctx, g, cplx);
     };
-    if (!adjoint) {
+    if (!adjoint && d_piv) {
         std::vector<LaswpDesc> sw{LaswpDesc{b.p, ldb, 0, nrhs, d_piv, 0, n, 0}};
         launch_laswp(ctx, cplx, sw);
     }
@@ -1455,7 +1472,7 @@ void getrs_free_order(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, i
         launch_trsm(ctx, cplx, 1, d);
         update(G + ((size_t)k0 * ldg) * es, b.p + (size_t)k0 * es, b.p, k0, w);
     }
-    if (adjoint) {
+    if (adjoint && d_piv) {
         std::vector<LaswpDesc> sw{LaswpDesc{b.p, ldb, 0, nrhs, d_piv, 0, n, 1}};
         launch_laswp(ctx, cplx, sw);
     }
@@ -1580,6 +1597,51 @@ std::vector<double> col_absmax(Context& ctx, const DMat& x) {
 
 constexpr int kMixedOuter = 512;  // depth of the split-precision trailing updates
 
+// Below a factored panel of w columns at column j: U12 := L11^-1 A12 (64-row
+// unit-lower blocks, DMMA updates below each), then A22 -= L21 U12 on the
+// split-precision product with `moduli` moduli.
+void mixed_trailing(Context& ctx, DMat& a, int j, int w, int moduli) {
+    const int n = a.rows, ld = a.ld();
+    const bool cplx = a.cplx;
+    const int es = cplx ? 2 : 1;
+    const int rest = n - j - w;
+    // U12 := L11^-1 A12: 64-row unit-lower blocks, DMMA updates below each.
+    for (int b0 = 0; b0 < w; b0 += 64) {
+        const int bw = std::min(64, w - b0);
+        std::vector<TrsmDesc> t{TrsmDesc{a.at(j + b0, j + b0), ld, a.at(j + b0, j + w), ld, bw, rest, 1, 1, 0}};
+        launch_trsm(ctx, cplx, 1, t);
+        if (b0 + bw < w) {
+            GemmProblem p{};
+            p.A = a.at(j + b0 + bw, j + b0);
+            p.B = a.at(j + b0, j + w);
+            p.C = a.at(j + b0 + bw, j + w);
+            p.lda = p.ldb = p.ldc = ld;
+            p.M = round_up(w - b0 - bw, 2);
+            p.N = round_up(rest, 2);
+            p.K = round_up(bw, 16);
+            p.alpha_re = -1.0;
+            p.beta_re = 1.0;
+            p.work = (long long)(w - b0 - bw) * rest * bw;
+            std::vector<GemmProblem> g{p};
+            gemm_grouped(ctx, g, cplx);
+        }
+    }
+    // A22 -= L21 U12 on the split-precision product: C += (-L21) U12.
+    DMat negl(ctx, rest, w, cplx, "the negated L21 block of a mixed-precision factorization");
+    {
+        const size_t total = (size_t)rest * es * w;
+        const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)ctx.num_sms * 16);
+        scaled_block_copy_kernel<<<grid, 256, 0, ctx.stream>>>(negl.p, negl.ld(), a.at(j + w, j), ld, rest, w,
+                                                              -1.0, es);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    }
+    DMat u12 = block_view(a, j, j + w, w, rest);
+    DMat a22 = block_view(a, j + w, j + w, rest, rest);
+    std::vector<SplitProduct> sp{SplitProduct{&negl, &u12, &a22, 1.0}};
+    gemm_split_batch(ctx, sp, moduli);
+}
+
 }  // namespace
 
 void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli) {
@@ -1605,42 +1667,7 @@ void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli) {
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches++;
         if (j + w >= n) break;
-        const int rest = n - j - w;
-        // U12 := L11^-1 A12: 64-row unit-lower blocks, DMMA updates below each.
-        for (int b0 = 0; b0 < w; b0 += 64) {
-            const int bw = std::min(64, w - b0);
-            std::vector<TrsmDesc> t{TrsmDesc{a.at(j + b0, j + b0), ld, a.at(j + b0, j + w), ld, bw, rest, 1, 1, 0}};
-            launch_trsm(ctx, cplx, 1, t);
-            if (b0 + bw < w) {
-                GemmProblem p{};
-                p.A = a.at(j + b0 + bw, j + b0);
-                p.B = a.at(j + b0, j + w);
-                p.C = a.at(j + b0 + bw, j + w);
-                p.lda = p.ldb = p.ldc = ld;
-                p.M = round_up(w - b0 - bw, 2);
-                p.N = round_up(rest, 2);
-                p.K = round_up(bw, 16);
-                p.alpha_re = -1.0;
-                p.beta_re = 1.0;
-                p.work = (long long)(w - b0 - bw) * rest * bw;
-                std::vector<GemmProblem> g{p};
-                gemm_grouped(ctx, g, cplx);
-            }
-        }
-        // A22 -= L21 U12 on the split-precision product: C += (-L21) U12.
-        DMat negl(ctx, rest, w, cplx, "the negated L21 block of a mixed-precision factorization");
-        {
-            const size_t total = (size_t)rest * es * w;
-            const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)ctx.num_sms * 16);
-            scaled_block_copy_kernel<<<grid, 256, 0, ctx.stream>>>(negl.p, negl.ld(), a.at(j + w, j), ld, rest, w,
-                                                                  -1.0, es);
-            TNS_CUDA(cudaGetLastError());
-            ctx.kernel_launches++;
-        }
-        DMat u12 = block_view(a, j, j + w, w, rest);
-        DMat a22 = block_view(a, j + w, j + w, rest, rest);
-        std::vector<SplitProduct> sp{SplitProduct{&negl, &u12, &a22, 1.0}};
-        gemm_split_batch(ctx, sp, moduli);
+        mixed_trailing(ctx, a, j, w, moduli);
     }
     std::vector<int> flags(blocks);
     TNS_CUDA(cudaMemcpyAsync(flags.data(), sing.p, sizeof(int) * blocks, cudaMemcpyDeviceToHost, ctx.stream));
@@ -1651,10 +1678,15 @@ void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli) {
                                      std::to_string(q * kMixedOuter + flags[q]) + ".");
 }
 
-void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter, MixedInfo& info) {
+namespace {
+
+// The precision form with partial pivoting (the fallback of gesv_mixed).
+void gesv_mixed_pivoted(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter,
+                        MixedInfo& info) {
     const int n = a.rows, nrhs = b.cols;
     const bool cplx = a.cplx;
     info = MixedInfo{};
+    info.pivoting = 1;
     DMat f(ctx, n, n, cplx, "the low-precision factors");
     DBuf piv(ctx, sizeof(int) * (size_t)std::max(1, n));
     auto factor = [&](int m) {
@@ -1673,7 +1705,11 @@ void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli,
         const int depth = cplx ? 2 * kMixedOuter : kMixedOuter;
         int m = info.moduli;
         while (m < 22 && split_integer_bits(m, depth) < need) ++m;
-        if (m > info.moduli) factor(m);
+        if (m > info.moduli) {
+            factor(m);
+            const NormestResult again = normest_lu_inverse(ctx, f, piv.as<int>(), 2, 5, 20260915, true);
+            info.rcond = (anorm1 > 0.0 && again.value > 0.0) ? 1.0 / (anorm1 * again.value) : 0.0;
+        }
     }
     x = DMat(ctx, n, nrhs, cplx, "the solution");
     copy_dmat(ctx, x, b);
@@ -1702,6 +1738,675 @@ void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli,
         ew_batch(ctx, add);
         info.iterations++;
     }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The precision form without row interchanges. Random butterfly transforms
+// (Parker, 1995; Baboulin, Dongarra, Herrmann and Tomov, 2013) make Gaussian
+// elimination without pivoting stable with high probability: A x = b becomes
+// (T A S) y = T b, x = S y, with T = T2 T1 and S = S1 S2 recursive
+// butterflies of depth 2. A butterfly of order 2h is
+// B = (1/sqrt 2) [[R0, R1], [R0, -R1]], R0 and R1 diagonal with entries
+// exp(r / 10), r uniform in [-1/2, 1/2]; level 1 is one butterfly of the
+// whole order N, level 2 two of order N/2. T_i = B_i^T act on rows, S_i = B_i
+// on columns. The order is padded to N = round_up(n, 4) with an identity
+// block. Without pivot searches the panels are a 64 x 64 diagonal block, a
+// right triangular solve and DMMA updates, so nothing serialises on one SM
+// per column; the refinement's residuals use A itself in FP64.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kInvSqrt2 = 0.70710678118654752440;
+constexpr int kNopivBlock = 64;
+constexpr int kNopivLd = kNopivBlock + 1;  // shared-memory column stride of the 64 x 64 blocks
+
+template <bool CPLX>
+__device__ __forceinline__ Z load_el(const double* p) {
+    return CPLX ? Z{p[0], p[1]} : Z{p[0], 0.0};
+}
+template <bool CPLX>
+__device__ __forceinline__ void store_el(double* p, Z v) {
+    p[0] = v.re;
+    if (CPLX) p[1] = v.im;
+}
+// acc - x y
+template <bool CPLX>
+__device__ __forceinline__ Z sub_prod(Z acc, Z x, Z y) {
+    if (!CPLX) return Z{sub_rn(acc.re, mul_rn(x.re, y.re)), 0.0};
+    const Z p = zmul(x, y);
+    return Z{sub_rn(acc.re, p.re), sub_rn(acc.im, p.im)};
+}
+template <bool CPLX>
+__device__ __forceinline__ Z div_el(Z x, Z y) {
+    return CPLX ? zdiv(x, y) : Z{__ddiv_rn(x.re, y.re), 0.0};
+}
+
+// One butterfly level on the rows of an N x cols panel (ld elements): the
+// pairs (i, i + h) of every segment of 2h rows. kind 0: B^T,
+// (u, v) -> (d_i (u + v), d_{i+h} (u - v)) / sqrt 2; kind 1: B,
+// (u, v) -> (d_i u + d_{i+h} v, d_i u - d_{i+h} v) / sqrt 2.
+template <bool CPLX>
+__global__ void butterfly_rows_kernel(double* a, int ld, int n, int cols, int h, const double* d, int kind) {
+    constexpr int ES = CPLX ? 2 : 1;
+    const int half = n / 2;
+    const size_t total = (size_t)half * cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(e % half), c = (int)(e / half);
+        const int i = (q / h) * 2 * h + q % h, j = i + h;
+        const double di = d[i], dj = d[j];
+        double* col = a + (size_t)c * ld * ES;
+#pragma unroll
+        for (int part = 0; part < ES; ++part) {
+            const double u = col[(size_t)i * ES + part], v = col[(size_t)j * ES + part];
+            double x, y;
+            if (kind == 0) {
+                x = mul_rn(mul_rn(di, add_rn(u, v)), kInvSqrt2);
+                y = mul_rn(mul_rn(dj, sub_rn(u, v)), kInvSqrt2);
+            } else {
+                const double p = mul_rn(di, u), r = mul_rn(dj, v);
+                x = mul_rn(add_rn(p, r), kInvSqrt2);
+                y = mul_rn(sub_rn(p, r), kInvSqrt2);
+            }
+            col[(size_t)i * ES + part] = x;
+            col[(size_t)j * ES + part] = y;
+        }
+    }
+}
+
+// One butterfly level on the columns of a rows x N matrix: A := A B, the
+// pairs (c, c + h) of every segment of 2h columns,
+// (u, v) -> (d_c (u + v), d_{c+h} (u - v)) / sqrt 2 along each row.
+template <bool CPLX>
+__global__ void butterfly_cols_kernel(double* a, int ld, int rows, int n, int h, const double* d) {
+    constexpr int ES = CPLX ? 2 : 1;
+    const size_t total = (size_t)rows * (n / 2);
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e % rows), q = (int)(e / rows);
+        const int c = (q / h) * 2 * h + q % h, c2 = c + h;
+        const double dc = d[c], dc2 = d[c2];
+        double* pu = a + ((size_t)c * ld + r) * ES;
+        double* pv = a + ((size_t)c2 * ld + r) * ES;
+#pragma unroll
+        for (int part = 0; part < ES; ++part) {
+            const double u = pu[part], v = pv[part];
+            pu[part] = mul_rn(mul_rn(dc, add_rn(u, v)), kInvSqrt2);
+            pv[part] = mul_rn(mul_rn(dc2, sub_rn(u, v)), kInvSqrt2);
+        }
+    }
+}
+
+__global__ void unit_diagonal_kernel(double* a, int ld, int from, int to, int es) {
+    const int i = from + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < to) a[((size_t)i * ld + i) * es] = 1.0;
+}
+
+// s[c * kNopivLd + r] := the rows x cols block at src (leading dimension ld),
+// upper: zeros below the diagonal. Eight loads in flight per thread before
+// their stores.
+template <bool CPLX>
+__device__ __forceinline__ void stage_block(Z* s, const double* src, int ld, int rows, int cols, bool upper) {
+    constexpr int ES = CPLX ? 2 : 1;
+    const int total = rows * cols;
+    for (int e0 = threadIdx.x; e0 < total; e0 += 8 * blockDim.x) {
+        Z v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            v[u] = Z{0.0, 0.0};
+            if (e < total) {
+                const int r = e % rows, c = e / rows;
+                if (!upper || r <= c) v[u] = load_el<CPLX>(src + ((size_t)c * ld + r) * ES);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < total) s[(e / rows) * kNopivLd + e % rows] = v[u];
+        }
+    }
+}
+
+// The w x w diagonal block (w <= 64) factored in place without pivoting,
+// L unit lower and U upper; an exactly zero pivot records its column (atomic
+// minimum into flag) and the factorization goes on in inf/NaN.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) lu_nopiv_diag_kernel(double* a, int ld, int w, int col0, int* flag) {
+    constexpr int ES = CPLX ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char nopiv_smem[];
+    Z* s = reinterpret_cast<Z*>(nopiv_smem);  // s[c * kNopivLd + r]
+    stage_block<CPLX>(s, a, ld, w, w, false);
+    __syncthreads();
+    for (int k = 0; k < w; ++k) {
+        const Z piv = s[k * kNopivLd + k];
+        if (threadIdx.x == 0 && piv.re == 0.0 && piv.im == 0.0) atomicMin(flag, col0 + k);
+        for (int r = k + 1 + threadIdx.x; r < w; r += blockDim.x)
+            s[k * kNopivLd + r] = div_el<CPLX>(s[k * kNopivLd + r], piv);
+        __syncthreads();
+        const int m = w - k - 1;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            const int r = k + 1 + e % m, c = k + 1 + e / m;
+            s[c * kNopivLd + r] = sub_prod<CPLX>(s[c * kNopivLd + r], s[k * kNopivLd + r], s[c * kNopivLd + k]);
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        const int r = e % w, c = e / w;
+        store_el<CPLX>(a + ((size_t)c * ld + r) * ES, s[c * kNopivLd + r]);
+    }
+}
+
+// X := X U^-1 for the rows x w block X (w <= 64) and the w x w upper factor
+// U (staged in shared memory): one warp per row, lane l holding columns l and
+// l + 32; step k divides x_k by u_kk in its lane, broadcasts it, and the lanes
+// of the columns beyond k subtract x_k u_kc.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) trsm_right_upper_kernel(const double* u, int ldu, double* x, int ldx,
+                                                             int rows, int w) {
+    constexpr int ES = CPLX ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char nopiv_smem[];
+    Z* su = reinterpret_cast<Z*>(nopiv_smem);  // su[c * kNopivLd + r]
+    stage_block<CPLX>(su, u, ldu, w, w, true);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < rows; row += gridDim.x * warps) {
+        Z v[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int c = lane + 32 * q;
+            v[q] = c < w ? load_el<CPLX>(x + ((size_t)c * ldx + row) * ES) : Z{0.0, 0.0};
+        }
+        for (int k = 0; k < w; ++k) {
+            const int h = k >> 5, src = k & 31;
+            if (lane == src) v[h] = div_el<CPLX>(v[h], su[k * kNopivLd + k]);
+            const Z xk{__shfl_sync(0xffffffffu, v[h].re, src), CPLX ? __shfl_sync(0xffffffffu, v[h].im, src) : 0.0};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int c = lane + 32 * q;
+                if (c > k && c < w) v[q] = sub_prod<CPLX>(v[q], xk, su[c * kNopivLd + k]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int c = lane + 32 * q;
+            if (c < w) store_el<CPLX>(x + ((size_t)c * ldx + row) * ES, v[q]);
+        }
+    }
+}
+
+constexpr int kNopivDiagSmem = kNopivBlock * kNopivLd * 16;
+constexpr int kNopivTrsmSmem = kNopivBlock * kNopivLd * 16;
+
+template <bool CPLX>
+void configure_nopiv_kernels() {
+    static bool done[64] = {};
+    int dev = 0;
+    TNS_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    TNS_CUDA(cudaFuncSetAttribute(lu_nopiv_diag_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kNopivDiagSmem));
+    TNS_CUDA(cudaFuncSetAttribute(trsm_right_upper_kernel<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kNopivTrsmSmem));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+// Inverses of the 64 x 64 diagonal blocks of packed factors without
+// interchanges (n x n, unit lower L and upper U): one CTA per block, thread j
+// of the first 64 computing column j of L_bb^-1 by forward substitution, of
+// the next 64 column j of U_bb^-1 by back substitution. A partial last block
+// is completed by the identity. inv holds nb blocks of L^-1, then nb of U^-1,
+// each column-major with leading dimension 64.
+template <bool CPLX>
+__global__ void __launch_bounds__(128) diag_block_inverse_kernel(const double* f, int ld, int n, int nb,
+                                                                double* inv) {
+    constexpr int ES = CPLX ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char inv_smem[];
+    Z* sd = reinterpret_cast<Z*>(inv_smem);  // the block, sd[c * kNopivLd + r]
+    Z* sl = sd + kNopivBlock * kNopivLd;     // columns of L^-1
+    Z* su = sl + kNopivBlock * kNopivLd;     // columns of U^-1
+    const int b = blockIdx.x, r0 = b * kNopivBlock, w = min(kNopivBlock, n - r0);
+    for (int e = threadIdx.x; e < kNopivBlock * kNopivBlock; e += blockDim.x) {
+        const int r = e & 63, c = e >> 6;
+        Z v = r == c ? Z{1.0, 0.0} : Z{0.0, 0.0};
+        if (r < w && c < w) v = load_el<CPLX>(f + ((size_t)(r0 + c) * ld + r0 + r) * ES);
+        sd[c * kNopivLd + r] = v;
+    }
+    __syncthreads();
+    const int j = threadIdx.x & 63;
+    if (threadIdx.x < 64) {
+        Z* col = sl + j * kNopivLd;
+        for (int i = 0; i < j; ++i) col[i] = Z{0.0, 0.0};
+        col[j] = Z{1.0, 0.0};
+        for (int i = j + 1; i < kNopivBlock; ++i) {
+            Z acc{0.0, 0.0};
+            for (int k = j; k < i; ++k) acc = sub_prod<CPLX>(acc, sd[k * kNopivLd + i], col[k]);
+            col[i] = acc;
+        }
+    } else {
+        Z* col = su + j * kNopivLd;
+        for (int i = kNopivBlock - 1; i > j; --i) col[i] = Z{0.0, 0.0};
+        for (int i = j; i >= 0; --i) {
+            Z acc = i == j ? Z{1.0, 0.0} : Z{0.0, 0.0};
+            for (int k = i + 1; k <= j; ++k) acc = sub_prod<CPLX>(acc, sd[k * kNopivLd + i], col[k]);
+            col[i] = div_el<CPLX>(acc, sd[i * kNopivLd + i]);
+        }
+    }
+    __syncthreads();
+    double* il = inv + (size_t)b * kNopivBlock * kNopivBlock * ES;
+    double* iu = inv + ((size_t)nb + b) * kNopivBlock * kNopivBlock * ES;
+    for (int e = threadIdx.x; e < kNopivBlock * kNopivBlock; e += blockDim.x) {
+        const int r = e & 63, c = e >> 6;
+        store_el<CPLX>(il + (size_t)e * ES, sl[c * kNopivLd + r]);
+        store_el<CPLX>(iu + (size_t)e * ES, su[c * kNopivLd + r]);
+    }
+}
+
+__device__ __forceinline__ int ld_acquire_int(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_int(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+template <bool CPLX>
+__device__ __forceinline__ Z load_el_cg(const double* p) {
+    return CPLX ? Z{__ldcg(p), __ldcg(p + 1)} : Z{__ldcg(p), 0.0};
+}
+
+// Wait until block j of a chained solve is published; false (the error flag
+// set) after kWaitTimeoutNs without it, or when another CTA gave up.
+__device__ bool chain_wait(const int* flag, int* err) {
+    if (ld_acquire_int(flag) != 0) return true;
+    const unsigned long long start = global_timer_ns();
+    for (unsigned it = 1;; ++it) {
+        if (ld_acquire_int(flag) != 0) return true;
+        if (it > 32) __nanosleep(64);
+        if ((it & 255u) == 0) {
+            if (*reinterpret_cast<volatile int*>(err) != 0) return false;
+            if (global_timer_ns() - start > kWaitTimeoutNs) {
+                atomicCAS(err, 0, kDevTimeoutChain);
+                return false;
+            }
+        }
+    }
+}
+
+constexpr int kChainCols = 4;  // right-hand sides per chained launch
+
+// One triangle of packed factors without interchanges (n x n) applied as
+// x := T^-1 x for up to 4 columns, row blocks of 64 chained through flags:
+// the CTA owning block b subtracts T_bj x_j for every earlier block j as
+// each is published, then x_b := T_bb^-1 (that sum) with the precomputed
+// inverse, and publishes it. LOWERF: the unit lower factor L (else U); ADJ:
+// T is the factor's conjugate transpose. Blocks go to CTAs in solve order and
+// the launch is cooperative, so every block a CTA waits for is owned by a
+// resident CTA that is working through earlier blocks only.
+template <bool CPLX, bool LOWERF, bool ADJ>
+__global__ void __launch_bounds__(256) chain_solve_kernel(const double* f, int ld, const double* inv, int n, int nb,
+                                                        double* x, int ldx, int ncols, int* ready, int* err) {
+    constexpr int ES = CPLX ? 2 : 1;
+    constexpr bool FORWARD = LOWERF != ADJ;
+    extern __shared__ __align__(16) unsigned char chain_smem[];
+    Z* st = reinterpret_cast<Z*>(chain_smem);  // a 64 x 64 block, st[c * kNopivLd + r]
+    Z* sx = st + kNopivBlock * kNopivLd;       // sx[c * 64 + k]
+    __shared__ int s_ok;
+    const int r = threadIdx.x & 63, c = threadIdx.x >> 6;
+    const double* invs = inv + (LOWERF ? 0 : (size_t)nb * kNopivBlock * kNopivBlock * ES);
+    for (int q = blockIdx.x; q < nb; q += gridDim.x) {
+        const int b = FORWARD ? q : nb - 1 - q, r0 = b * kNopivBlock;
+        Z acc = c < ncols ? load_el<CPLX>(x + ((size_t)c * ldx + r0 + r) * ES) : Z{0.0, 0.0};
+        const int deps = FORWARD ? b : nb - 1 - b;
+        for (int s = 0; s < deps; ++s) {
+            const int j = FORWARD ? s : nb - 1 - s, j0 = j * kNopivBlock;
+            __syncthreads();
+            // T_bj: F[r0.., j0..] or, for the adjoint, conj(F[j0.., r0..])^T
+            const int fr = ADJ ? j0 : r0, fc = ADJ ? r0 : j0;
+            stage_block<CPLX>(st, f + ((size_t)fc * ld + fr) * ES, ld, kNopivBlock, kNopivBlock, false);
+            if (threadIdx.x == 0) s_ok = chain_wait(ready + j, err) ? 1 : 0;
+            __syncthreads();
+            if (!s_ok) return;
+            for (int e = threadIdx.x; e < kNopivBlock * ncols; e += blockDim.x) {
+                const int k = e & 63, cc = e >> 6;
+                sx[cc * kNopivBlock + k] = load_el_cg<CPLX>(x + ((size_t)cc * ldx + j0 + k) * ES);
+            }
+            __syncthreads();
+            if (c < ncols) {
+#pragma unroll 8
+                for (int k = 0; k < kNopivBlock; ++k) {
+                    Z t = ADJ ? st[r * kNopivLd + k] : st[k * kNopivLd + r];
+                    if (ADJ) t.im = -t.im;
+                    acc = sub_prod<CPLX>(acc, t, sx[c * kNopivBlock + k]);
+                }
+            }
+        }
+        __syncthreads();
+        const double* ib = invs + (size_t)b * kNopivBlock * kNopivBlock * ES;
+        stage_block<CPLX>(st, ib, kNopivBlock, kNopivBlock, kNopivBlock, false);
+        if (c < ncols) sx[c * kNopivBlock + r] = acc;
+        __syncthreads();
+        if (c < ncols) {
+            Z v{0.0, 0.0};
+#pragma unroll 8
+            for (int k = 0; k < kNopivBlock; ++k) {
+                Z t = ADJ ? st[r * kNopivLd + k] : st[k * kNopivLd + r];
+                if (ADJ) t.im = -t.im;
+                v = sub_prod<CPLX>(v, Z{-t.re, -t.im}, sx[c * kNopivBlock + k]);
+            }
+            if (r0 + r < n) store_el<CPLX>(x + ((size_t)c * ldx + r0 + r) * ES, v);
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) st_release_int(ready + b, 1);
+    }
+}
+
+constexpr int kInverseSmem = 3 * kNopivBlock * kNopivLd * 16;
+constexpr int kChainSmem = kNopivBlock * kNopivLd * 16 + kChainCols * kNopivBlock * 16;
+
+template <bool CPLX, bool LOWERF, bool ADJ>
+void launch_chain(Context& ctx, const DMat& f, const double* inv, double* x, int ldx, int ncols, int* ready) {
+    auto kernel = chain_solve_kernel<CPLX, LOWERF, ADJ>;
+    static bool configured[64] = {};
+    static int per_sm[64] = {};
+    const int dev = ctx.device >= 0 && ctx.device < 64 ? ctx.device : 0;
+    if (!configured[dev]) {
+        TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChainSmem));
+        TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], kernel, 256, kChainSmem));
+        configured[dev] = true;
+    }
+    if (per_sm[dev] < 1) fail(TNS_E_DEVICE, "the chained triangular solve cannot be resident");
+    const int n = f.rows, nb = (n + kNopivBlock - 1) / kNopivBlock;
+    const int grid = std::min(nb, per_sm[dev] * ctx.num_sms);
+    TNS_CUDA(cudaMemsetAsync(ready, 0, sizeof(int) * nb, ctx.stream));
+    const double* fp = f.p;
+    int ld = f.ld();
+    int* err = ctx.d_err;
+    void* args[] = {(void*)&fp, (void*)&ld, (void*)&inv, (void*)&n, (void*)&nb, (void*)&x, (void*)&ldx,
+                    (void*)&ncols, (void*)&ready, (void*)&err};
+    TNS_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), dim3(grid), dim3(256), args, kChainSmem,
+                                         ctx.stream));
+    ctx.kernel_launches++;
+}
+
+// inv := the diagonal blocks' inverses of f (2 nb blocks of 64 x 64).
+void diagonal_block_inverses(Context& ctx, const DMat& f, DBuf& inv) {
+    const int n = f.rows, nb = (n + kNopivBlock - 1) / kNopivBlock;
+    const size_t doubles = (size_t)2 * nb * kNopivBlock * kNopivBlock * (f.cplx ? 2 : 1);
+    if (inv.bytes < sizeof(double) * doubles) inv = DBuf(ctx, sizeof(double) * doubles);
+    static bool configured[2][64] = {};
+    const int dev = ctx.device >= 0 && ctx.device < 64 ? ctx.device : 0;
+    if (!configured[f.cplx][dev]) {
+        if (f.cplx)
+            TNS_CUDA(cudaFuncSetAttribute(diag_block_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kInverseSmem));
+        else
+            TNS_CUDA(cudaFuncSetAttribute(diag_block_inverse_kernel<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kInverseSmem));
+        configured[f.cplx][dev] = true;
+    }
+    if (f.cplx)
+        diag_block_inverse_kernel<true><<<nb, 128, kInverseSmem, ctx.stream>>>(f.p, f.ld(), n, nb, inv.as<double>());
+    else
+        diag_block_inverse_kernel<false><<<nb, 128, kInverseSmem, ctx.stream>>>(f.p, f.ld(), n, nb, inv.as<double>());
+    TNS_CUDA(cudaGetLastError());
+    ctx.kernel_launches++;
+}
+
+// x := (LU)^-1 x or (LU)^-H x for packed factors without interchanges, a few
+// columns at a time through the chained kernel (the estimator's probes).
+void chain_solve(Context& ctx, const DMat& f, const double* inv, DMat& x, int cols, bool adjoint) {
+    const int nb = (f.rows + kNopivBlock - 1) / kNopivBlock;
+    DBuf ready(ctx, sizeof(int) * nb);
+    const size_t es = f.cplx ? 2 : 1;
+    for (int c0 = 0; c0 < cols; c0 += kChainCols) {
+        const int nc = std::min(kChainCols, cols - c0);
+        double* xc = x.p + (size_t)c0 * x.ld() * es;
+        if (f.cplx) {
+            if (!adjoint) {
+                launch_chain<true, true, false>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+                launch_chain<true, false, false>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+            } else {
+                launch_chain<true, false, true>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+                launch_chain<true, true, true>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+            }
+        } else {
+            if (!adjoint) {
+                launch_chain<false, true, false>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+                launch_chain<false, false, false>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+            } else {
+                launch_chain<false, false, true>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+                launch_chain<false, true, true>(ctx, f, inv, xc, x.ld(), nc, ready.as<int>());
+            }
+        }
+    }
+}
+
+// Columns [j, j + w) of rows [j, n) factored without pivoting in 64-column
+// steps: the diagonal block, L21 := A21 U11^-1, U12 := L11^-1 A12 within the
+// panel, and the DMMA update of the panel's rest.
+void lu_nopiv_panel(Context& ctx, DMat& a, int j, int w, int* flag) {
+    const int n = a.rows, ld = a.ld();
+    const bool cplx = a.cplx;
+    if (cplx) configure_nopiv_kernels<true>();
+    else configure_nopiv_kernels<false>();
+    for (int b0 = 0; b0 < w; b0 += kNopivBlock) {
+        const int bw = std::min(kNopivBlock, w - b0), k = j + b0;
+        if (cplx) lu_nopiv_diag_kernel<true><<<1, 256, kNopivDiagSmem, ctx.stream>>>(a.at(k, k), ld, bw, k, flag);
+        else lu_nopiv_diag_kernel<false><<<1, 256, kNopivDiagSmem, ctx.stream>>>(a.at(k, k), ld, bw, k, flag);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+        const int below = n - k - bw, right = w - b0 - bw;
+        if (below > 0) {
+            const int grid = std::min((below + 7) / 8, ctx.num_sms * 2);
+            if (cplx)
+                trsm_right_upper_kernel<true><<<grid, 256, kNopivTrsmSmem, ctx.stream>>>(a.at(k, k), ld,
+                                                                                        a.at(k + bw, k), ld, below, bw);
+            else
+                trsm_right_upper_kernel<false><<<grid, 256, kNopivTrsmSmem, ctx.stream>>>(a.at(k, k), ld,
+                                                                                         a.at(k + bw, k), ld, below, bw);
+            TNS_CUDA(cudaGetLastError());
+            ctx.kernel_launches++;
+        }
+        if (right > 0) {
+            std::vector<TrsmDesc> t{TrsmDesc{a.at(k, k), ld, a.at(k, k + bw), ld, bw, right, 1, 1, 0}};
+            launch_trsm(ctx, cplx, 1, t);
+            if (below > 0) {
+                GemmProblem p{};
+                p.A = a.at(k + bw, k);
+                p.B = a.at(k, k + bw);
+                p.C = a.at(k + bw, k + bw);
+                p.lda = p.ldb = p.ldc = ld;
+                p.M = round_up(below, 2);
+                p.N = round_up(right, 2);
+                p.K = round_up(bw, 16);
+                p.alpha_re = -1.0;
+                p.beta_re = 1.0;
+                p.work = (long long)below * right * bw;
+                std::vector<GemmProblem> g{p};
+                gemm_grouped(ctx, g, cplx);
+            }
+        }
+    }
+}
+
+// The butterfly route; false (nothing of x written) when the elimination met
+// an exactly zero pivot or the refinement did not reach an FP64 backward error.
+bool gesv_mixed_butterfly(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter,
+                          MixedInfo& info) {
+    const int n = a.rows, nrhs = b.cols;
+    const bool cplx = a.cplx;
+    const int es = cplx ? 2 : 1;
+    const size_t esz = sizeof(double) * es;
+    const int N = round_up(n, 4);
+    info = MixedInfo{};
+
+    // The four random diagonals (T1, T2, S1, S2), from a fixed seed.
+    std::vector<double> dh(4 * (size_t)N);
+    uint64_t state = 0x5DEECE66D2026ull;
+    for (auto& v : dh) {
+        state += 0x9E3779B97F4A7C15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        const double r = (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+        v = std::exp(r / 10.0);
+    }
+    DBuf diag(ctx, sizeof(double) * dh.size());
+    TNS_CUDA(cudaMemcpyAsync(diag.p, dh.data(), sizeof(double) * dh.size(), cudaMemcpyHostToDevice, ctx.stream));
+    const double* dT1 = diag.as<double>();
+    const double* dT2 = dT1 + N;
+    const double* dS1 = dT1 + 2 * (size_t)N;
+    const double* dS2 = dT1 + 3 * (size_t)N;
+    const int grid = ctx.num_sms * 8;
+    auto rows_level = [&](DMat& m, int cols, int h, const double* d, int kind) {
+        if (cplx) butterfly_rows_kernel<true><<<grid, 256, 0, ctx.stream>>>(m.p, m.ld(), N, cols, h, d, kind);
+        else butterfly_rows_kernel<false><<<grid, 256, 0, ctx.stream>>>(m.p, m.ld(), N, cols, h, d, kind);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    };
+    auto cols_level = [&](DMat& m, int h, const double* d) {
+        if (cplx) butterfly_cols_kernel<true><<<grid, 256, 0, ctx.stream>>>(m.p, m.ld(), N, N, h, d);
+        else butterfly_cols_kernel<false><<<grid, 256, 0, ctx.stream>>>(m.p, m.ld(), N, N, h, d);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    };
+
+    // T A S, A embedded as [[A, 0], [0, I]].
+    DMat t(ctx, N, N, cplx, "the transformed matrix of a butterfly solve");
+    TNS_CUDA(cudaMemcpy2DAsync(t.p, (size_t)t.ld() * esz, a.p, (size_t)a.ld() * esz, (size_t)n * esz, n,
+                               cudaMemcpyDeviceToDevice, ctx.stream));
+    if (N > n) {
+        unit_diagonal_kernel<<<1, 32, 0, ctx.stream>>>(t.p, t.ld(), n, N, es);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    }
+    rows_level(t, N, N / 2, dT1, 0);
+    rows_level(t, N, N / 4, dT2, 0);
+    cols_level(t, N / 2, dS1);
+    cols_level(t, N / 4, dS2);
+
+    DMat f(ctx, N, N, cplx, "the low-precision factors");
+    DBuf flag(ctx, sizeof(int));
+    DBuf inverses;  // the factors' diagonal blocks, inverted, for the chained solves
+    auto factor = [&](int m) {
+        copy_dmat(ctx, f, t);
+        const int init = INT_MAX;
+        TNS_CUDA(cudaMemcpyAsync(flag.p, &init, sizeof(int), cudaMemcpyHostToDevice, ctx.stream));
+        for (int j = 0; j < N; j += kMixedOuter) {
+            const int w = std::min(kMixedOuter, N - j);
+            lu_nopiv_panel(ctx, f, j, w, flag.as<int>());
+            if (j + w < N) mixed_trailing(ctx, f, j, w, m);
+        }
+        diagonal_block_inverses(ctx, f, inverses);
+        int zero_at = INT_MAX;
+        TNS_CUDA(cudaMemcpyAsync(&zero_at, flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        info.factorizations++;
+        info.moduli = m;
+        return zero_at == INT_MAX;
+    };
+    // (LU)^-1 or (LU)^-H in place: a few columns (the estimator's probes)
+    // through the chained solve, wide panels by blocked TRSM + DMMA updates.
+    auto lu_solve = [&](DMat& m, int cols, bool adjoint) {
+        if (cols <= 2 * kChainCols) chain_solve(ctx, f, inverses.as<double>(), m, cols, adjoint);
+        else getrs_free_order(ctx, f, nullptr, m, cols, adjoint);
+    };
+    // M := A^-1 M or A^-H M in place on an N-row panel (zeros below row n).
+    const std::function<void(DMat&, int, bool)> solve = [&](DMat& m, int cols, bool adjoint) {
+        if (!adjoint) {
+            rows_level(m, cols, N / 2, dT1, 0);
+            rows_level(m, cols, N / 4, dT2, 0);
+            lu_solve(m, cols, false);
+            rows_level(m, cols, N / 4, dS2, 1);
+            rows_level(m, cols, N / 2, dS1, 1);
+        } else {
+            rows_level(m, cols, N / 2, dS1, 0);
+            rows_level(m, cols, N / 4, dS2, 0);
+            lu_solve(m, cols, true);
+            rows_level(m, cols, N / 4, dT2, 1);
+            rows_level(m, cols, N / 2, dT1, 1);
+        }
+    };
+
+    if (!factor(moduli > 0 ? moduli : 8)) return false;
+    const double anorm1 = norm1(ctx, a);
+    const NormestResult est = normest_solve(ctx, n, N, cplx, solve, 2, 5, 20260915);
+    info.rcond = (anorm1 > 0.0 && est.value > 0.0) ? 1.0 / (anorm1 * est.value) : 0.0;
+    if (!std::isfinite(est.value)) return false;
+    if (moduli == 0) {
+        // Without pivoting the factors may grow (small pivots are rare but not
+        // excluded): the images keep log2(kappa_1) + log2(growth) + 7 bits,
+        // growth = max |L\U| / max |T A S|.
+        auto absmax = [&](const DMat& m) {
+            const std::vector<double> c = col_absmax(ctx, m);
+            return c.empty() ? 0.0 : *std::max_element(c.begin(), c.end());
+        };
+        const double fmax = absmax(f), tmax = absmax(t);
+        if (!std::isfinite(fmax)) return false;
+        const double growth = tmax > 0.0 ? std::max(1.0, fmax / tmax) : 1.0;
+        const double kappa = info.rcond > 0.0 ? 1.0 / info.rcond : 1e300;
+        const int need = (int)std::ceil(std::log2(std::max(1.0, kappa)) + std::log2(growth)) + 7;
+        const int depth = cplx ? 2 * kMixedOuter : kMixedOuter;
+        int m = info.moduli;
+        while (m < 22 && split_integer_bits(m, depth) < need) ++m;
+        if (m > info.moduli) {
+            if (!factor(m)) return false;
+            // The first factors may have inflated the estimate: take it again
+            // from the factors the refinement uses.
+            const NormestResult again = normest_solve(ctx, n, N, cplx, solve, 2, 5, 20260915);
+            if (!std::isfinite(again.value)) return false;
+            info.rcond = (anorm1 > 0.0 && again.value > 0.0) ? 1.0 / (anorm1 * again.value) : 0.0;
+        }
+    }
+
+    // x on N rows; the residual's rows below n stay zero.
+    DMat xs(ctx, N, nrhs, cplx, "the solution");
+    TNS_CUDA(cudaMemcpy2DAsync(xs.p, (size_t)xs.ld() * esz, b.p, (size_t)b.ld() * esz, (size_t)n * esz, nrhs,
+                               cudaMemcpyDeviceToDevice, ctx.stream));
+    solve(xs, nrhs, false);
+    DMat xv = block_view(xs, 0, 0, n, nrhs);
+    DMat r(ctx, N, nrhs, cplx, "the refinement residual");
+    DMat rv = block_view(r, 0, 0, n, nrhs);
+    const double ainf = norminf(ctx, a);
+    const std::vector<double> bmax = col_absmax(ctx, b);
+    double prev = INFINITY;
+    for (int it = 0;; ++it) {
+        TNS_CUDA(cudaMemcpy2DAsync(r.p, (size_t)r.ld() * esz, b.p, (size_t)b.ld() * esz, (size_t)n * esz, nrhs,
+                                   cudaMemcpyDeviceToDevice, ctx.stream));
+        std::vector<GemmProblem> g{make_gemm(a, xv, rv, -1.0, 0.0, 1.0, 0.0)};
+        gemm_grouped(ctx, g, cplx);
+        const std::vector<double> rmax = col_absmax(ctx, rv), xmax = col_absmax(ctx, xv);
+        double berr = 0.0;
+        for (int j = 0; j < nrhs; ++j) {
+            const double den = ainf * xmax[j] + bmax[j];
+            berr = std::max(berr, den > 0.0 ? rmax[j] / den : (rmax[j] > 0.0 ? INFINITY : 0.0));
+        }
+        info.backward_error = berr;
+        if (berr <= 4.0 * 1.1102230246251565e-16 || it >= max_iter || !(berr < 0.5 * prev)) break;
+        prev = berr;
+        solve(r, nrhs, false);
+        std::vector<EwDesc> add{ew_add_scaled(xs, r, 1.0)};
+        ew_batch(ctx, add);
+        info.iterations++;
+    }
+    // An FP64 backward error (8 u), or the pivoting route decides.
+    if (!(info.backward_error <= 8.0 * 1.1102230246251565e-16)) return false;
+    x = DMat(ctx, n, nrhs, cplx, "the solution");
+    TNS_CUDA(cudaMemcpy2DAsync(x.p, (size_t)x.ld() * esz, xs.p, (size_t)xs.ld() * esz, (size_t)n * esz, nrhs,
+                               cudaMemcpyDeviceToDevice, ctx.stream));
+    return true;
+}
+
+}  // namespace
+
+void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter, MixedInfo& info) {
+    if (gesv_mixed_butterfly(ctx, a, b, x, moduli, max_iter, info)) return;
+    const int tried = info.factorizations;
+    gesv_mixed_pivoted(ctx, a, b, x, moduli, max_iter, info);
+    info.factorizations += tried;
 }
 
 }  // namespace tns

@@ -999,6 +999,11 @@ void gemm_split_batch(Context& ctx, std::vector<SplitProduct>& v, int moduli) {
         if (p.a->rows > 0 && p.b->cols > 0) live.push_back(p);
     }
     if (live.empty()) return;
+    // Deepest products first: the modular GEMM's CTAs are dispatched in tile
+    // order and a tile's time grows with its depth, so the launch ends on the
+    // light tiles.
+    std::stable_sort(live.begin(), live.end(),
+                     [](const SplitProduct& x, const SplitProduct& y) { return x.a->cols > y.a->cols; });
     if (moduli < 8 || moduli > kMaxModuli)
         fail(TNS_E_ARGUMENT, "split-precision products take 8 to " + std::to_string(kMaxModuli) + " moduli");
     if (live[0].a->cplx) split_launch<true>(ctx, live, moduli);

@@ -331,6 +331,7 @@ void getrs(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bo
 // The same solves in no particular order: 64-row triangular blocks and DMMA
 // GEMM updates of the rows beyond them (for the precision form, whose
 // refinement and condition estimate have no reference order to keep).
+// d_piv null: factors without row interchanges.
 void getrs_free_order(Context& ctx, const DMat& lu, const int* d_piv, DMat& b, int nrhs, bool adjoint);
 // The triangular solves of the reference's kernel seam (KernelEntry.cs:98-173,
 // Triangular.cs) in its order of operations: B := T^-1 B or T^-T B in place
@@ -347,8 +348,12 @@ void getrf_mixed(Context& ctx, DMat& a, int* d_piv, int moduli);
 struct MixedInfo {
     int moduli = 0, factorizations = 0, iterations = 0;
     double backward_error = 0.0, rcond = 0.0;
+    int pivoting = 0;  // 1: the partial-pivoting factorization ran (the butterfly route declined)
 };
-// x := A^-1 b (x shaped as b). moduli 0: from the condition estimate.
+// x := A^-1 b (x shaped as b). moduli 0: from the condition estimate. First
+// by random butterfly transforms and elimination without pivoting; when that
+// meets a zero pivot or its refinement does not reach an FP64 backward error,
+// again with partial pivoting.
 void gesv_mixed(Context& ctx, const DMat& a, const DMat& b, DMat& x, int moduli, int max_iter, MixedInfo& info);
 
 // ---- algorithms (algos.cu) -------------------------------------------------
@@ -361,6 +366,11 @@ NormestResult normest_power(Context& ctx, const DMat& a, int power, int t, int i
 // keep: the precision form's condition estimate).
 NormestResult normest_lu_inverse(Context& ctx, const DMat& lu, const int* d_piv, int t, int itmax, int seed,
                                  bool free_order = false);
+// ||M||_1 estimate of an operator M of order n given as an in-place device
+// solve: solve(panel, cols, adjoint) replaces the panel's first cols columns
+// (rows >= n, zero below row n) by M x or M^H x.
+NormestResult normest_solve(Context& ctx, int n, int rows, bool cplx,
+                            const std::function<void(DMat&, int, bool)>& solve, int t, int itmax, int seed);
 
 struct ExpmInfo {
     int degree = 0, squarings = 0;

@@ -304,15 +304,21 @@ typedef struct {
     int factorizations;    /* 1, or 2 when the condition estimate asked for more precision */
     int iterations;        /* refinement steps taken */
     double backward_error; /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) at the end */
-    double rcond;          /* 1 / (||A||_1 est ||A^-1||_1) from the first factors */
+    double rcond;          /* 1 / (||A||_1 est ||A^-1||_1) through the factors the refinement used */
+    int pivoting;          /* 0: butterfly transforms, no row interchanges; 1: partial pivoting ran */
 } tns_mixed_info;
 
 /* X := A^-1 B (A n x n, B and X n x nrhs) by a low-precision LU and FP64
  * iterative refinement. The LU's trailing updates (depth 512), nearly all of
  * its flops, run on the split-precision product with `moduli` moduli (8..22;
  * the integer images keep 26 bits with 8, 49 with 14); panels of 512 columns
- * use the FP64 LU. The refinement computes residuals in FP64 and stops when
- * the backward error reaches 4 u, stops halving, or after max_iter steps.
+ * are factored in FP64. First route: A becomes T A S with random butterfly
+ * transforms (depth 2, order padded to a multiple of 4) and is factored
+ * without row interchanges; if that meets an exactly zero pivot or its
+ * refinement ends above 8 u, the solve runs again with partial pivoting
+ * (info->pivoting = 1, info->factorizations counting both routes). The
+ * refinement computes residuals with A itself in FP64 and stops when the
+ * backward error reaches 4 u, stops halving, or after max_iter steps.
  * moduli = 0: chosen from the condition estimate kappa_1 of a first 8-moduli
  * factorization so that the images keep log2(kappa_1) + 7 bits (refactoring
  * once when that needs more). No counterpart in the reference, whose solve

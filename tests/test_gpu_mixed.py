@@ -12,7 +12,14 @@ Checks:
     Lu.Solve, bit-identical on the GPU, test_gpu_lu.py), the forward difference
     is within 100 kappa u: two backward-stable solutions each sit about
     kappa u from the exact one;
-  - the moduli chosen from the condition estimate grow with kappa.
+  - the moduli chosen from the condition estimate grow with kappa;
+  - the first route (random butterfly transforms, elimination without row
+    interchanges, the order padded to a multiple of 4) is the one that runs on
+    these matrices, at orders that need the padding too, real and complex;
+  - when that route's refinement cannot reach an FP64 backward error (no
+    refinement steps allowed), the solve runs again with partial pivoting and
+    reports it; an all-zero matrix ends in TNS_E_SINGULAR through the same
+    fallback.
 """
 import math
 
@@ -56,15 +63,16 @@ def test_mixed_solve_configuration(ws, n, kappa):
     assert fwd <= max(1e-13, 100.0 * kappa * U)
     # 0 steps when the chosen precision already gives an FP64 backward error
     assert 0 <= info["iterations"] <= 10
+    assert info["pivoting"] == 0
 
 
 def test_moduli_follow_condition(ws):
     chosen = []
     for kappa in (1e2, 1e6, 1e10):
-        a, b = conditioned(512, kappa, seed=7)
+        a, b = conditioned(1024, kappa, seed=7)
         _, info = ws.solve_mixed(a, b)
         chosen.append(info["moduli"])
-    assert chosen[0] == 8 and chosen[0] <= chosen[1] < chosen[2]
+    assert chosen == sorted(chosen) and chosen[0] < chosen[2]
 
 
 def test_fixed_moduli_and_complex(ws):
@@ -73,3 +81,38 @@ def test_fixed_moduli_and_complex(ws):
     assert info["moduli"] == 12 and info["factorizations"] == 1
     assert info["backward_error"] <= 1e-15
     assert rel(x, ws.factor_lu(a).solve(b)) <= max(1e-13, 100.0 * 1e4 * U)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 63, 130, 1001])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_butterfly_route_padded_orders(ws, n, cplx):
+    a, b = conditioned(n, 1e3, seed=n, cplx=cplx)
+    b = b[:, :7]
+    x, info = ws.solve_mixed(a, b)
+    assert info["pivoting"] == 0 and info["factorizations"] in (1, 2)
+    assert info["backward_error"] <= 1e-15
+    assert rel(x, np.linalg.solve(a, b)) <= max(1e-13, 100.0 * 1e3 * U)
+    # the condition estimate (normest1 of A^-1 through the transformed
+    # factors) is a lower bound of kappa_1, rarely far below it
+    k1 = np.linalg.cond(a, 1)
+    assert k1 / 30.0 <= 1.0 / info["rcond"] <= k1 * 1.01
+
+
+def test_fallback_to_partial_pivoting(ws):
+    # No refinement step allowed: 8 moduli (26-bit images) cannot give an
+    # FP64 backward error alone, so the butterfly route declines and the
+    # pivoting route answers (with the same limit).
+    a, b = conditioned(1024, 1e2, seed=3)
+    x, info = ws.solve_mixed(a, b, moduli=8, max_iter=0)
+    assert info["pivoting"] == 1 and info["factorizations"] == 2 and info["iterations"] == 0
+    assert info["backward_error"] > 8 * 2.0 ** -53
+    assert rel(x, np.linalg.solve(a, b)) <= 1e-4
+
+
+def test_zero_matrix_is_singular(ws):
+    from csharp_linearalgebra_b200 import SingularMatrixError
+    a = np.zeros((96, 96), order="F")
+    b = np.ones((96, 2), order="F")
+    with pytest.raises(SingularMatrixError) as e:
+        ws.solve_mixed(a, b, moduli=8)
+    assert "zero pivot" in str(e.value)
