@@ -33,7 +33,7 @@ def test_plain_and_split_at_bench_orders(ws, orc):
     rng = np.random.default_rng(12345)
     pert = [np.asfortranarray(a * (1.0 + 2.0 ** -52 * rng.standard_normal(a.shape))) for a in mats]
     moved = ws.expm_batched(pert)
-    ws.set_split_moduli(18)
+    ws.set_split_moduli(17)
     try:
         split = ws.expm_batched(mats, sd)
     finally:

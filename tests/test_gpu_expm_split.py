@@ -1,5 +1,5 @@
 """Expm with its products in the split-precision form (8-bit residues modulo
-18 or 20 moduli on the tensor cores, Chinese-remainder reconstruction).
+17 or 20 moduli on the tensor cores, Chinese-remainder reconstruction).
 
 The degree and the squaring count are the reference's exactly: their inputs
 (norms, A^2, A^4, A^6, normest1) stay in plain FP64.
@@ -30,9 +30,9 @@ MODULI = 20
 SPLIT_FLOOR_FACTOR = 6.0
 
 
-@pytest.fixture(params=[18, 20])
+@pytest.fixture(params=[17, 20])
 def split_ws(ws, request):
-    """The split form at the benchmark's 18 moduli and at 20."""
+    """The split form at the benchmark's 17 moduli and at 20."""
     global MODULI
     MODULI = request.param
     ws.set_split_moduli(MODULI)

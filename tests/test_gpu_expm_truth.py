@@ -44,7 +44,7 @@ def matrices():
     return mats
 
 
-@pytest.mark.parametrize("moduli", [18, 20])
+@pytest.mark.parametrize("moduli", [17, 20])
 def test_split_form_is_as_accurate_as_the_reference(ws, orc, moduli):
     mats = matrices()
     ws.set_split_moduli(0)
