@@ -199,6 +199,186 @@ __global__ void __launch_bounds__(512) panel_kernel(const __grid_constant__ Batc
     }
 }
 
+// The same factorization with the panel's columns taken kPanelSub at a
+// time: the sub-panel (its rows j0.. of kPanelSub columns) is factored in
+// shared memory column by column exactly as above, then its updates reach
+// the panel's later columns in one pass: their kPanelSub pivot rows first
+// (each element's updates by the earlier pivot rows of the sub-panel, in
+// order), then every row below, updates in order. Every element receives the
+// same operations in the same order as in panel_kernel (the updates are
+// regrouped per element, never reordered; row interchanges act on the later
+// columns' values as they stand, which carry the same rows), so factors and
+// pivots are identical; the later columns are read and written once per
+// sub-panel instead of once per column. Shared memory: kPanelSub columns of
+// smem_rows rows and the sub-panel's pivot rows over up to 64 columns.
+constexpr int kPanelSub = 8;
+constexpr int kPanelMaxWidth = 64;
+
+template <bool CPLX>
+__global__ void __launch_bounds__(512) panel_blocked_kernel(const __grid_constant__ Batch<PanelFactorDesc> b,
+                                                           int smem_rows) {
+    const PanelFactorDesc& d = batch_item(b, blockIdx.x);
+    constexpr int ES = CPLX ? 2 : 1;
+    extern __shared__ __align__(16) double pb_smem[];
+    double* S = pb_smem;                                     // S[(cc * smem_rows + i) * ES]: column j0 + cc, row j0 + i
+    double* U = pb_smem + (size_t)kPanelSub * smem_rows * ES;  // U[(k * kPanelMaxWidth + c) * ES]
+    __shared__ double s_val[16];
+    __shared__ int s_idx[16];
+    const int tid = threadIdx.x, nthreads = blockDim.x, warps = nthreads >> 5;
+    const int ld = d.ld, w = d.w, r0 = d.r0;
+    const int M = d.m - r0;
+    const int limit = min(M, w);
+    double* P = d.a + ((size_t)r0 * ld + r0) * ES;  // panel origin
+    auto ldz = [](const double* e) { return Z{e[0], CPLX ? e[1] : 0.0}; };
+    auto stz = [](double* e, Z v) {
+        e[0] = v.re;
+        if (CPLX) e[1] = v.im;
+    };
+    // t + (-mult) l with the panel kernel's roundings
+    auto upd = [](Z t, Z mult, Z l) {
+        if (!CPLX) return Z{add_rn(t.re, mul_rn(-mult.re, l.re)), 0.0};
+        return zadd(t, zmul(Z{-mult.re, -mult.im}, l));
+    };
+    auto nonzero = [](Z v) { return CPLX ? !(v.re == 0.0 && v.im == 0.0) : v.re != 0.0; };
+
+    for (int j0 = 0; j0 < limit; j0 += kPanelSub) {
+        const int sb = min(kPanelSub, limit - j0), Mr = M - j0;
+        for (int e = tid; e < Mr * sb; e += nthreads) {
+            const int i = e % Mr, cc = e / Mr;
+            stz(S + ((size_t)cc * smem_rows + i) * ES, ldz(P + ((size_t)(j0 + cc) * ld + j0 + i) * ES));
+        }
+        __syncthreads();
+        for (int jj = 0; jj < sb; ++jj) {
+            const int j = j0 + jj;
+            double* Sj = S + (size_t)jj * smem_rows * ES;
+            // a. first index of the largest pivot measure in column j, rows j..M-1
+            double best = -1.0;
+            int bidx = INT_MAX;
+            for (int i = jj + tid; i < Mr; i += nthreads) {
+                const double* e = Sj + (size_t)i * ES;
+                const double v = CPLX ? add_rn(fabs(e[0]), fabs(e[1])) : fabs(e[0]);
+                if (v > best || (v == best && i < bidx)) {
+                    best = v;
+                    bidx = i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+                if (ov > best || (ov == best && oi < bidx)) {
+                    best = ov;
+                    bidx = oi;
+                }
+            }
+            if ((tid & 31) == 0) {
+                s_val[tid >> 5] = best;
+                s_idx[tid >> 5] = bidx;
+            }
+            __syncthreads();
+            double bv = s_val[0];
+            int bi = s_idx[0];
+            for (int q = 1; q < warps; ++q)
+                if (s_val[q] > bv || (s_val[q] == bv && s_idx[q] < bi)) {
+                    bv = s_val[q];
+                    bi = s_idx[q];
+                }
+            // A column of NaNs (no comparison succeeds) keeps the diagonal.
+            const int pl = bi == INT_MAX ? jj : bi;
+            if (tid == 0) d.piv[r0 + j] = r0 + j0 + pl;
+            // b. swap rows j and p across the panel's w columns
+            if (pl != jj) {
+                for (int c = tid; c < w; c += nthreads) {
+                    double* x;
+                    double* y;
+                    if (c >= j0 && c < j0 + sb) {
+                        x = S + ((size_t)(c - j0) * smem_rows + jj) * ES;
+                        y = S + ((size_t)(c - j0) * smem_rows + pl) * ES;
+                    } else {
+                        x = P + ((size_t)c * ld + j) * ES;
+                        y = P + ((size_t)c * ld + j0 + pl) * ES;
+                    }
+                    for (int q = 0; q < ES; ++q) {
+                        const double tmp = x[q];
+                        x[q] = y[q];
+                        y[q] = tmp;
+                    }
+                }
+            }
+            __syncthreads();
+            // c. scale column j below the diagonal, rank-1 update of the
+            // sub-panel's columns beyond j
+            const Z value = ldz(Sj + (size_t)jj * ES);
+            const bool zero = !nonzero(value);
+            if (zero && tid == 0) atomicMin(d.singular, r0 + j);
+            bool recip;
+            Z r;
+            if (!CPLX) {
+                recip = fabs(value.re) >= kSafeMin;
+                r = Z{__ddiv_rn(1.0, value.re), 0.0};
+            } else {
+                recip = cabs_net(value.re, value.im) >= kSafeMin;
+                r = zdiv(Z{1.0, 0.0}, value);
+            }
+            for (int i = jj + 1 + tid; i < Mr; i += nthreads) {
+                Z l = ldz(Sj + (size_t)i * ES);
+                if (!zero) {
+                    if (!CPLX) l = Z{recip ? mul_rn(l.re, r.re) : __ddiv_rn(l.re, value.re), 0.0};
+                    else l = recip ? zmul(l, r) : zdiv(l, value);
+                    stz(Sj + (size_t)i * ES, l);
+                }
+                for (int cc = jj + 1; cc < sb; ++cc) {
+                    const Z mult = ldz(S + ((size_t)cc * smem_rows + jj) * ES);
+                    if (nonzero(mult)) {
+                        double* t = S + ((size_t)cc * smem_rows + i) * ES;
+                        stz(t, upd(ldz(t), mult, l));
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < Mr * sb; e += nthreads) {
+            const int i = e % Mr, cc = e / Mr;
+            stz(P + ((size_t)(j0 + cc) * ld + j0 + i) * ES, ldz(S + ((size_t)cc * smem_rows + i) * ES));
+        }
+        const int tc = w - j0 - sb;  // the panel's later columns
+        if (tc > 0) {
+            // their pivot rows j0 .. j0 + sb - 1: the earlier pivot rows' updates in order
+            for (int c = tid; c < tc; c += nthreads) {
+                double* col = P + (size_t)(j0 + sb + c) * ld * ES;
+                for (int rr = 0; rr < sb; ++rr) {
+                    Z t = ldz(col + (size_t)(j0 + rr) * ES);
+                    for (int k = 0; k < rr; ++k) {
+                        const Z mult = ldz(U + ((size_t)k * kPanelMaxWidth + c) * ES);
+                        if (nonzero(mult)) t = upd(t, mult, ldz(S + ((size_t)k * smem_rows + rr) * ES));
+                    }
+                    stz(col + (size_t)(j0 + rr) * ES, t);
+                    stz(U + ((size_t)rr * kPanelMaxWidth + c) * ES, t);
+                }
+            }
+            __syncthreads();
+            // every row below: the sb updates in order
+            for (int i = sb + tid; i < Mr; i += nthreads) {
+                Z l[kPanelSub];
+#pragma unroll
+                for (int k = 0; k < kPanelSub; ++k) l[k] = k < sb ? ldz(S + ((size_t)k * smem_rows + i) * ES) : Z{0.0, 0.0};
+                for (int c = 0; c < tc; ++c) {
+                    double* t = P + ((size_t)(j0 + sb + c) * ld + j0 + i) * ES;
+                    Z v = ldz(t);
+#pragma unroll
+                    for (int k = 0; k < kPanelSub; ++k) {
+                        if (k < sb) {
+                            const Z mult = ldz(U + ((size_t)k * kPanelMaxWidth + c) * ES);
+                            if (nonzero(mult)) v = upd(v, mult, l[k]);
+                        }
+                    }
+                    stz(t, v);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // The same factorization for one tall panel (thousands of rows), spread over
 // every SM: CTA g owns panel rows [g R, (g + 1) R) and keeps them in shared
 // memory for the whole panel (the single-CTA kernel re-reads and re-writes
@@ -900,6 +1080,7 @@ constexpr int kGatherMaxRows = 24576;  // perm + pivots in 192 KB of shared memo
 // One tall panel over all SMs (panel_coop_kernel), when it has enough rows
 // to pay for a barrier per column and every CTA's slab fits shared memory.
 constexpr int kCoopPanelRows = 1024;
+constexpr size_t kPanelBlockedSmem = 200 * 1024;  // the blocked panel's largest shared-memory footprint
 
 template <bool CPLX>
 bool launch_panel_coop(Context& ctx, const PanelFactorDesc& p) {
@@ -950,8 +1131,32 @@ void launch_panels(Context& ctx, bool cplx, std::vector<PanelFactorDesc>& v) {
         if (cplx ? launch_panel_coop<true>(ctx, v[0]) : launch_panel_coop<false>(ctx, v[0])) return;
     }
     Batch<PanelFactorDesc> b = make_batch(ctx, v);
-    if (cplx) panel_kernel<true><<<b.count, 512, 0, ctx.stream>>>(b);
-    else panel_kernel<false><<<b.count, 512, 0, ctx.stream>>>(b);
+    // The blocked panel when every item's sub-panel fits shared memory.
+    int rows = 0, width = 0;
+    for (auto& p : v) {
+        rows = std::max(rows, p.m - p.r0);
+        width = std::max(width, p.w);
+    }
+    const size_t es = cplx ? 2 : 1;
+    const size_t smem = sizeof(double) * es * ((size_t)kPanelSub * rows + (size_t)kPanelSub * kPanelMaxWidth);
+    if (width <= kPanelMaxWidth && smem <= kPanelBlockedSmem) {
+        static bool configured[2][64] = {};
+        const int dev = ctx.device >= 0 && ctx.device < 64 ? ctx.device : 0;
+        if (!configured[cplx][dev]) {
+            if (cplx)
+                TNS_CUDA(cudaFuncSetAttribute(panel_blocked_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              kPanelBlockedSmem));
+            else
+                TNS_CUDA(cudaFuncSetAttribute(panel_blocked_kernel<false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelBlockedSmem));
+            configured[cplx][dev] = true;
+        }
+        if (cplx) panel_blocked_kernel<true><<<b.count, 512, smem, ctx.stream>>>(b, rows);
+        else panel_blocked_kernel<false><<<b.count, 512, smem, ctx.stream>>>(b, rows);
+    } else {
+        if (cplx) panel_kernel<true><<<b.count, 512, 0, ctx.stream>>>(b);
+        else panel_kernel<false><<<b.count, 512, 0, ctx.stream>>>(b);
+    }
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
 }
