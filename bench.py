@@ -642,6 +642,7 @@ def config_gemm(args, ws, torch, oracle, res, gpu_ms, cpu_s, cores, peak64):
                                         dc.data_ptr(), n), reps=5)
     e2e_ms, c = gpu_ms(lambda: ws.multiply(a, b), reps=5)
     cs, cref = cpu_s(lambda: oracle.gemm(a, b))
+    cs1, _ = cpu_s(lambda: oracle.gemm(a, b, multithreaded=False))
     flops = 2.0 * n ** 3
     kernel_ms = []
     for _ in range(5):
@@ -664,6 +665,8 @@ def config_gemm(args, ws, torch, oracle, res, gpu_ms, cpu_s, cores, peak64):
                                "operands in L2)"},
         "cpu_baseline": {"value": flops / cs / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
                          "sample": "the same product, the reference's threaded blocking (KC 256)"},
+        "cpu_baseline_one_thread": {"value": flops / cs1 / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
+                                    "sample": "the same product, the reference's serial Gemm (KC 384)"},
         "bit_identical_to_reference": bool(np.array_equal(c, cref))}
     del da, db, dc
 

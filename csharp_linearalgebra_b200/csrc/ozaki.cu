@@ -422,15 +422,16 @@ struct ModDesc {
     int mp;                  // rows of an output plane (multiple of 128)
     int tiles_m, tile_begin;
     uint8_t* u;              // nm planes of mp x np bytes, row-major: u_q of each product entry
+    int m_base;              // first output row of the tiles (a strip left over by the CTA-pair kernel)
 };
 struct ModMaps {
     CUtensorMap a, b;  // residues as (kp bytes) x (rows) x nm; boxes of 128 bytes x 128 (A) or 256 (B) rows, 128-byte swizzle
 };
 
+// One CTA's work on output tile `tile` of the launch's tile list.
 template <int TN>
-__global__ void __launch_bounds__(kSplitThreads, 1)
-    modular_gemm_kernel(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps, int nprob,
-                        const __grid_constant__ CrtParams cp, int* err) {
+__device__ __forceinline__ void modular_tile(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps,
+                                             int nprob, const CrtParams& cp, int* err, int tile) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -448,13 +449,13 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].tile_begin <= (int)blockIdx.x) lo = mid;
+        if (descs[mid].tile_begin <= tile) lo = mid;
         else hi = mid - 1;
     }
     const ModDesc& D = descs[lo];
     const ModMaps& MP = maps[lo];
-    const int local = blockIdx.x - D.tile_begin;
-    const int m0 = (local % D.tiles_m) * kTile, n0 = (local / D.tiles_m) * TN;
+    const int local = tile - D.tile_begin;
+    const int m0 = D.m_base + (local % D.tiles_m) * kTile, n0 = (local / D.tiles_m) * TN;
     const int nkb = D.kp / kKb;
     const int nm = cp.nm;
 
@@ -606,6 +607,218 @@ __global__ void __launch_bounds__(kSplitThreads, 1)
         __syncwarp();
         tc_fence_after_sync();
         tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+template <int TN>
+__global__ void __launch_bounds__(kSplitThreads, 1)
+    modular_gemm_kernel(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps, int nprob,
+                        const __grid_constant__ CrtParams cp, int* err) {
+    modular_tile<TN>(descs, maps, nprob, cp, err, (int)blockIdx.x);
+}
+
+// The same product by CTA pairs (a cluster of two CTAs, cta_group::2): a pair
+// owns a 256 x 256 output tile. Each CTA loads 128 rows of A and its half
+// (128 rows) of B into its own shared memory, both reporting the bytes to the
+// even CTA's barrier; one thread of the even CTA issues the M = 256 MMAs,
+// which write 128 accumulator rows into each CTA's TMEM, and its commits
+// arrive on both CTAs' barriers. Per SM a stage is 32 KB instead of 48, so six
+// stages are in flight. Each CTA's epilogue reduces its own accumulator rows
+// and frees the buffer on the even CTA's barrier (8 warps). Every wait is
+// bounded; both CTAs meet at a cluster barrier before TMEM is released.
+constexpr int kStagesPair = 6;
+constexpr int kPairN = 256;                                    // output tile columns of a pair
+constexpr uint32_t kPairStageBytes = (uint32_t)(kTile + kPairN / 2) * kKb;  // A rows and half of B's
+constexpr int kPairSmem = kStagesPair * (int)kPairStageBytes + 1024 + 256;
+constexpr uint32_t kPairTmemCols = 2 * kPairN;
+
+static_assert(kPairSmem >= split_smem<kPairN>(), "the pair kernel's shared memory holds a one-CTA tile");
+
+// The first CTAs (odd_tiles rounded up to a whole cluster) take the one-CTA
+// tiles of odd last strips (odescs), one each, as modular_gemm_kernel<256>,
+// so that they run among the first pairs instead of after the last; the
+// clusters after them take the pair tiles (npairs of them).
+__global__ void __launch_bounds__(kSplitThreads, 1)
+    modular_gemm_pair_kernel(const ModDesc* __restrict__ descs, const ModMaps* __restrict__ maps, int nprob,
+                             int npairs, const ModDesc* __restrict__ odescs, const ModMaps* __restrict__ omaps,
+                             int nodd, int odd_tiles, const __grid_constant__ CrtParams cp, int* err) {
+    const int solo_ctas = odd_tiles + (odd_tiles & 1);
+    if ((int)blockIdx.x < solo_ctas) {  // the same for both CTAs of a cluster
+        if ((int)blockIdx.x < odd_tiles) modular_tile<kPairN>(odescs, omaps, nodd, cp, err, (int)blockIdx.x);
+        return;
+    }
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStagesPair * kPairStageBytes);  // even CTA's are used
+    uint64_t* empty = full + kStagesPair;
+    uint64_t* accf = empty + kStagesPair;
+    uint64_t* acce = accf + 2;  // even CTA's are used: 4 epilogue warps of each CTA arrive
+    uint64_t* done = acce + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint32_t* consumed = tmem_slot + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int pair = ((int)blockIdx.x - solo_ctas) >> 1;
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].tile_begin <= pair) lo = mid;
+        else hi = mid - 1;
+    }
+    const ModDesc& D = descs[lo];
+    const ModMaps& MP = maps[lo];
+    const int local = pair - D.tile_begin;
+    const int m0 = (2 * (local % D.tiles_m) + (int)rank) * kTile, n0 = (local / D.tiles_m) * kPairN;
+    const int nb0 = n0 + (int)rank * (kPairN / 2);  // this CTA's B rows
+    const int nkb = D.kp / kKb;
+    const int nm = cp.nm;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStagesPair; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 8);
+        }
+        mbar_init(done, 1);
+        *consumed = 0;
+        mbar_fence_init();
+    }
+    if (warp == 1) {
+        tmem_alloc2(tmem_slot, kPairTmemCols);
+        tmem_relinquish2();
+    }
+    tc_fence_before_sync();
+    __syncthreads();
+    cluster_sync();  // both CTAs' barriers exist before either reaches the other's
+    tc_fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+
+    auto stage_a = [&](int s) { return smem + s * kPairStageBytes; };
+    auto stage_b = [&](int s) { return smem + s * kPairStageBytes + kTile * kKb; };
+
+    uint32_t issued = 0;
+    if (warp == 0) {
+        if (lane == 0) {
+            tensormap_acquire(&MP.a);
+            tensormap_acquire(&MP.b);
+            bool ok = true;
+            for (int q = 0; q < nm && ok; ++q) {
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int st = issued % kStagesPair;
+                    if (!mbar_wait_bounded(&empty[st], ((issued / kStagesPair) & 1) ^ 1, err, kErrSplitEmpty)) {
+                        ok = false;
+                        break;
+                    }
+                    if (rank == 0) mbar_arrive_expect_tx(&full[st], 2 * kPairStageBytes);
+                    const uint32_t bar = cluster_addr(&full[st], 0);
+                    tma_load_3d_pair(stage_a(st), &MP.a, kb * kKb, m0, q, bar);
+                    tma_load_3d_pair(stage_b(st), &MP.b, kb * kKb, nb0, q, bar);
+                    ++issued;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {
+            constexpr uint32_t idesc = i8_instr_desc(2 * kTile, kPairN);
+            uint32_t it = 0;
+            bool ok = true;
+            for (int q = 0; q < nm && ok; ++q) {
+                const int buf = q & 1;
+                if (!mbar_wait_bounded(&acce[buf], ((q >> 1) & 1) ^ 1, err, kErrSplitAcc)) break;
+                tc_fence_after_sync();
+                const uint32_t dacc = tmem + buf * kPairN;
+                for (int kb = 0; kb < nkb; ++kb) {
+                    const int st = it % kStagesPair;
+                    if (!mbar_wait_bounded(&full[st], (it / kStagesPair) & 1, err, kErrSplitFull)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after_sync();
+#pragma unroll
+                    for (int kk = 0; kk < kKb / 32; ++kk) {
+                        mma_i8_pair(dacc, sw128_kmajor_desc(stage_a(st), kk * 32),
+                                    sw128_kmajor_desc(stage_b(st), kk * 32), idesc, !(kb == 0 && kk == 0));
+                    }
+                    mma_commit_pair(&empty[st], 0x3);
+                    ++it;
+                }
+                if (ok) mma_commit_pair(&accf[buf], 0x3);
+            }
+            *consumed = it;
+            mma_commit_pair(done, 0x3);
+        }
+    } else {
+        // Epilogue: as in modular_gemm_kernel, over this CTA's 128 accumulator
+        // rows and the pair's 256 columns.
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+        const uint32_t acce_even[2] = {cluster_addr(&acce[0], 0), cluster_addr(&acce[1], 0)};
+        for (int q = 0; q < nm; ++q) {
+            const int buf = q & 1;
+            const bool got = mbar_wait_bounded(&accf[buf], (q >> 1) & 1, err, kErrSplitAcc);
+            if (!__all_sync(0xffffffffu, got)) break;
+            tc_fence_after_sync();
+            const float2 w0 = make_float2(cp.w0[q], cp.w0[q]), w16 = make_float2(cp.w16[q], cp.w16[q]);
+            const float2 w0_off = make_float2(cp.w0_off[q], cp.w0_off[q]);
+            const float2 inv = make_float2(cp.inv[q], cp.inv[q]);
+            const float2 negp = make_float2((float)-cp.p[q], (float)-cp.p[q]);
+            const float2 magic = make_float2(kRoundMagicF, kRoundMagicF);
+            const float2 neg_magic = make_float2(-kRoundMagicF, -kRoundMagicF);
+            uint8_t* plane = D.u + ((size_t)q * D.mp + m0 + row) * D.np + n0;
+            for (int c0 = 0; c0 < kPairN; c0 += 16) {
+                uint32_t v[16];
+                tmem_ld16(tmem + lane_addr + buf * kPairN + c0, v);
+                tmem_wait_ld();
+                uint32_t bytes[16];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const uint32_t x0 = v[2 * e], x1 = v[2 * e + 1];
+                    const float2 lm = make_float2(__uint_as_float((x0 & 0xffffu) | 0x4B000000u),
+                                                  __uint_as_float((x1 & 0xffffu) | 0x4B000000u));
+                    const float2 hm = make_float2(__int_as_float(((int)x0 >> 16) + kRoundMagicBits),
+                                                  __int_as_float(((int)x1 >> 16) + kRoundMagicBits));
+                    const float2 sv = __ffma2_rn(__fadd2_rn(hm, neg_magic), w16, __ffma2_rn(lm, w0, w0_off));
+                    const float2 t = __fadd2_rn(__ffma2_rd(sv, inv, magic), neg_magic);
+                    const float2 u = __fadd2_rn(__ffma2_rn(t, negp, sv), magic);
+                    bytes[2 * e] = __float_as_uint(u.x);
+                    bytes[2 * e + 1] = __float_as_uint(u.y);
+                }
+                uint4 words;
+                words.x = pack4(bytes[0], bytes[1], bytes[2], bytes[3]);
+                words.y = pack4(bytes[4], bytes[5], bytes[6], bytes[7]);
+                words.z = pack4(bytes[8], bytes[9], bytes[10], bytes[11]);
+                words.w = pack4(bytes[12], bytes[13], bytes[14], bytes[15]);
+                *reinterpret_cast<uint4*>(plane + c0) = words;
+            }
+            tc_fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(acce_even[buf]);
+        }
+    }
+
+    // Leave only when nothing is in flight. The even CTA waits for the stages
+    // it issued but did not consume (all bytes of both CTAs report there);
+    // each CTA waits for the pair's last commit; then both meet, so neither
+    // leaves while the other's MMAs or arrivals may still reach it.
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0 && lane == 0 && rank == 0) {
+        for (uint32_t j = *consumed; j < issued; ++j)
+            if (!mbar_wait_bounded(&full[j % kStagesPair], (j / kStagesPair) & 1, err, kErrSplitDrain)) break;
+    }
+    if (warp == 1 && lane == 0) mbar_wait_bounded(done, 0, err, kErrSplitDrain);
+    tc_fence_before_sync();
+    __syncthreads();
+    cluster_sync();
+    if (warp == 1) {
+        tc_fence_after_sync();
+        tmem_dealloc2(tmem, kPairTmemCols);
     }
 }
 
@@ -883,13 +1096,13 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         cols.push_back(ExpDesc{p.b->p, p.b->ld(), s.k, s.n, eb});
         ra.push_back(ResDesc{p.a->p, p.a->ld(), s.m, s.k, s.kh, s.mp, s.kp, ea, a8});
         rb.push_back(ResDesc{p.b->p, p.b->ld(), s.n, s.k, s.kh, s.np, s.kp, eb, b8});
-        md.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles, u8});
+        md.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles, u8, 0});
         cd.push_back(CrtDesc{u8, s.mp, s.np, s.m, s.n, ea, eb, p.c->p, p.c->ld(), p.beta != 0.0 ? 1 : 0});
         tiles += (s.mp / kTile) * (s.np / tn);
         encode_residues(&maps[q].a, a8, s.kp, s.mp, nm, kTile);
         encode_residues(&maps[q].b, b8, s.kp, s.np, nm, tn);
         if (trial) {
-            md_narrow.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles_narrow, u8});
+            md_narrow.push_back(ModDesc{s.kp, s.np, s.mp, s.mp / kTile, tiles_narrow, u8, 0});
             tiles_narrow += (s.mp / kTile) * (s.np / 128);
             maps_narrow[q].a = maps[q].a;
             encode_residues(&maps_narrow[q].b, b8, s.kp, s.np, nm, 128);
@@ -934,12 +1147,13 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         TNS_CUDA(cudaEventRecord(e0, ctx.stream));
     }
     auto launch = [&](auto kernel, int smem_bytes, bool& configured, const ModDesc* descs, const ModMaps* mps,
-                      int ntiles) {
+                      int ntiles, int nprob = -1) {
         if (!configured) {
             TNS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
             configured = true;
         }
-        kernel<<<ntiles, kSplitThreads, smem_bytes, ctx.stream>>>(descs, mps, (int)md.size(), cp, ctx.d_err);
+        kernel<<<ntiles, kSplitThreads, smem_bytes, ctx.stream>>>(descs, mps, nprob < 0 ? (int)md.size() : nprob, cp,
+                                                                  ctx.d_err);
         TNS_CUDA(cudaGetLastError());
     };
     static bool configured_wide[64] = {}, configured_narrow[64] = {};
@@ -958,7 +1172,60 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
         ctx.autotune_trials++;
         ctx.kernel_launches++;
     } else if (tn == 256) {
-        launch(modular_gemm_kernel<256>, split_smem<256>(), configured_wide[ctx.device], d_desc, d_maps, tiles);
+        // CTA pairs over every two 128-row strips of a product; a product's
+        // odd last strip by the one-CTA kernel.
+        std::vector<ModDesc> pd, od;
+        std::vector<ModMaps> pmaps, omaps;
+        int pairs = 0, odd_tiles = 0;
+        for (size_t q = 0; q < v.size(); ++q) {
+            const auto& s = z[q];
+            const int strips = s.mp / kTile, cols = s.np / kPairN;
+            if (strips >= 2) {
+                ModMaps pm;
+                pm.a = maps[q].a;
+                encode_residues(&pm.b, reinterpret_cast<int8_t*>(at(s.b_off)), s.kp, s.np, nm, kPairN / 2);
+                pd.push_back(ModDesc{s.kp, s.np, s.mp, strips / 2, pairs, md[q].u, 0});
+                pmaps.push_back(pm);
+                pairs += (strips / 2) * cols;
+            }
+            if (strips % 2) {
+                od.push_back(ModDesc{s.kp, s.np, s.mp, 1, odd_tiles, md[q].u, (strips - 1) * kTile});
+                omaps.push_back(maps[q]);
+                odd_tiles += cols;
+            }
+        }
+        {
+            static bool configured_pair[64] = {};
+            if (!configured_pair[ctx.device]) {
+                TNS_CUDA(cudaFuncSetAttribute(modular_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              kPairSmem));
+                configured_pair[ctx.device] = true;
+            }
+            const ModDesc* pdd =
+                pd.empty() ? nullptr : static_cast<const ModDesc*>(ctx.upload(pd.data(), sizeof(ModDesc) * pd.size()));
+            const ModMaps* pmd = pmaps.empty() ? nullptr
+                                               : static_cast<const ModMaps*>(
+                                                     ctx.upload(pmaps.data(), sizeof(ModMaps) * pmaps.size()));
+            const ModDesc* odd =
+                od.empty() ? nullptr : static_cast<const ModDesc*>(ctx.upload(od.data(), sizeof(ModDesc) * od.size()));
+            const ModMaps* omd = omaps.empty() ? nullptr
+                                               : static_cast<const ModMaps*>(
+                                                     ctx.upload(omaps.data(), sizeof(ModMaps) * omaps.size()));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)(2 * pairs + odd_tiles + (odd_tiles & 1)));
+            cfg.blockDim = dim3(kSplitThreads);
+            cfg.dynamicSmemBytes = kPairSmem;
+            cfg.stream = ctx.stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            TNS_CUDA(cudaLaunchKernelEx(&cfg, modular_gemm_pair_kernel, pdd, pmd, (int)pd.size(), pairs, odd, omd,
+                                        (int)od.size(), odd_tiles, cp, ctx.d_err));
+        }
     } else {
         launch(modular_gemm_kernel<128>, split_smem<128>(), configured_narrow[ctx.device], d_desc, d_maps, tiles);
     }

@@ -98,3 +98,22 @@ def test_kernel_accuracy_at_sweep_orders(ws):
     got = ws.multiply_split(np.asfortranarray(a), np.asfortranarray(a), 20)
     ref = a @ a
     assert np.abs(got - ref).sum(axis=0).max() / np.abs(ref).sum(axis=0).max() < 1e-15
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cplx,n", [(False, 2560), (True, 1600)])
+def test_cta_pair_kernel_matches_one_cta_kernel(ws, cplx, n):
+    """Products whose 256-column tiles fill the GPU run on CTA pairs (two
+    CTAs sharing one M = 256 MMA); with 13 row strips (complex, n = 1600) the
+    last strip runs on the one-CTA kernel. Each 128-row block of A multiplied
+    alone runs the one-CTA kernel on the same integer images (row scales per
+    row, column scales per column, the same depth), so every row of the full
+    product must equal the block's bit for bit."""
+    rng = np.random.default_rng(n)
+    a, b = _mats(rng, n, n, n, cplx)
+    full = ws.multiply_split(a, b, 17)
+    for r0 in range(0, n, 128):
+        block = ws.multiply_split(np.asfortranarray(a[r0:r0 + 128]), b, 17)
+        assert np.array_equal(block, full[r0:r0 + 128]), f"rows {r0}.."
+    ref = a @ b
+    assert np.abs(full - ref).sum(axis=0).max() / np.abs(ref).sum(axis=0).max() < 1e-14
