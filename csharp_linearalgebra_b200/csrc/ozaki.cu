@@ -36,9 +36,12 @@
 // (M = 128, N = 256, K = 32) into one of two TMEM accumulators (all 512
 // columns); four epilogue warps reduce each
 // finished accumulator to u_q (tcgen05.ld) and store it as a byte plane while
-// the next modulus' MMAs run. Every wait is bounded; TMEM is released on
-// every path. Reconstruction: one CTA per 32 x 32 output tile, all planes
-// staged in shared memory, one column of 32 rows per warp store.
+// the next modulus' MMAs run. When the 256-column tiles fill the GPU, two
+// CTAs of a cluster share each M = 256 MMA instead (cta_group::2): each loads
+// its own 128 rows of A and half of B, so a stage is 32 KB per SM and six are
+// in flight (modular_gemm_pair_kernel). Every wait is bounded; TMEM is
+// released on every path. Reconstruction: one CTA per 32 x 32 output tile,
+// all planes staged in shared memory, one column of 32 rows per warp store.
 //
 // Accuracy: each entry differs from the exact product by at most about
 // K 2^-t of its row scale times its column scale (A' and B' rounded), the
