@@ -116,16 +116,37 @@ struct ExpDesc {
     int* out;
 };
 
-// Row exponents of A: one thread per row, over every column.
-template <bool CPLX>
-__global__ void row_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
+// Row exponents of A: one thread per (row, chunk of kRowExpChunk columns),
+// the exponents of the chunks with a nonzero entry folded by atomicMax into
+// out (set to INT_MIN first by exponent_init_kernel), then INT_MIN (an
+// all-zero row) replaced by 0, bound_exponent's value for zero
+// (exponent_fix_kernel). bound_exponent is increasing on positive values, so
+// the largest chunk exponent is the exponent of the row's largest magnitude.
+constexpr int kRowExpChunk = 64;
+
+__global__ void exponent_init_kernel(const __grid_constant__ Batch<ExpDesc> b) {
     const ExpDesc& d = batch_item(b, blockIdx.y);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.rows) return;
+    if (i < d.rows) d.out[i] = INT_MIN;
+}
+
+__global__ void exponent_fix_kernel(const __grid_constant__ Batch<ExpDesc> b) {
+    const ExpDesc& d = batch_item(b, blockIdx.y);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d.rows && d.out[i] == INT_MIN) d.out[i] = 0;
+}
+
+template <bool CPLX>
+__global__ void row_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
+    const ExpDesc& d = batch_item(b, blockIdx.z);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = blockIdx.y * kRowExpChunk;
+    if (i >= d.rows || k0 >= d.cols) return;
+    const int k1 = min(d.cols, k0 + kRowExpChunk);
     double m = 0.0;
     // Eight columns' loads in flight per step; the maximum is order-free.
-    int k = 0;
-    for (; k + 8 <= d.cols; k += 8) {
+    int k = k0;
+    for (; k + 8 <= k1; k += 8) {
         if (CPLX) {
             double2 z[8];
 #pragma unroll
@@ -140,7 +161,7 @@ __global__ void row_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
             for (int u = 0; u < 8; ++u) m = fmax(m, fabs(z[u]));
         }
     }
-    for (; k < d.cols; ++k) {
+    for (; k < k1; ++k) {
         if (CPLX) {
             const double2 z = reinterpret_cast<const double2*>(d.a)[(size_t)k * d.ld + i];
             m = fmax(m, fmax(fabs(z.x), fabs(z.y)));
@@ -148,7 +169,7 @@ __global__ void row_exponent_kernel(const __grid_constant__ Batch<ExpDesc> b) {
             m = fmax(m, fabs(d.a[(size_t)k * d.ld + i]));
         }
     }
-    d.out[i] = bound_exponent(m);
+    if (m > 0.0) atomicMax(d.out + i, bound_exponent(m));
 }
 
 // Column exponents of B: one warp per column.
@@ -1124,7 +1145,15 @@ void split_launch(Context& ctx, std::vector<SplitProduct>& v, int nm) {
     if (tiles == 0) return;
     {
         Batch<ExpDesc> br = make_batch(ctx, rows);
-        row_exponent_kernel<CPLX><<<dim3((max_m + 127) / 128, br.count), 128, 0, ctx.stream>>>(br);
+        exponent_init_kernel<<<dim3((max_m + 255) / 256, br.count), 256, 0, ctx.stream>>>(br);
+        TNS_CUDA(cudaGetLastError());
+        int max_k = 1;
+        for (auto& r : rows) max_k = std::max(max_k, r.cols);
+        row_exponent_kernel<CPLX><<<dim3((max_m + 127) / 128, (max_k + kRowExpChunk - 1) / kRowExpChunk, br.count),
+                                    128, 0, ctx.stream>>>(br);
+        TNS_CUDA(cudaGetLastError());
+        exponent_fix_kernel<<<dim3((max_m + 255) / 256, br.count), 256, 0, ctx.stream>>>(br);
+        ctx.kernel_launches += 2;
         TNS_CUDA(cudaGetLastError());
         Batch<ExpDesc> bc = make_batch(ctx, cols);
         col_exponent_kernel<CPLX><<<dim3((max_cols + 7) / 8, bc.count), 256, 0, ctx.stream>>>(bc);
