@@ -144,16 +144,23 @@ __global__ void pade_assemble_kernel(const __grid_constant__ Batch<PadeDesc> bt)
 
 // ---- norms ------------------------------------------------------------------
 
-// One thread per column: sequential sum of moduli in row order.
+// One warp per column: lanes load 32 consecutive entries (coalesced) and
+// form their moduli in parallel; the sum then takes them one by one in row
+// order (each broadcast by a shuffle), the same sequential sum as one thread
+// walking the column.
 template <bool CPLX>
 __global__ void col_abs_sums_kernel(const __grid_constant__ Batch<SumDesc> b) {
     const SumDesc& d = batch_item(b, blockIdx.y);
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= d.n) return;
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= d.n) return;  // the whole warp
     const double* col = d.a + (size_t)j * d.ld * (CPLX ? 2 : 1);
     double sum = 0.0;
-    for (int i = 0; i < d.m; ++i) sum = add_rn(sum, mag(col, i, CPLX));
-    d.out[j] = sum;
+    for (int i0 = 0; i0 < d.m; i0 += 32) {
+        const double v = i0 + lane < d.m ? mag(col, i0 + lane, CPLX) : 0.0;
+        const int cnt = min(32, d.m - i0);
+        for (int l = 0; l < cnt; ++l) sum = add_rn(sum, __shfl_sync(0xffffffffu, v, l));
+    }
+    if (lane == 0) d.out[j] = sum;
 }
 
 // One thread per row: sequential sum over columns in column order.
@@ -552,7 +559,7 @@ std::vector<double> norm1_batch(Context& ctx, const std::vector<const DMat*>& ma
         nmax = std::max(nmax, m->cols);
     }
     Batch<SumDesc> bs = make_batch(ctx, sums);
-    dim3 grid((nmax + 127) / 128, bs.count);
+    dim3 grid((nmax + 3) / 4, bs.count);  // 4 warps, one column each
     if (cplx) col_abs_sums_kernel<true><<<grid, 128, 0, ctx.stream>>>(bs);
     else col_abs_sums_kernel<false><<<grid, 128, 0, ctx.stream>>>(bs);
     Batch<SumDesc> bf = make_batch(ctx, folds);
