@@ -885,16 +885,37 @@ __global__ void __launch_bounds__(128) subst_diag_kernel(const __grid_constant__
         }
 }
 
+// Asynchronous 16- or 8-byte copies global -> shared; src_bytes 0 fills the
+// destination with zeros and reads nothing.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+constexpr int kSubstKC = 16;  // steps per staged round of the update kernel
+constexpr int kSubstUpdateSmem = 2 * kSubstKC * (64 + 65) * (int)sizeof(double) * 2;  // two rounds' buffers
+
 // Step 2: rows [r0, r1) of every column take the updates of steps [k0, k1)
 // (ascending for the lower factor, descending for the upper), 64 x 64 tiles
 // of (row, column) per CTA over a flat grid of every item's tiles. Thread
 // (tx, ty) keeps rows tx + 16 r and columns ty + 16 s (r, s < 4) in registers
 // from the value x already holds; each round stages 16 steps of the factor
-// column and of the solved x[k] in shared memory.
+// column and of the solved x[k] in shared memory, the next round's copies in
+// flight (cp.async, two buffers) while this one is applied.
 template <bool CPLX, bool UPPER>
 __global__ void __launch_bounds__(256, 2) subst_update_kernel(const __grid_constant__ Batch<SubstUpdateDesc> b) {
     constexpr int ES = CPLX ? 2 : 1;
-    constexpr int KC = 16;
+    constexpr int KC = kSubstKC;
     int lo = 0, hi = b.count - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -904,9 +925,40 @@ __global__ void __launch_bounds__(256, 2) subst_update_kernel(const __grid_const
     const SubstUpdateDesc& d = batch_item(b, lo);
     const int tile = blockIdx.x - d.tile_begin;
     const int i0 = d.r0 + (tile % d.tiles_m) * 64, c0 = (tile / d.tiles_m) * 64;
-    __shared__ Z sF[KC][64];
-    __shared__ Z sX[KC][64 + 1];
+    extern __shared__ __align__(16) unsigned char subst_smem[];
+    Z* sF = reinterpret_cast<Z*>(subst_smem);  // [2][KC][64]
+    Z* sX = sF + 2 * KC * 64;                   // [2][KC][65]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    if (!CPLX) {
+        // 8-byte copies fill only the real parts; the imaginary parts stay 0.
+        for (int e = tid; e < 2 * KC * (64 + 65); e += 256) sF[e] = Z{0.0, 0.0};
+        __syncthreads();
+    }
+    auto stage = [&](int q, int buf) {
+        const int kq = UPPER ? d.k1 - (q + 1) * KC : d.k0 + q * KC;
+        Z* F = sF + buf * KC * 64;
+        Z* X = sX + buf * KC * 65;
+        for (int e = tid; e < KC * 64; e += 256) {
+            const int kk = e >> 6, r = e & 63;
+            const int k = kq + kk, i = i0 + r;
+            const bool ok = k >= d.k0 && k < d.k1 && i < d.r1;
+            const double* p = ok ? d.f + ((size_t)k * d.ldf + i) * ES : d.f;
+            if (CPLX) cp_async16(&F[kk * 64 + r], p, ok);
+            else cp_async8(&F[kk * 64 + r], p, ok);
+        }
+        for (int e = tid; e < KC * 64; e += 256) {
+            const int kk = e % KC, c = e / KC;
+            const int k = kq + kk, col = c0 + c;
+            // steps outside [k0, k1) read as zero and are skipped
+            const bool ok = k >= d.k0 && k < d.k1 && col < d.nrhs;
+            const double* p = ok ? d.x + ((size_t)col * d.ldx + k) * ES : d.x;
+            if (CPLX) cp_async16(&X[kk * 65 + c], p, ok);
+            else cp_async8(&X[kk * 65 + c], p, ok);
+        }
+    };
+    const int rounds = (d.k1 - d.k0 + KC - 1) / KC;
+    stage(0, 0);
+    cp_async_commit();
     Z acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
@@ -919,30 +971,17 @@ __global__ void __launch_bounds__(256, 2) subst_update_kernel(const __grid_const
                 acc[r][s] = Z{p[0], CPLX ? p[1] : 0.0};
             }
         }
-    const int rounds = (d.k1 - d.k0 + KC - 1) / KC;
     for (int q = 0; q < rounds; ++q) {
-        const int kq = UPPER ? d.k1 - (q + 1) * KC : d.k0 + q * KC;
-        for (int e = tid; e < KC * 64; e += 256) {
-            const int kk = e >> 6, r = e & 63;
-            const int k = kq + kk, i = i0 + r;
-            Z v{0.0, 0.0};
-            if (k >= d.k0 && k < d.k1 && i < d.r1) {
-                const double* p = d.f + ((size_t)k * d.ldf + i) * ES;
-                v = Z{p[0], CPLX ? p[1] : 0.0};
-            }
-            sF[kk][r] = v;
-        }
-        for (int e = tid; e < KC * 64; e += 256) {
-            const int kk = e % KC, c = e / KC;
-            const int k = kq + kk, col = c0 + c;
-            Z v{0.0, 0.0};  // steps outside [k0, k1) read as zero and are skipped
-            if (k >= d.k0 && k < d.k1 && col < d.nrhs) {
-                const double* p = d.x + ((size_t)col * d.ldx + k) * ES;
-                v = Z{p[0], CPLX ? p[1] : 0.0};
-            }
-            sX[kk][c] = v;
+        if (q + 1 < rounds) {
+            stage(q + 1, (q + 1) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
+        const Z* F = sF + (q & 1) * KC * 64;
+        const Z* X = sX + (q & 1) * KC * 65;
 #pragma unroll
         for (int j = 0; j < KC; ++j) {
             const int kk = UPPER ? KC - 1 - j : j;
@@ -950,13 +989,13 @@ __global__ void __launch_bounds__(256, 2) subst_update_kernel(const __grid_const
             bool live[4];
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
-                const Z xv = sX[kk][ty + 16 * s];
+                const Z xv = X[kk * 65 + ty + 16 * s];
                 live[s] = !(xv.re == 0.0 && xv.im == 0.0);
                 nxk[s] = Z{-xv.re, -xv.im};
             }
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const Z fv = sF[kk][tx + 16 * r];
+                const Z fv = F[kk * 64 + tx + 16 * r];
 #pragma unroll
                 for (int s = 0; s < 4; ++s)
                     if (live[s]) acc[r][s] = subst_axpy<CPLX>(acc[r][s], nxk[s], fv);
@@ -1232,7 +1271,14 @@ void launch_subst_step_t(Context& ctx, std::vector<SubstDiagDesc>& diag, std::ve
         }
         if (total > INT_MAX) fail(TNS_E_ARGUMENT, "triangular solve too large for one launch");
         Batch<SubstUpdateDesc> b = make_batch(ctx, upd);
-        subst_update_kernel<CPLX, UPPER><<<(unsigned)total, 256, 0, ctx.stream>>>(b);
+        static bool configured[64] = {};
+        const int dev = ctx.device >= 0 && ctx.device < 64 ? ctx.device : 0;
+        if (!configured[dev]) {
+            TNS_CUDA(cudaFuncSetAttribute(subst_update_kernel<CPLX, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSubstUpdateSmem));
+            configured[dev] = true;
+        }
+        subst_update_kernel<CPLX, UPPER><<<(unsigned)total, 256, kSubstUpdateSmem, ctx.stream>>>(b);
         TNS_CUDA(cudaGetLastError());
         ctx.kernel_launches++;
     }
