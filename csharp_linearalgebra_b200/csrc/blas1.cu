@@ -228,31 +228,46 @@ __global__ void moduli_kernel(const __grid_constant__ Batch<ChainDesc> b) {
     }
 }
 
-// One pass: next[j] = sum_i row[i] * mags[i, j], sequential in i.
-__global__ void abs_power_step_kernel(const __grid_constant__ Batch<ChainDesc> b, int parity) {
+// One pass: next[j] = sum_i row[i] * mags[i, j], sequential in i. One warp
+// per 32 columns: each 32-row chunk of them is read by 32 coalesced loads
+// (one column each, a row per lane, the next chunk's loads issued before this
+// chunk is used), transposed through shared memory, and lane c continues
+// column c's sum over the chunk's rows in order: one thread's sequential sum
+// per column, as before, with the reads in whole sectors.
+constexpr int kChainWarps = 4;
+__global__ void __launch_bounds__(32 * kChainWarps) abs_power_step_kernel(const __grid_constant__ Batch<ChainDesc> b,
+                                                                          int parity) {
     const ChainDesc& d = batch_item(b, blockIdx.y);
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= d.n) return;
+    __shared__ double tile[kChainWarps][32][33];
+    __shared__ double rowv[kChainWarps][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j0 = (blockIdx.x * kChainWarps + warp) * 32;
+    if (j0 >= d.n) return;  // the whole warp; only warp-level synchronisation below
     const double* row = parity ? d.next : d.row;
     double* out = parity ? d.row : d.next;
-    const double* col = d.mags + (size_t)j * d.ld;
+    const int ncol = min(32, d.n - j0);
+    double cur[32], nxt[32];
+    auto load = [&](int i0, double (&v)[32]) {
+        const int i = i0 + lane;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = (c < ncol && i < d.n) ? d.mags[(size_t)(j0 + c) * d.ld + i] : 0.0;
+    };
     double sum = 0.0;
-    // The sum stays sequential in i; the column is loaded 16 entries ahead
-    // (16-byte loads: ld and the block starts are even).
-    constexpr int U = 16;
-    int i0 = 0;
-    for (; i0 + U <= d.n; i0 += U) {
-        double2 cv[U / 2];
+    load(0, cur);
+    for (int i0 = 0; i0 < d.n; i0 += 32) {
+        if (i0 + 32 < d.n) load(i0 + 32, nxt);
 #pragma unroll
-        for (int u = 0; u < U / 2; ++u) cv[u] = reinterpret_cast<const double2*>(col + i0)[u];
+        for (int c = 0; c < 32; ++c) tile[warp][c][lane] = cur[c];
+        rowv[warp][lane] = i0 + lane < d.n ? row[i0 + lane] : 0.0;
+        __syncwarp();
+        const int cnt = min(32, d.n - i0);
+        if (lane < ncol)
+            for (int r = 0; r < cnt; ++r) sum = add_rn(sum, mul_rn(rowv[warp][r], tile[warp][lane][r]));
+        __syncwarp();
 #pragma unroll
-        for (int u = 0; u < U / 2; ++u) {
-            sum = add_rn(sum, mul_rn(row[i0 + 2 * u], cv[u].x));
-            sum = add_rn(sum, mul_rn(row[i0 + 2 * u + 1], cv[u].y));
-        }
+        for (int c = 0; c < 32; ++c) cur[c] = nxt[c];
     }
-    for (int i = i0; i < d.n; ++i) sum = add_rn(sum, mul_rn(row[i], col[i]));
-    out[j] = sum;
+    if (lane < ncol) out[j0 + lane] = sum;
 }
 
 // ---- normest1 panel products ------------------------------------------------
@@ -645,9 +660,9 @@ std::vector<double> abs_power_batch(Context& ctx, const std::vector<const DMat*>
     if (cplx) moduli_kernel<true><<<g0, kThreads, 0, ctx.stream>>>(bc);
     else moduli_kernel<false><<<g0, kThreads, 0, ctx.stream>>>(bc);
     ctx.kernel_launches++;
-    dim3 g1((nmax + 127) / 128, bc.count);
+    dim3 g1((nmax + 32 * kChainWarps - 1) / (32 * kChainWarps), bc.count);
     for (int step = 0; step < p; ++step) {
-        abs_power_step_kernel<<<g1, 128, 0, ctx.stream>>>(bc, step & 1);
+        abs_power_step_kernel<<<g1, 32 * kChainWarps, 0, ctx.stream>>>(bc, step & 1);
         ctx.kernel_launches++;
     }
     Batch<SumDesc> bf = make_batch(ctx, folds);
