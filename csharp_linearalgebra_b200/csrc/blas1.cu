@@ -144,43 +144,23 @@ __global__ void pade_assemble_kernel(const __grid_constant__ Batch<PadeDesc> bt)
 
 // ---- norms ------------------------------------------------------------------
 
-constexpr int kSumWarps = 4;  // warps per CTA of the column-sum kernel, 32 columns each
-
-// One warp per 32 columns: each 32-row chunk of them is read by 32 coalesced
-// loads (one column each, a row per lane; the next chunk's loads issued
-// before this chunk is used), the moduli formed by the loading lanes,
-// transposed through shared memory, and lane c continues column c's sum over
-// the chunk's rows in order: one thread's sequential sum per column.
+// One warp per column: lanes load 32 consecutive entries (coalesced) and
+// form their moduli in parallel; the sum then takes them one by one in row
+// order (each broadcast by a shuffle), the same sequential sum as one thread
+// walking the column.
 template <bool CPLX>
-__global__ void __launch_bounds__(32 * kSumWarps) col_abs_sums_kernel(const __grid_constant__ Batch<SumDesc> b) {
+__global__ void col_abs_sums_kernel(const __grid_constant__ Batch<SumDesc> b) {
     const SumDesc& d = batch_item(b, blockIdx.y);
-    __shared__ double tile[kSumWarps][32][33];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int j0 = (blockIdx.x * kSumWarps + warp) * 32;
-    if (j0 >= d.n) return;  // the whole warp; only warp-level synchronisation below
-    const int ncol = min(32, d.n - j0);
-    double cur[32], nxt[32];
-    auto load = [&](int i0, double (&v)[32]) {
-        const int i = i0 + lane;
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-            v[c] = (c < ncol && i < d.m) ? mag(d.a + (size_t)(j0 + c) * d.ld * (CPLX ? 2 : 1), i, CPLX) : 0.0;
-    };
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= d.n) return;  // the whole warp
+    const double* col = d.a + (size_t)j * d.ld * (CPLX ? 2 : 1);
     double sum = 0.0;
-    load(0, cur);
     for (int i0 = 0; i0 < d.m; i0 += 32) {
-        if (i0 + 32 < d.m) load(i0 + 32, nxt);
-#pragma unroll
-        for (int c = 0; c < 32; ++c) tile[warp][c][lane] = cur[c];
-        __syncwarp();
+        const double v = i0 + lane < d.m ? mag(col, i0 + lane, CPLX) : 0.0;
         const int cnt = min(32, d.m - i0);
-        if (lane < ncol)
-            for (int r = 0; r < cnt; ++r) sum = add_rn(sum, tile[warp][lane][r]);
-        __syncwarp();
-#pragma unroll
-        for (int c = 0; c < 32; ++c) cur[c] = nxt[c];
+        for (int l = 0; l < cnt; ++l) sum = add_rn(sum, __shfl_sync(0xffffffffu, v, l));
     }
-    if (lane < ncol) d.out[j0 + lane] = sum;
+    if (lane == 0) d.out[j] = sum;
 }
 
 // One thread per row: sequential sum over columns in column order.
@@ -594,9 +574,9 @@ std::vector<double> norm1_batch(Context& ctx, const std::vector<const DMat*>& ma
         nmax = std::max(nmax, m->cols);
     }
     Batch<SumDesc> bs = make_batch(ctx, sums);
-    dim3 grid((nmax + 32 * kSumWarps - 1) / (32 * kSumWarps), bs.count);
-    if (cplx) col_abs_sums_kernel<true><<<grid, 32 * kSumWarps, 0, ctx.stream>>>(bs);
-    else col_abs_sums_kernel<false><<<grid, 32 * kSumWarps, 0, ctx.stream>>>(bs);
+    dim3 grid((nmax + 3) / 4, bs.count);  // 4 warps, one column each
+    if (cplx) col_abs_sums_kernel<true><<<grid, 128, 0, ctx.stream>>>(bs);
+    else col_abs_sums_kernel<false><<<grid, 128, 0, ctx.stream>>>(bs);
     Batch<SumDesc> bf = make_batch(ctx, folds);
     max_fold_kernel<<<bf.count, 256, 0, ctx.stream>>>(bf);
     TNS_CUDA(cudaGetLastError());
