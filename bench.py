@@ -564,8 +564,8 @@ def ours(args, world, rank, local, dist):
 
 
 def measured_hbm_peak():
-    """The copy bandwidth (GB/s) MEASURED_PEAKS.json holds, else this pool's
-    earlier measurement (6650 GB/s), with where it came from."""
+    """The copy bandwidth (GB/s) MEASURED_PEAKS.json holds, else 6650 GB/s (an
+    earlier copy-bandwidth measurement of a B200), with where it came from."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(path) as f:
@@ -575,7 +575,7 @@ def measured_hbm_peak():
                 return float(d[k]), "MEASURED_PEAKS.json " + k
     except (OSError, ValueError):
         pass
-    return 6650.0, "fallback 6650 GB/s (earlier measurement on this pool)"
+    return 6650.0, "fallback 6650 GB/s (an earlier B200 copy-bandwidth measurement)"
 
 
 def other_configurations(args, ws, torch, peak64, peak8, sweep):
