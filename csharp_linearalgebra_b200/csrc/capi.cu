@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <sstream>
@@ -568,11 +569,38 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             groups[g].push_back(i);
             load[g] += std::pow((double)orders[i], 3.0);
         }
-        auto run_group = [&](Context& wc, const std::vector<int>& idx) {
-            if (idx.empty()) return;
+        int nworkers = ngroups;
+        // Host inputs: the groups' copies in take turns (group w's after group
+        // w - 1's, ordered by an event), so that the first group computes
+        // while the others' matrices are still crossing instead of every
+        // group waiting for all the copies at once.
+        std::vector<cudaEvent_t> uploaded(nworkers, nullptr);
+        std::vector<char> recorded(nworkers, 0);
+        std::mutex turn_mu;
+        std::condition_variable turn_cv;
+        if (!dev && nworkers > 1)
+            for (auto& e : uploaded) TNS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        auto mark_recorded = [&](int w) {
+            std::lock_guard<std::mutex> g(turn_mu);
+            recorded[w] = 1;
+            turn_cv.notify_all();
+        };
+        auto run_group = [&](Context& wc, const std::vector<int>& idx, int w) {
+            const bool turns = !dev && nworkers > 1;
+            if (turns && w > 0) {
+                std::unique_lock<std::mutex> g(turn_mu);
+                turn_cv.wait(g, [&] { return recorded[w - 1] != 0; });
+                g.unlock();
+                TNS_CUDA(cudaStreamWaitEvent(wc.stream, uploaded[w - 1], 0));
+            }
             std::vector<DMat> in;
             in.reserve(idx.size());
             for (int i : idx) in.push_back(upload(wc, a[i], orders[i], orders[i], lda[i], true, dev, "a matrix to exponentiate"));
+            if (turns) {
+                TNS_CUDA(cudaEventRecord(uploaded[w], wc.stream));
+                mark_recorded(w);
+            }
+            if (idx.empty()) return;
             std::vector<const DMat*> ptrs;
             for (auto& m : in) ptrs.push_back(&m);
             std::vector<DMat> res;
@@ -585,7 +613,6 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             wc.sync();
         };
 
-        int nworkers = ngroups;
         while ((int)ctx.workers.size() < nworkers) ctx.workers.emplace_back(new Context(ctx.device));
         std::atomic<bool> stop{false};
         std::mutex mu;
@@ -600,7 +627,7 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             wc.concurrent = true;
             try {
                 TNS_CUDA(cudaSetDevice(ctx.device));
-                run_group(wc, groups[w]);
+                run_group(wc, groups[w], w);
                 check_device_flag(wc);
             } catch (const Error& e) {
                 std::lock_guard<std::mutex> g(mu);
@@ -620,14 +647,21 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
                 cudaStreamSynchronize(wc.stream);
             }
         };
+        // A worker that stops early still lets the next one take its turn.
+        auto worker_turn = [&](int w) {
+            worker(w);
+            mark_recorded(w);
+        };
         if (nworkers == 1) {
-            worker(0);
+            worker_turn(0);
         } else {
             std::vector<std::thread> threads;
             threads.reserve(nworkers);
-            for (int w = 0; w < nworkers; ++w) threads.emplace_back(worker, w);
+            for (int w = 0; w < nworkers; ++w) threads.emplace_back(worker_turn, w);
             for (auto& th : threads) th.join();
         }
+        for (auto& e : uploaded)
+            if (e) cudaEventDestroy(e);
         if (err_code != TNS_OK) fail(err_code, err_msg);
         if (infos)
             for (int i = 0; i < count; ++i) infos[i] = results[i];
