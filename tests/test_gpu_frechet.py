@@ -4,9 +4,9 @@ L(A, E) of exp and the gradient of ||exp(tA) B - Y||_F^2.
 Oracles:
   - the reference's way to L(A, E): the upper right block of its Expm of
     [[A, E], [0, A]]. At small orders that is the oracle's Expm (pinned in
-    test_frechet_pins.py); at the differentiation configuration's orders it
-    is the library's plain Expm of the block, which repeats the reference's
-    Expm arithmetic bit for bit (test_gpu_expm.py);
+    test_frechet_pins.py); at the differentiation configuration's n = 1024 it
+    is the library's plain Expm of the 2048-order block, itself checked equal
+    to the oracle's Expm of that block bit for bit;
   - central finite differences, fourth order,
         dF ~ (-F(2h) + 8 F(h) - 8 F(-h) + F(-2h)) / (12 h),
     in unit-1-norm directions with h = 1e-3 to 3e-3, each F from the exact
@@ -139,9 +139,11 @@ def test_frechet_finite_differences(ws):
     assert rel(l, fd) <= TOL_FD
 
 
-def test_frechet_block_n1024(ws):
+def test_frechet_block_n1024(ws, orc):
     """L(A, E) at n = 1024 (the differentiation configuration's Frechet case),
-    A as in the batching sweep at w = 1e4, E random."""
+    A as in the batching sweep at w = 1e4, E random. The block Expm it is
+    checked against is first checked against the oracle's Expm of the same
+    2048-order block, bit for bit (the reference's own route to L)."""
     from csharp_linearalgebra_b200 import ExpmDiagnostics
     rng = np.random.default_rng(1024)
     a = sweep_operator(rng, 1024, 1e4)
@@ -149,6 +151,14 @@ def test_frechet_block_n1024(ws):
     d = ExpmDiagnostics()
     x, l = ws.expm_frechet(a, e, d)
     lb = gpu_block_frechet(ws, a, e)
+    n = a.shape[0]
+    scale = np.abs(e).sum(axis=0).max()
+    blk = np.zeros((2 * n, 2 * n), dtype=np.complex128, order="F")
+    blk[:n, :n] = a
+    blk[:n, n:] = e / scale
+    blk[n:, n:] = a
+    ref, _ = orc.expm(blk)
+    assert np.array_equal(ref[:n, n:] * scale, lb)
     print(f"Frechet n=1024 (s={d.squarings}) vs block Expm: {rel(l, lb):.2e}; exp vs Expm {rel(x, ws.expm(a)):.2e}")
     assert rel(l, lb) <= TOL_BLOCK
     assert rel(x, ws.expm(a)) <= TOL_BLOCK
