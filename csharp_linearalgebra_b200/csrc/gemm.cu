@@ -28,6 +28,12 @@
 //    consecutive rows of column-major C and the epilogue moves 16-byte pairs.
 //  - Persistent CTAs walk a list of problems (grouped GEMM): the same kernel
 //    serves one product, or every matrix of a batch in one launch.
+//  - A single product with fewer tiles than SMs and several KC slabs (1024^3:
+//    64 tiles of 128 x 128, four slabs) is slab-split: every (tile, slab,
+//    pass) is a unit of its own, writes its raw slab product to a plane, and
+//    a fold kernel adds the planes into C in slab order. Each slab's
+//    accumulation starts from zero in both forms, so the split changes which
+//    CTA computes a slab, not the operations, and C gets the same bits.
 //  - Every wait is bounded (device_util.cuh): a stuck pipeline records an error
 //    in the context flag and the kernel returns.
 //
@@ -45,6 +51,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <functional>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -124,7 +131,60 @@ struct GemmLaunch {
     int* err;
 };
 
-template <class Cfg>
+// Combine (ComplexKernels.cs:213-240): alpha (P + iQ) + beta C with the
+// reference's special cases for unit and real alpha, zero and unit beta. C is
+// read only when beta is nonzero.
+__device__ __forceinline__ double2 combine_4m(double2 pq, double ar, double ai, double br, double bi,
+                                              const double2* c_at) {
+    const bool unit_alpha = (ar == 1.0 && ai == 0.0);
+    const bool real_alpha = (ai == 0.0);
+    const bool zero_beta = (br == 0.0 && bi == 0.0);
+    const bool unit_beta = (br == 1.0 && bi == 0.0);
+    double pr, pi;
+    if (unit_alpha) {
+        pr = pq.x;
+        pi = pq.y;
+    } else if (real_alpha) {
+        pr = mul_rn(ar, pq.x);
+        pi = mul_rn(ar, pq.y);
+    } else {
+        pr = sub_rn(mul_rn(ar, pq.x), mul_rn(ai, pq.y));
+        pi = add_rn(mul_rn(ai, pq.x), mul_rn(ar, pq.y));
+    }
+    if (zero_beta) return make_double2(pr, pi);
+    const double2 c = *c_at;
+    if (unit_beta) return make_double2(add_rn(c.x, pr), add_rn(c.y, pi));
+    const double cr = sub_rn(mul_rn(br, c.x), mul_rn(bi, c.y));
+    const double ci = add_rn(mul_rn(bi, c.x), mul_rn(br, c.y));
+    return make_double2(add_rn(cr, pr), add_rn(ci, pi));
+}
+
+// The k-range of one unit of work. Unsplit, a unit is a tile: all of K, every
+// pass. Slab-split (SPLIT), a unit is one tile's one KC slab of one pass, and
+// the units of a problem are numbered pass-major, then slab, then tile.
+struct UnitRange {
+    int local;  // the tile within its problem
+    int part;   // pass * slabs + slab (slab-split), else 0
+    int kt0;    // first k-step
+    int iters;  // k-steps the unit runs (all passes' when unsplit)
+};
+
+template <bool SPLIT, int PASSES>
+__device__ __forceinline__ UnitRange unit_range(const GemmProblem& P, int local, int bk) {
+    const int nk = P.K / bk;
+    UnitRange u{local, 0, 0, nk * PASSES};
+    if constexpr (SPLIT) {
+        const int tiles = P.tiles_m * P.tiles_n;
+        const int slab_kt = P.kc / bk;
+        u.part = local / tiles;
+        u.local = local - u.part * tiles;
+        u.kt0 = (u.part % P.slabs) * slab_kt;
+        u.iters = min(nk - u.kt0, slab_kt);
+    }
+    return u;
+}
+
+template <class Cfg, bool SPLIT>
 __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid_constant__ GemmLaunch L) {
     using E = typename std::conditional<Cfg::kComplex, double2, double>::type;
     constexpr int PASSES = Cfg::kComplex ? 2 : 1;
@@ -213,12 +273,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
                 tensormap_acquire(ma);
                 tensormap_acquire(mb);
             }
-            int local = tile - P.tile_begin;
-            int m0 = (local % P.tiles_m) * Cfg::BM;
-            int n0 = (local / P.tiles_m) * Cfg::BN;
+            const UnitRange u = unit_range<SPLIT, PASSES>(P, tile - P.tile_begin, Cfg::BK);
+            int m0 = (u.local % P.tiles_m) * Cfg::BM;
+            int n0 = (u.local / P.tiles_m) * Cfg::BN;
             const int nk = P.K / Cfg::BK;
-            for (int q = 0; q < nk * PASSES; ++q, ++it) {
-                const int k0 = (q % nk) * Cfg::BK;
+            for (int q = 0; q < u.iters; ++q, ++it) {
+                const int k0 = (SPLIT ? u.kt0 + q : q % nk) * Cfg::BK;
                 int s = it % Cfg::STAGES;
                 uint32_t round = it / Cfg::STAGES;
                 if (!mbar_wait_bounded(&empty[s], (round & 1) ^ 1, err, kDevTimeoutEmpty)) {
@@ -263,9 +323,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
         const int tile = tile_slot[it % Cfg::STAGES];
         if (tile < 0) break;
         const GemmProblem& P = probs[find_problem(probs, nprob, tile)];
-        int local = tile - P.tile_begin;
-        const int m0 = (local % P.tiles_m) * Cfg::BM;
-        const int n0 = (local / P.tiles_m) * Cfg::BN;
+        const UnitRange u = unit_range<SPLIT, PASSES>(P, tile - P.tile_begin, Cfg::BK);
+        const int m0 = (u.local % P.tiles_m) * Cfg::BM;
+        const int n0 = (u.local / P.tiles_m) * Cfg::BN;
         const int nk = P.K / Cfg::BK;
         const int slab = P.kc / Cfg::BK;  // k-tiles per KC slab
         const double ar = P.alpha_re, ai = P.alpha_im, br = P.beta_re, bi = P.beta_im;
@@ -286,9 +346,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
         };
         zero_acc();
 
-        for (int q = 0; q < nk * PASSES; ++q, ++it) {
-            const int pass = q / nk;
-            const int kt = q % nk;
+        for (int q = 0; q < u.iters; ++q, ++it) {
+            const int pass = SPLIT ? u.part / P.slabs : q / nk;
+            const int kt = SPLIT ? u.kt0 + q : q % nk;
             int s = it % Cfg::STAGES;
             if (q > 0 && !mbar_wait_bounded(&full[s], (it / Cfg::STAGES) & 1, err, kDevTimeoutFull)) return;
             const E* As = stage_a(s) + (wm * Cfg::WM / Cfg::A_BOX_ROWS) * Cfg::A_BOX +
@@ -337,6 +397,36 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
             else mma_step(std::integral_constant<int, 1>{});
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
+
+            if constexpr (SPLIT) {
+                // The unit's slab ends here: its raw product goes to the
+                // unit's plane (complex: P and Q of this pass side by side).
+                if (q + 1 < u.iters) continue;
+                const size_t at0 = (size_t)u.part * P.M * P.N;
+#pragma unroll
+                for (int i = 0; i < Cfg::NF; ++i)
+#pragma unroll
+                    for (int j = 0; j < Cfg::MF; ++j) {
+                        const int m = m0 + wm * Cfg::WM + j * 8 + 2 * t;
+                        if (m >= P.M) continue;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int n = n0 + wn * Cfg::WN + i * 16 + g + 8 * h;
+                            if (n >= P.N) continue;
+                            const size_t at = at0 + (size_t)n * P.M + m;
+                            if constexpr (Cfg::kComplex) {
+                                double2* dst = reinterpret_cast<double2*>(P.S) + at;
+                                dst[0] = make_double2(acc0[i][j][2 * h], acc1[i][j][2 * h]);
+                                dst[1] = make_double2(acc0[i][j][2 * h + 1], acc1[i][j][2 * h + 1]);
+                            } else {
+                                *reinterpret_cast<double2*>(reinterpret_cast<double*>(P.S) + at) =
+                                    make_double2(acc0[i][j][2 * h], acc0[i][j][2 * h + 1]);
+                            }
+                        }
+                    }
+                zero_acc();
+                continue;
+            }
 
             const bool slab_end = ((kt + 1) % slab == 0) || (kt + 1 == nk);
             if (!slab_end) continue;
@@ -405,7 +495,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
                                     W[e] = pq;
                                     continue;
                                 }
-                                // Combine (ComplexKernels.cs:213-240).
+                                // Combine (ComplexKernels.cs:213-240): combine_4m written
+                                // out, which in this kernel compiles without the spills
+                                // the call form measured under ptxas.
                                 const bool unit_alpha = (ar == 1.0 && ai == 0.0);
                                 const bool real_alpha = (ai == 0.0);
                                 const bool zero_beta = (br == 0.0 && bi == 0.0);
@@ -445,6 +537,45 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1) gemm_dmma_kernel(const __grid
     }
 }
 
+// Folds a slab-split product's planes into C in slab order, with the same
+// operations the unsplit kernel applies at each slab end, so C gets the same
+// bits. Real: C scaled by beta (ScaleC, Gemm.cs:187-203), then
+// c = fma(alpha, slab, c) slab by slab. Complex: P and Q summed over pass 0's
+// slabs from zero, pass 1's folded in (P -= Ai*Bi, Q += Ai*Br), then Combine.
+// One thread per element, consecutive threads on consecutive rows.
+template <bool CPLX>
+__global__ void __launch_bounds__(256) slab_fold_kernel(const __grid_constant__ GemmProblem p) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = blockIdx.y;
+    if (m >= p.M) return;
+    const size_t plane = (size_t)p.M * p.N;
+    const size_t at = (size_t)n * p.M + m;
+    if constexpr (!CPLX) {
+        double* c = reinterpret_cast<double*>(p.C) + (size_t)n * p.ldc + m;
+        double x = 0.0;  // beta == 0 overwrites
+        if (p.beta_re != 0.0) {
+            x = *c;
+            if (p.beta_re != 1.0) x = mul_rn(x, p.beta_re);
+        }
+        const double* s = reinterpret_cast<const double*>(p.S) + at;
+        for (int k = 0; k < p.slabs; ++k) x = fma(p.alpha_re, s[k * plane], x);
+        *c = x;
+    } else {
+        const double2* s = reinterpret_cast<const double2*>(p.S) + at;
+        double2 pq = make_double2(0.0, 0.0);
+        for (int k = 0; k < p.slabs; ++k) {
+            const double2 v = s[k * plane];
+            pq = make_double2(fma(1.0, v.x, pq.x), fma(1.0, v.y, pq.y));
+        }
+        for (int k = p.slabs; k < 2 * p.slabs; ++k) {
+            const double2 v = s[k * plane];
+            pq = make_double2(fma(-1.0, v.x, pq.x), fma(1.0, v.y, pq.y));
+        }
+        double2* c = reinterpret_cast<double2*>(p.C) + (size_t)n * p.ldc + m;
+        *c = combine_4m(pq, p.alpha_re, p.alpha_im, p.beta_re, p.beta_im, c);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -459,11 +590,11 @@ using CplxSmall = GemmCfg<true, 2, 2, 4>;   // 64 x 64 tiles, 4 math warps
 // The math warpgroups' register increase can only be met when the kernel is
 // launched with exactly the allocation the split assumes; with any other
 // allocation they would wait forever, so such a build is refused.
-template <class Cfg>
+template <class Cfg, bool SPLIT>
 void check_register_split() {
     if constexpr (Cfg::kSplitRegs) {
         cudaFuncAttributes fa{};
-        TNS_CUDA(cudaFuncGetAttributes(&fa, gemm_dmma_kernel<Cfg>));
+        TNS_CUDA(cudaFuncGetAttributes(&fa, gemm_dmma_kernel<Cfg, SPLIT>));
         if (fa.numRegs != Cfg::kLaunchRegs)
             fail(TNS_E_DEVICE, "GEMM kernel built with " + std::to_string(fa.numRegs) +
                                    " registers per thread; its register split needs " +
@@ -507,13 +638,17 @@ GemmMaps encode_maps(const GemmProblem& p) {
     return m;
 }
 
-template <class Cfg>
-void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
+// One launch of configuration Cfg over `probs`. SPLIT: every problem carries
+// its slab planes (S, slabs) and `tail` enqueues the fold that follows the
+// kernel, inside the launch's timing events.
+template <class Cfg, bool SPLIT = false>
+void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs, const std::function<void()>& tail = {}) {
     static std::atomic<bool> configured[64];
     int dev = ctx.device;
     if (!configured[dev].load(std::memory_order_acquire)) {
-        TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
-        check_register_split<Cfg>();
+        TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      Cfg::SMEM));
+        check_register_split<Cfg, SPLIT>();
         configured[dev].store(true, std::memory_order_release);
     }
     int total = 0;
@@ -521,7 +656,7 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
         p.tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM;
         p.tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
         p.tile_begin = total;
-        total += p.tiles_m * p.tiles_n;
+        total += p.tiles_m * p.tiles_n * (SPLIT ? p.slabs * (Cfg::kComplex ? 2 : 1) : 1);
     }
     if (total == 0) return;
     GemmLaunch L{};
@@ -544,7 +679,8 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
         L.maps_list = static_cast<const GemmMaps*>(ctx.upload(maps.data(), sizeof(GemmMaps) * maps.size()));
     }
     int ctas_per_sm = 1;
-    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg, SPLIT>, Cfg::THREADS,
+                                                           Cfg::SMEM));
     int grid = std::min(total, std::max(1, ctas_per_sm) * ctx.num_sms);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ctx.timing) {
@@ -552,10 +688,11 @@ void launch_cfg(Context& ctx, std::vector<GemmProblem>& probs) {
         e1 = ctx.take_event();
         TNS_CUDA(cudaEventRecord(e0, ctx.stream));
     }
-    gemm_dmma_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, ctx.stream>>>(L);
+    gemm_dmma_kernel<Cfg, SPLIT><<<grid, Cfg::THREADS, Cfg::SMEM, ctx.stream>>>(L);
     TNS_CUDA(cudaGetLastError());
     ctx.kernel_launches++;
     ctx.gemm_launches++;
+    if (tail) tail();
     for (auto& p : probs) {
         ctx.gemm_flops += (Cfg::kComplex ? 8.0 : 2.0) * (double)(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
         const bool reads_c = p.beta_re != 0.0 || p.beta_im != 0.0;
@@ -581,10 +718,44 @@ void check_problem(const GemmProblem& p, bool cplx) {
 
 }  // namespace
 
-void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
+namespace {
+
+// Slab planes of a slab-split product stay below this size.
+constexpr size_t kSlabPlaneBytes = size_t(512) << 20;
+
+// One product whose tiles leave SMs idle and whose K spans several KC slabs:
+// each tile's slabs (and passes) run as separate units, so more CTAs work at
+// once, each unit's raw slab product goes to its own plane, and a fold kernel
+// adds the slabs into C in slab order with the operations the unsplit kernel
+// applies at each slab end (the same bits). False when the split does not
+// apply.
+template <class Big, class Small>
+bool slab_split_launch(Context& ctx, const GemmProblem& p0, long long tiles_big) {
+    constexpr bool CPLX = Big::kComplex;
+    constexpr int passes = CPLX ? 2 : 1;
+    const int slabs = (p0.K + p0.kc - 1) / p0.kc;
+    const size_t bytes = (size_t)passes * slabs * p0.M * p0.N * Big::ESZ;
+    if (slabs < 2 || tiles_big >= ctx.num_sms || bytes > kSlabPlaneBytes) return false;
+    DBuf planes(ctx, bytes);
+    GemmProblem p = p0;
+    p.S = planes.p;
+    p.slabs = slabs;
+    p.W = nullptr;
+    p.ldw = 0;
+    std::vector<GemmProblem> v{p};
+    auto fold = [&] {
+        slab_fold_kernel<CPLX><<<dim3((p.M + 255) / 256, p.N), 256, 0, ctx.stream>>>(p);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+    };
+    if (tiles_big * slabs * passes >= ctx.num_sms) launch_cfg<Big, true>(ctx, v, fold);
+    else launch_cfg<Small, true>(ctx, v, fold);
+    return true;
+}
+
+void gemm_run(Context& ctx, std::vector<GemmProblem>& probs, bool cplx, bool slab_split) {
     std::vector<GemmProblem> work;
     work.reserve(probs.size());
-    std::vector<DBuf> scratch;
     for (auto& p0 : probs) {
         GemmProblem p = p0;
         if (p.kc <= 0) p.kc = reference_kc(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
@@ -594,12 +765,6 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
             // No product: C := beta*C.
             scale_inplace(ctx, p.C, p.M, p.N, p.ldc, cplx, p.beta_re, p.beta_im);
             continue;
-        }
-        if (cplx && !p.W && !(p.alpha_re == 1.0 && p.alpha_im == 0.0 && p.beta_re == 0.0 && p.beta_im == 0.0)) {
-            // P + iQ need their own storage when the combine is not a plain copy.
-            scratch.emplace_back(ctx, (size_t)p.M * p.N * 16);
-            p.W = scratch.back().p;
-            p.ldw = p.M;
         }
         work.push_back(p);
     }
@@ -616,6 +781,20 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
                       : (long long)((p.M + RealBig::BM - 1) / RealBig::BM) * ((p.N + RealBig::BN - 1) / RealBig::BN);
         depth = std::max(depth, p.K);
         if (p.beta_re != 0.0 || p.beta_im != 0.0) overwrite = false;
+    }
+    if (slab_split && work.size() == 1 &&
+        (cplx ? slab_split_launch<CplxBig, CplxSmall>(ctx, work[0], tiles)
+              : slab_split_launch<RealBig, RealSmall>(ctx, work[0], tiles)))
+        return;
+    std::vector<DBuf> scratch;
+    scratch.reserve(work.size());
+    for (auto& p : work) {
+        if (cplx && !p.W && !(p.alpha_re == 1.0 && p.alpha_im == 0.0 && p.beta_re == 0.0 && p.beta_im == 0.0)) {
+            // P + iQ need their own storage when the combine is not a plain copy.
+            scratch.emplace_back(ctx, (size_t)p.M * p.N * 16);
+            p.W = scratch.back().p;
+            p.ldw = p.M;
+        }
     }
     auto run = [&](int big) {
         if (cplx) big ? launch_cfg<CplxBig>(ctx, work) : launch_cfg<CplxSmall>(ctx, work);
@@ -638,16 +817,22 @@ void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) {
     run(variant);
 }
 
+}  // namespace
+
+void gemm_grouped(Context& ctx, std::vector<GemmProblem>& probs, bool cplx) { gemm_run(ctx, probs, cplx, false); }
+
+// One product through the public entry points: slab-split when its tiles
+// alone would leave SMs idle.
 void gemm(Context& ctx, const GemmProblem& p, bool cplx) {
     std::vector<GemmProblem> v{p};
-    gemm_grouped(ctx, v, cplx);
+    gemm_run(ctx, v, cplx, true);
 }
 
 namespace {
 template <class Cfg>
 void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p) {
-    TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
-    check_register_split<Cfg>();
+    TNS_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+    check_register_split<Cfg, false>();
     p.tiles_m = (p.M + Cfg::BM - 1) / Cfg::BM;
     p.tiles_n = (p.N + Cfg::BN - 1) / Cfg::BN;
     p.tile_begin = 0;
@@ -663,9 +848,10 @@ void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p
     L.err = d_err;
     L.tiles = nullptr;  // no counter without a context: static round robin
     int ctas_per_sm = 1;
-    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg>, Cfg::THREADS, Cfg::SMEM));
+    TNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, gemm_dmma_kernel<Cfg, false>, Cfg::THREADS,
+                                                           Cfg::SMEM));
     int grid = std::min(total, std::max(1, ctas_per_sm) * num_sms);
-    gemm_dmma_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(L);
+    gemm_dmma_kernel<Cfg, false><<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(L);
     TNS_CUDA(cudaGetLastError());
 }
 }  // namespace

@@ -1,7 +1,8 @@
 // Fifth-generation tensor core (tcgen05) primitives for sm_100a: tensor
 // memory (TMEM) allocation, the single-thread MMA issue with shared-memory
 // operand descriptors, commits to mbarriers, and TMEM <-> register moves.
-// Only the forms the split-precision GEMM uses (cta_group::1, kind::i8).
+// Only the forms the split-precision GEMM uses: kind::i8, on one CTA
+// (cta_group::1) or on a CTA pair (cta_group::2).
 #pragma once
 
 #include <cstdint>

@@ -58,6 +58,11 @@ struct GemmProblem {
     void* W;
     int ldw;
     long long work;  // m*n*k of the unpadded product, for the KC rule
+    // Slab-split launches only (one product whose tiles leave SMs idle): each
+    // KC slab's raw product (per pass, complex) lands in its own M x N plane
+    // of S, and a fold kernel adds the slabs into C in slab order.
+    void* S;
+    int slabs;
 };
 
 // The reference's KC rule (GemmDispatch.cs:45,109; Gemm.cs:62; ParallelGemm):

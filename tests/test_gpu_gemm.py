@@ -92,3 +92,49 @@ def test_4m_keeps_small_imaginary_parts(ws, orc):
     c = ws.multiply(ar + 1j * ai, br + 1j * bi)
     im_exact = ar @ bi + ai @ br
     assert np.linalg.norm(c.imag - im_exact) / np.linalg.norm(im_exact) < 1e-13
+
+
+# A single product whose tiles leave SMs idle and whose K spans several KC
+# slabs runs slab-split: one unit per (tile, slab, pass), each slab's raw
+# product to its own plane, then a fold into C in slab order. These shapes take
+# that route with both tile sizes and ragged last slabs (K = 704: 256 + 256 +
+# 192; K = 528: 256 + 256 + 16; K = 4096: sixteen slabs of one tile).
+SLAB_SPLIT_REAL = [((520, 390, 700), 1.0, 0.0), ((520, 390, 700), 2.5, -0.5), ((520, 390, 700), -1.0, 1.0),
+                   ((64, 64, 4096), 1.0, 0.0), ((1030, 900, 520), 0.75, 1.0)]
+
+
+@pytest.mark.parametrize("shape,alpha,beta", SLAB_SPLIT_REAL)
+def test_dgemm_slab_split_matches_oracle(ws, orc, shape, alpha, beta):
+    m, n, k = shape
+    rng = np.random.default_rng(m + n + k)
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    c0 = rng.uniform(-1, 1, (m, n))
+    c = ws.multiply(a, b, c0, alpha, beta)
+    assert np.array_equal(c, orc.gemm(a, b, c0, alpha, beta))
+
+
+def test_dgemm_slab_split_beta_zero_overwrites_nan(ws, orc):
+    rng = np.random.default_rng(5)
+    a = rng.uniform(-1, 1, (300, 600))
+    b = rng.uniform(-1, 1, (600, 250))
+    c0 = np.full((300, 250), np.nan)
+    c = ws.multiply(a, b, c0, 1.5, 0.0)
+    assert not np.isnan(c).any()
+    assert np.array_equal(c, orc.gemm(a, b, c0, 1.5, 0.0))
+
+
+SLAB_SPLIT_COMPLEX = [((300, 200, 600), 1.0, 0.0), ((300, 200, 600), 2.0 - 1.0j, 0.5 + 0.25j),
+                      ((300, 200, 600), 1.0, 1.0), ((300, 200, 600), -0.5, 0.0),
+                      ((768, 640, 520), 2.0 - 1.0j, 0.5 + 0.25j), ((1024, 1024, 1024), 1.0, 0.0)]
+
+
+@pytest.mark.parametrize("shape,alpha,beta", SLAB_SPLIT_COMPLEX)
+def test_zgemm_slab_split_matches_oracle(ws, orc, shape, alpha, beta):
+    m, n, k = shape
+    rng = np.random.default_rng(m * n + k)
+    a = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    c0 = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    c = ws.multiply(a, b, c0, complex(alpha), complex(beta))
+    assert np.array_equal(c, orc.gemm(a, b, c0, complex(alpha), complex(beta)))
