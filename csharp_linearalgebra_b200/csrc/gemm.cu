@@ -859,7 +859,8 @@ void launch_detached(cudaStream_t stream, int num_sms, int* d_err, GemmProblem p
 // One complex product launched on a caller's stream without a context: the
 // problem's operands and its P + iQ workspace (W) are the caller's, nothing is
 // allocated and nothing is uploaded (the problem travels in the launch
-// parameters). Same kernel, tiles and KC rule as gemm().
+// parameters). Same kernel, tiles and KC rule as gemm(), always unsplit (a
+// slab split's planes would need storage); the bits are the same either way.
 void gemm_detached_complex(cudaStream_t stream, int device, int* d_err, const GemmProblem& p0) {
     GemmProblem p = p0;
     if (p.kc <= 0) p.kc = reference_kc(p.work > 0 ? p.work : (long long)p.M * p.N * p.K);
