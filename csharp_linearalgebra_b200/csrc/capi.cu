@@ -526,6 +526,16 @@ int expmv_operator_entry(tns_context* c, bool cplx, int n, tns_apply_fn apply, v
     });
 }
 
+// True for page-locked host memory (cudaHostAlloc / cudaHostRegister).
+bool host_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
 int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, const double* const* a, const int* lda,
                         double* const* out, const int* ldo, tns_expm_info* infos) {
     return guarded(c, [&](Context& ctx) {
@@ -605,11 +615,42 @@ int zexpm_batched_entry(tns_context* c, bool dev, int count, const int* orders, 
             for (auto& m : in) ptrs.push_back(&m);
             std::vector<DMat> res;
             std::vector<tns::ExpmInfo> infs;
-            tns::expm_batch(wc, ptrs, res, infs);
-            for (size_t k = 0; k < idx.size(); ++k) {
-                tns::copy_out(wc, res[k], out[idx[k]], ldo[idx[k]], dev);
-                results[idx[k]] = tns_expm_info{infs[k].degree, infs[k].squarings};
+            const bool early = !dev && std::all_of(idx.begin(), idx.end(), [&](int i) { return host_pinned(out[i]); });
+            if (!early) {
+                tns::expm_batch(wc, ptrs, res, infs);
+                for (size_t k = 0; k < idx.size(); ++k) tns::copy_out(wc, res[k], out[idx[k]], ldo[idx[k]], dev);
+            } else {
+                // Pinned host outputs: each result crosses to the host on the
+                // copy stream as soon as it is final, while the group's other
+                // matrices still square. (A copy into pageable memory would
+                // hold this thread until the copy ran, so those results go at
+                // the end.) The results outlive the fence, whose destructor,
+                // on every path, orders their frees on the group's stream
+                // after the copies.
+                std::vector<DMat> finished(idx.size());
+                cudaStream_t cs = wc.copies();
+                cudaEvent_t ready = nullptr;
+                TNS_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+                struct CopyFence {
+                    Context& wc;
+                    cudaStream_t cs;
+                    cudaEvent_t ev;
+                    ~CopyFence() {
+                        cudaEventRecord(ev, cs);
+                        cudaStreamWaitEvent(wc.stream, ev, 0);
+                        cudaStreamSynchronize(wc.stream);
+                        cudaEventDestroy(ev);
+                    }
+                } fence{wc, cs, ready};
+                tns::expm_batch(wc, ptrs, res, infs, [&](size_t k, DMat&& r) {
+                    finished[k] = std::move(r);
+                    TNS_CUDA(cudaEventRecord(ready, wc.stream));
+                    TNS_CUDA(cudaStreamWaitEvent(cs, ready, 0));
+                    tns::copy_out_on(cs, finished[k], out[idx[k]], ldo[idx[k]], false);
+                });
             }
+            for (size_t k = 0; k < idx.size(); ++k)
+                results[idx[k]] = tns_expm_info{infs[k].degree, infs[k].squarings};
             wc.sync();
         };
 

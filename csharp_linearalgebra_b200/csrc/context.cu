@@ -81,7 +81,16 @@ Context::~Context() {
     if (d_ring) cudaFree(d_ring);
     if (d_err) cudaFree(d_err);
     if (d_tiles) cudaFree(d_tiles);
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+    }
     if (stream) cudaStreamDestroy(stream);
+}
+
+cudaStream_t Context::copies() {
+    if (!copy_stream) TNS_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    return copy_stream;
 }
 
 const void* Context::upload(const void* src, size_t bytes) {
@@ -221,11 +230,15 @@ void copy_in(Context& ctx, DMat& dst, const double* src, int ld, bool src_on_dev
                                src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx.stream));
 }
 
-void copy_out(Context& ctx, const DMat& src, double* dst, int ld, bool dst_on_device) {
+void copy_out_on(cudaStream_t stream, const DMat& src, double* dst, int ld, bool dst_on_device) {
     if (src.rows == 0 || src.cols == 0) return;
     size_t esz = src.esz();
     TNS_CUDA(cudaMemcpy2DAsync(dst, (size_t)ld * esz, src.p, (size_t)src.ld() * esz, (size_t)src.rows * esz, src.cols,
-                               dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx.stream));
+                               dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+}
+
+void copy_out(Context& ctx, const DMat& src, double* dst, int ld, bool dst_on_device) {
+    copy_out_on(ctx.stream, src, dst, ld, dst_on_device);
 }
 
 void copy_dmat(Context& ctx, DMat& dst, const DMat& src) {

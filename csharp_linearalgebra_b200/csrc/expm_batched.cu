@@ -201,7 +201,7 @@ std::vector<double> power_norm_estimates(Context& ctx, const std::vector<const D
 }
 
 void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,
-                std::vector<ExpmInfo>& infos) {
+                std::vector<ExpmInfo>& infos, const std::function<void(size_t, DMat&&)>& on_final) {
     const size_t cnt = inputs.size();
     results.clear();
     results.resize(cnt);
@@ -520,6 +520,13 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
                                          ", which indicates a non-finite input rather than a property of the algorithm.");
         getrs_batch(ctx, solves, false);
     }
+    // A result is final after the solve (s = 0) or after its last squaring.
+    auto hand_over = [&](int s_done) {
+        if (!on_final) return;
+        for (size_t k = 0; k < cnt; ++k)
+            if (jobs[k].s == s_done) on_final(k, std::move(num[k]));
+    };
+    hand_over(0);
     // Squarings (:262-267): round r squares every matrix with s > r.
     {
         std::vector<DMat> sq(cnt);
@@ -538,6 +545,7 @@ void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vecto
             product_batch(ctx, ab, c, 0.0, Form::kSplittable);
             for (size_t k = 0; k < cnt; ++k)
                 if (jobs[k].s > r) std::swap(num[k], sq[k]);
+            hand_over(r + 1);
         }
     }
     for (size_t k = 0; k < cnt; ++k) {

@@ -133,6 +133,11 @@ struct Context {
     double lu_panel_ms = 0.0, lu_swaps_ms = 0.0, lu_triangular_ms = 0.0, lu_gemm_ms = 0.0, lu_total_ms = 0.0;
     long long lu_block_steps = 0, lu_factorizations = 0;
 
+    // A second stream for copies of finished results that overlap the work
+    // still running on `stream` (created on first use).
+    cudaStream_t copy_stream = nullptr;
+    cudaStream_t copies();
+
     // Batched work runs on worker contexts (one host thread and one stream
     // each), created on first use, so that independent matrices overlap on
     // the GPU. Their counters are summed into this context's statistics.
@@ -200,6 +205,8 @@ void selftest_wait(Context& ctx, long long limit_ns);
 // elements) into / out of a padded device matrix.
 void copy_in(Context& ctx, DMat& dst, const double* src, int ld, bool src_on_device);
 void copy_out(Context& ctx, const DMat& src, double* dst, int ld, bool dst_on_device);
+// The same on another stream (the caller orders it after the producer).
+void copy_out_on(cudaStream_t stream, const DMat& src, double* dst, int ld, bool dst_on_device);
 void copy_dmat(Context& ctx, DMat& dst, const DMat& src);
 
 // ---- GEMM (gemm.cu) --------------------------------------------------------
@@ -383,8 +390,12 @@ struct ExpmInfo {
 // result := exp(a) for the valid n x n block (n >= 2).
 void expm(Context& ctx, const DMat& a, DMat& result, ExpmInfo* info);
 // The same for a batch of matrices of any orders >= 2, one launch per phase.
+// With `on_final`, each matrix's result is handed over (moved out, its slot in
+// `results` left empty) as soon as it is final -- after the Pade solve for
+// s = 0, else after its last squaring -- while the others still square; the
+// result is complete once the context's stream reaches the point of the call.
 void expm_batch(Context& ctx, const std::vector<const DMat*>& inputs, std::vector<DMat>& results,
-                std::vector<ExpmInfo>& infos);
+                std::vector<ExpmInfo>& infos, const std::function<void(size_t, DMat&&)>& on_final = {});
 
 struct ExpmvInfo {
     int degree = 0, scaling = 0, applications = 0, early_exits = 0;

@@ -236,7 +236,9 @@ int tns_zexpm(tns_context* ctx, int n, const double* a, int lda, double* out, in
 /* A batch of complex exponentials of independent orders: out[i] = exp(a[i]).
  * The frequency-sweep form of the same algorithm; every decision per matrix
  * is the one tns_zexpm takes. Host pointers (synchronous) or, for
- * _device, device pointers. infos may be NULL. */
+ * _device, device pointers. infos may be NULL. With page-locked host outputs
+ * each result is copied out as soon as it is final, while the other matrices
+ * are still being computed; pageable outputs are copied at the end. */
 int tns_zexpm_batched(tns_context* ctx, int count, const int* orders, const double* const* a,
                       const int* lda, double* const* out, const int* ldo, tns_expm_info* infos);
 int tns_zexpm_batched_device(tns_context* ctx, int count, const int* orders, const double* const* a,
