@@ -29,6 +29,7 @@
 #include "tns_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <vector>
@@ -1403,11 +1404,175 @@ __global__ void __launch_bounds__(64) left_subst_cplx_unit_back_kernel(const dou
     }
 }
 
+// The same two solves with the right-hand sides and the factor in shared
+// memory, for the orders that fit: one warp per pair of right-hand sides (a
+// half-warp each, both on the same row at each step), the pair's columns kept
+// in shared memory, and the factor column a step reads (with its diagonal)
+// copied in by cp.async two steps ahead into one of three slots. A step then
+// reads nothing from global memory, and its sums are the kernels' above,
+// term for term. Complex: the products conj(f_ki) x[k] of a row are formed by
+// the half-warp, then one lane subtracts them in ascending k.
+constexpr int kLeftSlots = 3;
+constexpr int kLeftRealMaxN = 5120;  // 3 slots + 2 columns of doubles: 200 KB
+constexpr int kLeftCplxMaxN = 1920;  // 3 slots + 2 columns + 2 product rows of complex: 210 KB
+
+template <bool FORWARD, bool UNIT>
+__global__ void __launch_bounds__(32) left_subst_real_staged_kernel(const double* __restrict__ f, int ldf, double* x,
+                                                                    int ldx, int n, int nrhs) {
+    extern __shared__ __align__(16) double lsm[];
+    double* slots = lsm;                   // kLeftSlots x n
+    double* xs = lsm + kLeftSlots * n;     // 2 x n
+    const int lane = threadIdx.x, L = lane & 15, base = lane & 16, h = lane >> 4;
+    const int col = blockIdx.x * 2 + h;
+    const bool active = col < nrhs;
+    // A half-warp past the last column works on a copy of column 0 and never
+    // writes it back, so that every shuffle sees a converged warp.
+    double* xg = x + (size_t)(active ? col : 0) * ldx;
+    double* y = xs + h * n;
+    for (int p = L; p < n; p += 16) y[p] = xg[p];
+    // Step s reads column i of the factor over rows [0, i] (forward; the
+    // diagonal last) or [i, n) (backward; the diagonal first).
+    auto issue = [&](int s) {
+        if (s < n) {
+            const int i = FORWARD ? s : n - 1 - s;
+            const int r0 = FORWARD ? 0 : i, cnt = FORWARD ? i + 1 : n - i;
+            const double* src = f + (size_t)i * ldf + r0;
+            double* dst = slots + (size_t)(s % kLeftSlots) * n;
+            for (int p = lane; p < cnt; p += 32) cp_async8(dst + p, src + p, true);
+        }
+        cp_async_commit();  // empty past the last step, so that every step waits alike
+    };
+    issue(0);
+    issue(1);
+    constexpr int W = 4;
+    for (int s = 0; s < n; ++s) {
+        issue(s + 2);
+        cp_async_wait<2>();
+        __syncwarp();
+        const int i = FORWARD ? s : n - 1 - s;
+        const int off = FORWARD ? 0 : i + 1;
+        const int len = FORWARD ? i : n - i - 1;
+        const double* col_f = slots + (size_t)(s % kLeftSlots) * n;
+        const double* a = FORWARD ? col_f : col_f + 1;
+        const double diag = FORWARD ? col_f[i] : col_f[0];
+        const double* yy = y + off;
+        const int n16 = (len / (4 * W)) * (4 * W);
+        const int n4 = len >= W ? n16 + ((len - n16) / W) * W : 0;
+        double total = 0.0;
+        if (len >= W) {
+            double acc = 0.0;
+            for (int p = L; p < n16; p += 16) acc = add_rn(acc, mul_rn(a[p], yy[p]));
+            if (L < W)
+                for (int p = n16 + L; p < n4; p += W) acc = add_rn(acc, mul_rn(a[p], yy[p]));
+            total = netdot_combine(acc, L, base);
+        }
+        if (L == 0) {
+            for (int p = n4; p < len; ++p) total = add_rn(total, mul_rn(a[p], yy[p]));
+            double v = sub_rn(y[i], total);
+            if (!UNIT) v = __ddiv_rn(v, diag);
+            y[i] = v;
+        }
+        __syncwarp();
+    }
+    if (active)
+        for (int p = L; p < n; p += 16) xg[p] = y[p];
+}
+
+__global__ void __launch_bounds__(32) left_subst_cplx_unit_back_staged_kernel(const double* __restrict__ f, int ldf,
+                                                                              double* x, int ldx, int n, int nrhs) {
+    extern __shared__ __align__(16) double lsm[];
+    double2* slots = reinterpret_cast<double2*>(lsm);  // kLeftSlots x n
+    double2* xs = slots + kLeftSlots * n;              // 2 x n
+    double2* prod = xs + 2 * n;                        // 2 x n
+    const int lane = threadIdx.x, L = lane & 15, h = lane >> 4;
+    const int col = blockIdx.x * 2 + h;
+    const bool active = col < nrhs;
+    double2* xg = reinterpret_cast<double2*>(x) + (size_t)(active ? col : 0) * ldx;
+    double2* y = xs + h * n;
+    double2* pr = prod + h * n;
+    for (int p = L; p < n; p += 16) y[p] = xg[p];
+    // Step s reads column i = n-1-s of the factor below the diagonal.
+    auto issue = [&](int s) {
+        if (s < n) {
+            const int i = n - 1 - s, cnt = n - i - 1;
+            const double2* src = reinterpret_cast<const double2*>(f) + (size_t)i * ldf + i + 1;
+            double2* dst = slots + (size_t)(s % kLeftSlots) * n;
+            for (int p = lane; p < cnt; p += 32) cp_async16(dst + p, src + p, true);
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    issue(1);
+    for (int s = 0; s < n; ++s) {
+        issue(s + 2);
+        cp_async_wait<2>();
+        __syncwarp();
+        const int i = n - 1 - s, len = n - i - 1;
+        const double2* a = slots + (size_t)(s % kLeftSlots) * n;
+        for (int q = L; q < len; q += 16) {
+            const double2 fk = a[q], xk = y[i + 1 + q];
+            // conj(f) * x in .NET's product order
+            const Z p = zmul(Z{fk.x, -fk.y}, Z{xk.x, xk.y});
+            pr[q] = make_double2(p.re, p.im);
+        }
+        __syncwarp();
+        if (L == 0) {
+            double2 sum = y[i];
+            for (int q = 0; q < len; ++q) {
+                const double2 p = pr[q];
+                sum = make_double2(sub_rn(sum.x, p.x), sub_rn(sum.y, p.y));
+            }
+            y[i] = sum;
+        }
+        __syncwarp();
+    }
+    if (active)
+        for (int p = L; p < n; p += 16) xg[p] = y[p];
+}
+
+// Once per kernel and device: the staged kernels take up to 227 KB of
+// dynamic shared memory. (One instantiation per kernel: the four share a
+// signature, so the flag is keyed on the kernel itself.)
+template <auto KERNEL>
+void allow_left_smem(int device) {
+    static std::atomic<bool> done[64];
+    if (done[device].load(std::memory_order_acquire)) return;
+    TNS_CUDA(cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    done[device].store(true, std::memory_order_release);
+}
+
 // One left-looking solve (see left_subst_real_kernel): real forward U^T
 // (unit = false) or backward L^T (unit or not); complex: backward L^H, unit.
 void left_substitute(Context& ctx, bool cplx, bool forward, bool unit, const double* f, int ldf, double* x, int ldx,
                      int n, int nrhs) {
     if (n == 0 || nrhs == 0) return;
+    const unsigned pairs = (unsigned)((nrhs + 1) / 2);
+    if (!cplx && n <= kLeftRealMaxN) {
+        const size_t smem = sizeof(double) * (size_t)(kLeftSlots + 2) * n;
+        if (forward && !unit) {
+            allow_left_smem<left_subst_real_staged_kernel<true, false>>(ctx.device);
+            left_subst_real_staged_kernel<true, false><<<pairs, 32, smem, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        } else if (!forward && unit) {
+            allow_left_smem<left_subst_real_staged_kernel<false, true>>(ctx.device);
+            left_subst_real_staged_kernel<false, true><<<pairs, 32, smem, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        } else if (!forward && !unit) {
+            allow_left_smem<left_subst_real_staged_kernel<false, false>>(ctx.device);
+            left_subst_real_staged_kernel<false, false><<<pairs, 32, smem, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        } else {
+            fail(TNS_E_ARGUMENT, "internal: no unit forward transposed solve");
+        }
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+        return;
+    }
+    if (cplx && !forward && unit && n <= kLeftCplxMaxN) {
+        const size_t smem = sizeof(double2) * (size_t)(kLeftSlots + 4) * n;
+        allow_left_smem<left_subst_cplx_unit_back_staged_kernel>(ctx.device);
+        left_subst_cplx_unit_back_staged_kernel<<<pairs, 32, smem, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
+        TNS_CUDA(cudaGetLastError());
+        ctx.kernel_launches++;
+        return;
+    }
     if (!cplx) {
         const unsigned grid = (unsigned)((nrhs * 16 + 127) / 128);
         if (forward && !unit) left_subst_real_kernel<true, false><<<grid, 128, 0, ctx.stream>>>(f, ldf, x, ldx, n, nrhs);
