@@ -123,12 +123,13 @@ def test_rcond_matches_oracle(ws, orc, n, cplx):
     assert exact * (1 - 1e-10) <= r <= 3 * exact
 
 
-@pytest.mark.parametrize("n,cplx", [(512, False), (512, True), (1900, True), (3000, False)])
+@pytest.mark.parametrize("n,cplx", [(512, False), (512, True), (1200, True), (3000, False)])
 def test_rcond_and_adjoint_solves_at_larger_orders(ws, orc, n, cplx):
     """The transposed and adjoint solves stage the factor's columns through
-    shared memory up to n = 5120 (real) and 1920 (complex); the estimate and
-    the solves stay the oracle's bit for bit there, odd right-hand-side
-    counts included."""
+    shared memory up to n = 3200 (real) and 1280 (complex), and complex solves
+    of up to 16 right-hand sides run in one launch up to n = 1536; the
+    estimate and the solves stay the oracle's bit for bit there, odd
+    right-hand-side counts included."""
     rng = np.random.default_rng(n + 7)
     a = rng.uniform(-0.5, 0.5, (n, n))
     b = rng.uniform(-0.5, 0.5, (n, 3))
@@ -138,6 +139,7 @@ def test_rcond_and_adjoint_solves_at_larger_orders(ws, orc, n, cplx):
     lu = ws.factor_lu(a)
     f, piv, _ = orc.getrf(a)
     assert np.array_equal(lu.solve_adjoint(b), orc.getrs(f, piv, b, adjoint=True))
+    assert np.array_equal(lu.solve(b), orc.getrs(f, piv, b))
     assert lu.reciprocal_condition() == orc.gecon(f, piv, -1, orc.norm1(a))
 
 
