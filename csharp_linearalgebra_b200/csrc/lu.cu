@@ -1393,15 +1393,28 @@ __global__ void __launch_bounds__(32) subst_fused_kernel(const __grid_constant__
         if (!(xk.re == 0.0 && xk.im == 0.0)) {
             const Z nxk{-xk.re, -xk.im};
             const int i0 = UPPER ? 0 : p + 1, i1 = UPPER ? p : n;
-            for (int i = i0 + L; i < i1; i += 16) {
-                const E fv = fc[i - r0], xv = y[i];
+            auto update = [&](int i, E fv, E xv) {
                 if constexpr (CPLX) {
                     const Z r = subst_axpy<true>(Z{xv.x, xv.y}, nxk, Z{fv.x, fv.y});
                     y[i] = make_double2(r.re, r.im);
                 } else {
                     y[i] = subst_axpy<false>(Z{xv, 0.0}, nxk, Z{fv, 0.0}).re;
                 }
+            };
+            // Rows are independent within a step: four rows' operands are
+            // loaded before their updates.
+            int i = i0 + L;
+            for (; i + 48 < i1; i += 64) {
+                E fv[4], xv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    fv[u] = fc[i + 16 * u - r0];
+                    xv[u] = y[i + 16 * u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) update(i + 16 * u, fv[u], xv[u]);
             }
+            for (; i < i1; i += 16) update(i, fc[i - r0], y[i]);
         }
         // Every lane read x_p above; the divided value goes back only now.
         if ((UPPER || LDIV) && L == 0) {
@@ -1657,8 +1670,17 @@ __global__ void __launch_bounds__(32) left_subst_cplx_unit_back_staged_kernel(co
         }
         __syncwarp();
         if (L == 0) {
+            // Ascending q; eight products loaded ahead of their subtractions.
             double2 sum = y[i];
-            for (int q = 0; q < len; ++q) {
+            int q = 0;
+            for (; q + 8 <= len; q += 8) {
+                double2 pv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) pv[u] = pr[q + u];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) sum = make_double2(sub_rn(sum.x, pv[u].x), sub_rn(sum.y, pv[u].y));
+            }
+            for (; q < len; ++q) {
                 const double2 p = pr[q];
                 sum = make_double2(sub_rn(sum.x, p.x), sub_rn(sum.y, p.y));
             }
